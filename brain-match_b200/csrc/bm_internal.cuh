@@ -1,0 +1,157 @@
+// bm_internal.cuh — device data layout and shared helpers of libbmcuda.
+//
+// HBM layout of one graph (ids 1..n, slot 0 unused):
+//   out_ptr[n+2], in_ptr[n+2]   int32 row offsets (CSR of out-lists, CSC of in-lists)
+//   out_ent[m], in_ent[m]       uint32 packed entries: neighbour id in bits 0..16,
+//                               weight in bits 17..31 (n <= 131071, w <= 32767)
+//   self_w[n+1]                 self-loop weight (0 if none); self-loops are kept
+//                               out of the lists and scored separately
+// Graph B additionally holds
+//   out_twin[m], in_twin[m]     index of the same edge in the other direction
+//   out_ent0[m], in_ent0[m]     the entries with B ids (immutable)
+//   hash[2^k]                   open-addressing table (g*(n+1)+h) -> w of B edges
+// and its live out_ent/in_ent carry neighbour ids relabelled into A space
+// (id = pi^-1(B id)), so B'-out(x) = B-out(pi x) lists A vertices directly.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/bm_cuda.h"
+
+#define BM_ID_BITS 17
+#define BM_ID_MASK ((1u << BM_ID_BITS) - 1u)
+#define BM_MAX_N ((int32_t)BM_ID_MASK)
+#define BM_MAX_W 32767
+#define BM_HASH_EMPTY 0xFFFFFFFFFFFFFFFFull
+
+__host__ __device__ __forceinline__ uint32_t bm_pack(uint32_t id, uint32_t w) { return id | (w << BM_ID_BITS); }
+__host__ __device__ __forceinline__ int32_t bm_eid(uint32_t e) { return (int32_t)(e & BM_ID_MASK); }
+__host__ __device__ __forceinline__ int32_t bm_ew(uint32_t e) { return (int32_t)(e >> BM_ID_BITS); }
+
+struct DevGraph {
+    int32_t n = 0;
+    int64_t m = 0;  // non-self list entries
+    int32_t* out_ptr = nullptr;
+    int32_t* in_ptr = nullptr;
+    uint32_t* out_ent = nullptr;
+    uint32_t* in_ent = nullptr;
+    int32_t* self_w = nullptr;
+    // B only
+    int32_t* out_twin = nullptr;
+    int32_t* in_twin = nullptr;
+    uint32_t* out_ent0 = nullptr;
+    uint32_t* in_ent0 = nullptr;
+    unsigned long long* hash = nullptr;
+    int32_t hash_log2 = 0;
+    // statistics
+    int32_t max_deg = 0;
+    int64_t max_wdeg = 0;
+    int has_self = 0;
+    bool loaded = false;
+};
+
+// Read-only view handed to kernels.
+struct GView {
+    const int32_t* out_ptr;
+    const int32_t* in_ptr;
+    const uint32_t* out_ent;
+    const uint32_t* in_ent;
+    const int32_t* self_w;
+};
+
+struct HashView {
+    const unsigned long long* tab;
+    int32_t log2;
+    int32_t np1;  // n+1, key = g*(n+1)+h
+};
+
+struct bm_ctx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    size_t smem_optin = 0;
+    DevGraph g[2];
+    int32_t n = 0;
+    // mapping state (device)
+    int32_t* pi = nullptr;
+    int32_t* pinv = nullptr;
+    int32_t* ov = nullptr;          // S(v): per-vertex non-self overlap
+    unsigned long long* d_score = nullptr;  // scratch for score reductions
+    bool mapped = false;
+    int64_t score = 0;              // tracked score
+    // staging buffers (device) grown on demand
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+    void* hstage = nullptr;         // pinned host staging
+    size_t hstage_bytes = 0;
+    void* flush_buf = nullptr;
+    size_t flush_bytes = 0;
+    int64_t launches = 0;
+    int32_t row_ctas = 0;           // CTAs per row (cluster size); 0 = auto
+    int32_t row_threads = 512;
+    // host copy of A's adjacency (independence tests of batched swaps)
+    std::vector<int32_t> hA_optr, hA_iptr;
+    std::vector<uint32_t> hA_oent, hA_ient;
+    std::string err;
+};
+
+// Set the error string and return a status.
+bm_status bm_fail(bm_ctx* ctx, bm_status s, const char* fmt, ...);
+bm_status bm_cuda_fail(bm_ctx* ctx, cudaError_t e, const char* what);
+
+#define BM_CUDA(ctx, call)                                            \
+    do {                                                              \
+        cudaError_t _e = (call);                                      \
+        if (_e != cudaSuccess) return bm_cuda_fail((ctx), _e, #call); \
+    } while (0)
+
+#define BM_LAUNCH_CHECK(ctx, name)                                      \
+    do {                                                                \
+        (ctx)->launches++;                                              \
+        cudaError_t _e = cudaGetLastError();                            \
+        if (_e != cudaSuccess) return bm_cuda_fail((ctx), _e, name);    \
+    } while (0)
+
+// Ensure the device staging buffer holds `bytes`.
+bm_status bm_stage(bm_ctx* ctx, size_t bytes);
+bm_status bm_hstage(bm_ctx* ctx, size_t bytes);
+bm_status bm_require_mapped(bm_ctx* ctx);
+
+inline GView gview(const DevGraph& g) { return GView{g.out_ptr, g.in_ptr, g.out_ent, g.in_ent, g.self_w}; }
+inline HashView hview(const DevGraph& g) { return HashView{g.hash, g.hash_log2, g.n + 1}; }
+
+// ------------------------------------------------------------------ device
+
+__host__ __device__ __forceinline__ unsigned long long bm_hash_slot0(unsigned long long key, int log2) {
+    return (key * 0x9E3779B97F4A7C15ull) >> (64 - log2);
+}
+
+// Weight of B edge g->h (B ids), 0 if absent.  The table is at most 3/4 full,
+// so an empty slot ends every probe sequence; the loop is also bounded by the
+// table size.
+__device__ __forceinline__ int32_t bm_hash_get(const HashView& hv, int32_t g, int32_t h) {
+    unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;
+    unsigned long long mask = (1ull << hv.log2) - 1ull;
+    unsigned long long s = bm_hash_slot0(key, hv.log2);
+    for (unsigned long long it = 0; it <= mask; it++) {
+        unsigned long long v = __ldg(hv.tab + s);
+        if (v == BM_HASH_EMPTY) return 0;
+        if ((v >> 16) == key) return (int32_t)(v & 0xFFFFull);
+        s = (s + 1) & mask;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ int32_t imin(int32_t a, int32_t b) { return a < b ? a : b; }
+
+// Kernel launchers implemented across the .cu files.
+bm_status bm_launch_score(bm_ctx* ctx, int64_t* score_out);
+bm_status bm_launch_relabel(bm_ctx* ctx);
+bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_out);
+bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
+                         int64_t* d_full, bm_row_result* d_res);
+bm_status bm_launch_apply(bm_ctx* ctx, const int32_t* d_pairs, int32_t k);
+bm_status bm_rows_smem_check(bm_ctx* ctx);

@@ -1,0 +1,500 @@
+// bm_rows.cu — exact swap deltas of whole rows: delta(u, v) for one u and
+// every v, the m2 sweep of one m1 row of optimize_mapping
+// (src/graph-alignment-optimized.c:542-579), with the per-row reductions the
+// schedules need (first improving column, best column, count).
+//
+// Instead of walking the neighbourhoods of u and v for every pair (about 650
+// scattered probes per pair at the full-scale workload), a row is computed by
+// scattering 2-hop sums into an accumulator acc[v] in shared memory:
+//
+//   T1  x in out_A(u), weight a:  for (v, b) in B'-in(x):   acc[v] += min(a, b)
+//   T2  x in in_A(u),  weight a:  for (v, b) in B'-out(x):  acc[v] += min(a, b)
+//   T3  (y, b) in B'-out(u):      for (v, w) in A-in(y):    acc[v] += min(w, b)
+//   T4  (y, b) in B'-in(u):       for (v, w) in A-out(y):   acc[v] += min(w, b)
+//   C   x in out_A(u) or in_A(u), weight a:  acc[x] += min(a, B(pi u, pi x)) + min(a, B(pi x, pi u))
+//
+// where B'-out(x) = B-out(pi x) with neighbour ids relabelled into A space
+// (maintained by the apply kernel).  Then
+//   delta(u, v) = acc[v] - S(u) - S(v) + self-loop terms     (v != u)
+// which is exactly score(after swap) - score(before) (see bm_pairs.cu for the
+// per-pair form of the same identity).  T1+T2 are the new contributions of u
+// moved to pi v, T3+T4 those of v moved to pi u, C repairs the direct edges.
+//
+// Work per row is the number of 2-hop entries (about 10 per delta at the
+// full-scale workload) and every list is read as a coalesced stream.  Load
+// balance: first-hop items are cut into units of kSeg second-hop entries; the
+// units of a row are dealt round-robin to the CTAs of a thread-block cluster
+// (1..8 CTAs per row) and to their warps.  Each CTA scatters into its own
+// accumulator; after a cluster barrier each CTA sums one slice of v across the
+// cluster's accumulators through distributed shared memory and finalises it.
+#include <cooperative_groups.h>
+
+#include <climits>
+
+#include "bm_internal.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+constexpr int kItemChunk = 1024;  // first-hop items staged per pass
+constexpr int kSeg = 512;         // second-hop entries per work unit
+constexpr int kMaxCluster = 8;
+
+struct RowArgs {
+    const int32_t* Aout_ptr;
+    const int32_t* Ain_ptr;
+    const uint32_t* Aout_ent;
+    const uint32_t* Ain_ent;
+    const int32_t* Bout_ptr;
+    const int32_t* Bin_ptr;
+    const uint32_t* Bout_ent;  // live: ids in A space
+    const uint32_t* Bin_ent;
+    const int32_t* selfA;
+    const int32_t* selfB;
+    int has_self;
+    HashView hb;
+    const int32_t* pi;
+    const int32_t* ov;
+    int32_t n;
+    const int32_t* rows;
+    const int32_t* col_lo;
+    int32_t nrows;
+    int64_t* full;
+    bm_row_result* res;
+};
+
+struct Partial {
+    int32_t first_v;
+    int32_t best_v;
+    int32_t npos;
+    int32_t pad;
+    long long first_d;
+    long long best_d;
+};
+
+__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__host__ __device__ inline size_t rows_smem_bytes(int32_t n) {
+    return align16(sizeof(int32_t) * ((size_t)n + 1))  // acc
+           + sizeof(void*) * kItemChunk                  // item base
+           + sizeof(int32_t) * kItemChunk * 2            // len, cap
+           + sizeof(int32_t) * (kItemChunk + 4)          // unit prefix
+           + sizeof(int32_t) * 32                        // scan scratch
+           + sizeof(Partial) * (kMaxCluster + 32);       // cluster partials + warp partials
+}
+
+__device__ __forceinline__ void better_first(int32_t& v, long long& d, int32_t v2, long long d2) {
+    if (v2 < v) { v = v2; d = d2; }
+}
+
+__device__ __forceinline__ void better_best(int32_t& v, long long& d, int32_t v2, long long d2) {
+    if (d2 > d || (d2 == d && v2 < v)) { v = v2; d = d2; }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
+    constexpr int NW = THREADS / 32;
+    constexpr int IPT = kItemChunk / THREADS;  // items built per thread
+    extern __shared__ __align__(16) unsigned char smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int CL = (int)cluster.num_blocks();
+    const int crank = (int)cluster.block_rank();
+    const int r = blockIdx.x / CL;
+    const int32_t n = a.n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    int32_t* acc = (int32_t*)smem;
+    unsigned char* p = smem + align16(sizeof(int32_t) * ((size_t)n + 1));
+    const uint32_t** it_base = (const uint32_t**)p;
+    p += sizeof(void*) * kItemChunk;
+    int32_t* it_len = (int32_t*)p;
+    int32_t* it_cap = it_len + kItemChunk;
+    int32_t* it_upre = it_cap + kItemChunk;
+    int32_t* scan_tmp = it_upre + kItemChunk + 4;
+    Partial* parts = (Partial*)(scan_tmp + 32);  // [kMaxCluster] cluster partials
+    Partial* wparts = parts + kMaxCluster;       // [32] warp partials
+
+    const int32_t u = (r < a.nrows) ? __ldg(a.rows + r) : 0;
+    const bool valid = (u >= 1 && u <= n);
+
+    for (int32_t i = tid; i <= n; i += THREADS) acc[i] = 0;
+    __syncthreads();
+
+    int32_t fu = 0;
+    if (valid) {
+        fu = __ldg(a.pi + u);
+        const int32_t ao = __ldg(a.Aout_ptr + u), d1 = __ldg(a.Aout_ptr + u + 1) - ao;
+        const int32_t ai = __ldg(a.Ain_ptr + u), d2 = __ldg(a.Ain_ptr + u + 1) - ai;
+        const int32_t bo = __ldg(a.Bout_ptr + fu), d3 = __ldg(a.Bout_ptr + fu + 1) - bo;
+        const int32_t bi = __ldg(a.Bin_ptr + fu), d4 = __ldg(a.Bin_ptr + fu + 1) - bi;
+        const int32_t F = d1 + d2 + d3 + d4;
+        for (int32_t c0 = 0; c0 < F; c0 += kItemChunk) {
+            const int32_t cnt = min(kItemChunk, F - c0);
+            // ---- build this thread's IPT consecutive items
+            int32_t tsum = 0;
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                const int32_t li = tid * IPT + k;
+                const int32_t i = c0 + li;
+                if (li >= cnt) break;
+                const uint32_t* base;
+                int32_t len, cap;
+                if (i < d1 + d2) {
+                    const uint32_t ent = (i < d1) ? __ldg(a.Aout_ent + ao + i) : __ldg(a.Ain_ent + ai + (i - d1));
+                    const int32_t x = bm_eid(ent), w = bm_ew(ent);
+                    const int32_t g = __ldg(a.pi + x);
+                    if (i < d1) {
+                        const int32_t o = __ldg(a.Bin_ptr + g);
+                        base = a.Bin_ent + o;
+                        len = __ldg(a.Bin_ptr + g + 1) - o;
+                    } else {
+                        const int32_t o = __ldg(a.Bout_ptr + g);
+                        base = a.Bout_ent + o;
+                        len = __ldg(a.Bout_ptr + g + 1) - o;
+                    }
+                    cap = w;
+                    if (crank == 0) {
+                        const int32_t c = imin(w, bm_hash_get(a.hb, fu, g)) + imin(w, bm_hash_get(a.hb, g, fu));
+                        if (c) atomicAdd(acc + x, c);
+                    }
+                } else {
+                    const bool outb = i < d1 + d2 + d3;
+                    const uint32_t ent = outb ? __ldg(a.Bout_ent + bo + (i - d1 - d2))
+                                              : __ldg(a.Bin_ent + bi + (i - d1 - d2 - d3));
+                    const int32_t y = bm_eid(ent);
+                    if (outb) {
+                        const int32_t o = __ldg(a.Ain_ptr + y);
+                        base = a.Ain_ent + o;
+                        len = __ldg(a.Ain_ptr + y + 1) - o;
+                    } else {
+                        const int32_t o = __ldg(a.Aout_ptr + y);
+                        base = a.Aout_ent + o;
+                        len = __ldg(a.Aout_ptr + y + 1) - o;
+                    }
+                    cap = bm_ew(ent);
+                }
+                it_base[li] = base;
+                it_len[li] = len;
+                it_cap[li] = cap;
+                tsum += (len + kSeg - 1) / kSeg;
+            }
+            // ---- exclusive scan of units over the block
+            int32_t incl = tsum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (lane == 31) scan_tmp[warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                int32_t wv = (lane < NW) ? scan_tmp[lane] : 0;
+                int32_t wi = wv;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                    if (lane >= o) wi += t;
+                }
+                if (lane < NW) scan_tmp[lane] = wi - wv;  // exclusive warp offsets
+            }
+            __syncthreads();
+            {
+                int32_t run = scan_tmp[warp] + incl - tsum;
+#pragma unroll
+                for (int k = 0; k < IPT; k++) {
+                    const int32_t li = tid * IPT + k;
+                    if (li >= cnt) break;
+                    it_upre[li] = run;
+                    run += (it_len[li] + kSeg - 1) / kSeg;
+                }
+                if (tid * IPT < cnt && (tid + 1) * IPT >= cnt) it_upre[cnt] = run;
+            }
+            __syncthreads();
+            // ---- scatter: units k = crank, crank+CL, ... over this CTA's warps
+            const int32_t U = it_upre[cnt];
+            for (int32_t k = crank + CL * warp; k < U; k += CL * NW) {
+                int32_t lo = 0, hi = cnt;  // last i with it_upre[i] <= k
+                while (hi - lo > 1) {
+                    const int32_t mid = (lo + hi) >> 1;
+                    if (it_upre[mid] <= k) lo = mid; else hi = mid;
+                }
+                const uint32_t* base = it_base[lo];
+                const int32_t cap = it_cap[lo];
+                const int32_t s = (k - it_upre[lo]) * kSeg;
+                const int32_t e = min(it_len[lo], s + kSeg);
+                int32_t j = s + lane;
+                for (; j + 96 < e; j += 128) {
+                    const uint32_t e0 = __ldg(base + j), e1 = __ldg(base + j + 32);
+                    const uint32_t e2 = __ldg(base + j + 64), e3 = __ldg(base + j + 96);
+                    atomicAdd(acc + bm_eid(e0), imin(cap, bm_ew(e0)));
+                    atomicAdd(acc + bm_eid(e1), imin(cap, bm_ew(e1)));
+                    atomicAdd(acc + bm_eid(e2), imin(cap, bm_ew(e2)));
+                    atomicAdd(acc + bm_eid(e3), imin(cap, bm_ew(e3)));
+                }
+                for (; j < e; j += 32) {
+                    const uint32_t e0 = __ldg(base + j);
+                    atomicAdd(acc + bm_eid(e0), imin(cap, bm_ew(e0)));
+                }
+            }
+            __syncthreads();
+        }
+    }
+    cluster.sync();
+
+    // ---- finalise this CTA's slice of v
+    const int32_t slice = (n + CL - 1) / CL;
+    const int32_t vlo = 1 + crank * slice;
+    const int32_t vhi = min(n + 1, vlo + slice);
+    const int32_t collo = (valid && a.col_lo) ? __ldg(a.col_lo + r) : 1;
+    int32_t first_v = INT_MAX, best_v = INT_MAX, npos = 0;
+    long long first_d = 0, best_d = LLONG_MIN;
+    const long long ovu = valid ? (long long)__ldg(a.ov + u) : 0;
+    int32_t sAu = 0, sBu = 0;
+    if (valid && a.has_self) { sAu = __ldg(a.selfA + u); sBu = __ldg(a.selfB + fu); }
+    int64_t* frow = a.full ? a.full + (size_t)r * ((size_t)n + 1) : nullptr;
+    if (frow && crank == 0 && tid == 0) frow[0] = 0;
+    for (int32_t v = vlo + tid; v < vhi; v += THREADS) {
+        long long d = 0;
+        if (valid && v != u) {
+            long long s = acc[v];
+            for (int q = 1; q < CL; q++) {
+                const int rr = (crank + q) % CL;
+                s += *cluster.map_shared_rank(acc + v, rr);
+            }
+            d = s - ovu - (long long)__ldg(a.ov + v);
+            if (a.has_self) {
+                const int32_t sAv = __ldg(a.selfA + v), sBv = __ldg(a.selfB + __ldg(a.pi + v));
+                d += imin(sAu, sBv) - imin(sAu, sBu) + imin(sAv, sBu) - imin(sAv, sBv);
+            }
+            if (v >= collo) {
+                if (d > 0) {
+                    npos++;
+                    if (v < first_v) { first_v = v; first_d = d; }
+                }
+                better_best(best_v, best_d, v, d);
+            }
+        }
+        if (frow) frow[v] = d;
+    }
+    if (a.res) {
+        // warp, then block reduction
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const int32_t fv2 = __shfl_xor_sync(0xffffffffu, first_v, o);
+            const long long fd2 = __shfl_xor_sync(0xffffffffu, first_d, o);
+            const int32_t bv2 = __shfl_xor_sync(0xffffffffu, best_v, o);
+            const long long bd2 = __shfl_xor_sync(0xffffffffu, best_d, o);
+            npos += __shfl_xor_sync(0xffffffffu, npos, o);
+            better_first(first_v, first_d, fv2, fd2);
+            better_best(best_v, best_d, bv2, bd2);
+        }
+        if (lane == 0) wparts[warp] = Partial{first_v, best_v, npos, 0, first_d, best_d};
+        __syncthreads();
+        if (tid == 0) {
+            Partial t = wparts[0];
+            for (int w = 1; w < NW; w++) {
+                better_first(t.first_v, t.first_d, wparts[w].first_v, wparts[w].first_d);
+                better_best(t.best_v, t.best_d, wparts[w].best_v, wparts[w].best_d);
+                t.npos += wparts[w].npos;
+            }
+            *cluster.map_shared_rank(parts + crank, 0) = t;
+        }
+    }
+    cluster.sync();
+    if (a.res && crank == 0 && tid == 0) {
+        Partial t = parts[0];
+        for (int q = 1; q < CL; q++) {
+            better_first(t.first_v, t.first_d, parts[q].first_v, parts[q].first_d);
+            better_best(t.best_v, t.best_d, parts[q].best_v, parts[q].best_d);
+            t.npos += parts[q].npos;
+        }
+        bm_row_result out;
+        out.row = u;
+        out.first_pos = (t.first_v == INT_MAX) ? 0 : t.first_v;
+        out.first_delta = (t.first_v == INT_MAX) ? 0 : t.first_d;
+        out.best = (t.best_v == INT_MAX) ? 0 : t.best_v;
+        out.best_delta = (t.best_v == INT_MAX) ? 0 : t.best_d;
+        out.npos = t.npos;
+        a.res[r] = out;
+    }
+}
+
+template <int THREADS>
+bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem) {
+    static bool configured[64] = {false};
+    auto kern = rows_kernel<THREADS>;
+    if (!configured[ctx->device & 63]) {
+        BM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_optin));
+        configured[ctx->device & 63] = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(args.nrows * cl), 1, 1);
+    cfg.blockDim = dim3(THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BM_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, args));
+    BM_LAUNCH_CHECK(ctx, "rows_kernel");
+    return BM_OK;
+}
+
+template <int THREADS>
+bm_status max_clusters_t(bm_ctx* ctx, int cl, size_t smem, int* out) {
+    auto kern = rows_kernel<THREADS>;
+    BM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_optin));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(cl * 64), 1, 1);
+    cfg.blockDim = dim3(THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BM_CUDA(ctx, cudaOccupancyMaxActiveClusters(out, kern, &cfg));
+    return BM_OK;
+}
+
+}  // namespace
+
+bm_status bm_rows_smem_check(bm_ctx* ctx) {
+    const size_t smem = rows_smem_bytes(ctx->n);
+    if (smem > ctx->smem_optin)
+        return bm_fail(ctx, BM_UNSUPPORTED, "row kernel needs %zu B of shared memory for n=%d; the device allows %zu",
+                       smem, ctx->n, ctx->smem_optin);
+    // Accumulator bound: |acc| <= 4 * max weighted degree of A must fit int32.
+    if (ctx->g[0].max_wdeg * 4 >= (int64_t)INT_MAX)
+        return bm_fail(ctx, BM_UNSUPPORTED, "weighted degree %lld too large for the row kernel's int32 accumulators",
+                       (long long)ctx->g[0].max_wdeg);
+    return BM_OK;
+}
+
+bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows, int64_t* d_full,
+                         bm_row_result* d_res) {
+    if (nrows <= 0) return BM_OK;
+    bm_status st = bm_rows_smem_check(ctx);
+    if (st != BM_OK) return st;
+    const size_t smem = rows_smem_bytes(ctx->n);
+    const DevGraph& A = ctx->g[0];
+    const DevGraph& B = ctx->g[1];
+    RowArgs args;
+    args.Aout_ptr = A.out_ptr;
+    args.Ain_ptr = A.in_ptr;
+    args.Aout_ent = A.out_ent;
+    args.Ain_ent = A.in_ent;
+    args.Bout_ptr = B.out_ptr;
+    args.Bin_ptr = B.in_ptr;
+    args.Bout_ent = B.out_ent;
+    args.Bin_ent = B.in_ent;
+    args.selfA = A.self_w;
+    args.selfB = B.self_w;
+    args.has_self = A.has_self && B.has_self;
+    args.hb = hview(B);
+    args.pi = ctx->pi;
+    args.ov = ctx->ov;
+    args.n = ctx->n;
+    args.rows = d_rows;
+    args.col_lo = d_col_lo;
+    args.full = d_full;
+    args.res = d_res;
+    int cl = ctx->row_ctas;
+    if (cl == 0) {
+        // fill about two CTAs per SM: the largest cluster size with nrows*cl <= 2*SMs
+        cl = 1;
+        while (cl < kMaxCluster && (int64_t)nrows * cl * 2 <= (int64_t)ctx->num_sms * 2) cl *= 2;
+    }
+    // grid.x is limited to 2^31-1; chunk very long row lists
+    const int32_t max_rows_per_launch = 1 << 20;
+    for (int32_t r0 = 0; r0 < nrows; r0 += max_rows_per_launch) {
+        RowArgs ar = args;
+        ar.nrows = min(max_rows_per_launch, nrows - r0);
+        ar.rows = d_rows + r0;
+        ar.col_lo = d_col_lo ? d_col_lo + r0 : nullptr;
+        ar.full = d_full ? d_full + (size_t)r0 * ((size_t)ctx->n + 1) : nullptr;
+        ar.res = d_res ? d_res + r0 : nullptr;
+        st = (ctx->row_threads == 256) ? launch_rows_t<256>(ctx, ar, cl, smem) : launch_rows_t<512>(ctx, ar, cl, smem);
+        if (st != BM_OK) return st;
+    }
+    return BM_OK;
+}
+
+extern "C" bm_status bm_delta_rows_dev(bm_ctx* ctx, const int32_t* d_rows, int32_t nrows, int64_t* d_deltas) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (nrows < 0 || (nrows > 0 && (!d_rows || !d_deltas))) return bm_fail(ctx, BM_INVALID_ARG, "bad row buffers");
+    return bm_launch_rows(ctx, d_rows, nullptr, nrows, d_deltas, nullptr);
+}
+
+extern "C" bm_status bm_rows_best_dev(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
+                                      bm_row_result* d_out) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (nrows < 0 || (nrows > 0 && (!d_rows || !d_out))) return bm_fail(ctx, BM_INVALID_ARG, "bad row buffers");
+    return bm_launch_rows(ctx, d_rows, d_col_lo, nrows, nullptr, d_out);
+}
+
+static bm_status check_rows(bm_ctx* ctx, const int32_t* rows, int32_t nrows) {
+    for (int32_t i = 0; i < nrows; i++)
+        if (rows[i] < 1 || rows[i] > ctx->n)
+            return bm_fail(ctx, BM_INVALID_ARG, "row %d = %d outside 1..%d", i, rows[i], ctx->n);
+    return BM_OK;
+}
+
+extern "C" bm_status bm_delta_rows(bm_ctx* ctx, const int32_t* rows, int32_t nrows, int64_t* deltas) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (nrows < 0 || (nrows > 0 && (!rows || !deltas))) return bm_fail(ctx, BM_INVALID_ARG, "bad row buffers");
+    if (nrows == 0) return BM_OK;
+    if ((s = check_rows(ctx, rows, nrows)) != BM_OK) return s;
+    const size_t in_al = (sizeof(int32_t) * (size_t)nrows + 255) & ~(size_t)255;
+    const size_t out_bytes = sizeof(int64_t) * (size_t)nrows * ((size_t)ctx->n + 1);
+    if ((s = bm_stage(ctx, in_al + out_bytes)) != BM_OK) return s;
+    int32_t* d_rows = (int32_t*)ctx->stage;
+    int64_t* d_out = (int64_t*)((char*)ctx->stage + in_al);
+    BM_CUDA(ctx, cudaMemcpyAsync(d_rows, rows, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = bm_launch_rows(ctx, d_rows, nullptr, nrows, d_out, nullptr)) != BM_OK) return s;
+    BM_CUDA(ctx, cudaMemcpyAsync(deltas, d_out, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_rows_best(bm_ctx* ctx, const int32_t* rows, const int32_t* col_lo, int32_t nrows,
+                                  bm_row_result* out) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (nrows < 0 || (nrows > 0 && (!rows || !out))) return bm_fail(ctx, BM_INVALID_ARG, "bad row buffers");
+    if (nrows == 0) return BM_OK;
+    if ((s = check_rows(ctx, rows, nrows)) != BM_OK) return s;
+    const size_t rb = (sizeof(int32_t) * (size_t)nrows + 255) & ~(size_t)255;
+    const size_t ob = sizeof(bm_row_result) * (size_t)nrows;
+    if ((s = bm_stage(ctx, 2 * rb + ob)) != BM_OK) return s;
+    int32_t* d_rows = (int32_t*)ctx->stage;
+    int32_t* d_col = (int32_t*)((char*)ctx->stage + rb);
+    bm_row_result* d_out = (bm_row_result*)((char*)ctx->stage + 2 * rb);
+    BM_CUDA(ctx, cudaMemcpyAsync(d_rows, rows, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
+    if (col_lo)
+        BM_CUDA(ctx, cudaMemcpyAsync(d_col, col_lo, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = bm_launch_rows(ctx, d_rows, col_lo ? d_col : nullptr, nrows, nullptr, d_out)) != BM_OK) return s;
+    BM_CUDA(ctx, cudaMemcpyAsync(out, d_out, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_rows_max_active_clusters(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads, int32_t* out) {
+    if (!ctx || !out) return BM_INVALID_ARG;
+    const size_t smem = rows_smem_bytes(ctx->n > 0 ? ctx->n : 1);
+    int v = 0;
+    bm_status s = (threads == 256) ? max_clusters_t<256>(ctx, ctas_per_row, smem, &v)
+                                   : max_clusters_t<512>(ctx, ctas_per_row, smem, &v);
+    *out = v;
+    return s;
+}

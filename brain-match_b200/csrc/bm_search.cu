@@ -1,0 +1,310 @@
+// bm_search.cu — host-driven schedules over the row and apply kernels.
+//
+// bm_sweep_parity reproduces the serial first-improvement loop of
+// optimize_mapping (src/graph-alignment-optimized.c:513-580) exactly: rows in
+// order, columns ascending, accept the first delta > 0, continue with the next
+// column under the new mapping.  A batch of K consecutive rows is evaluated at
+// once under the current mapping; rows before the first row with an improving
+// column are exactly what the serial loop would have scanned, the first
+// improving column of that row is the serial loop's next accept, and
+// everything after it is discarded and re-evaluated after the swap.  K adapts
+// (doubling while batches hold no accept, halving after one).
+//
+// bm_search_batched is the throughput schedule: best improving column per row
+// (the row argmax of src/re-alignment-parallel.c:598-618), then a greedy
+// independent subset (descending delta, ascending row; no shared vertex and
+// no A edge between two chosen swaps, the independence rule of
+// src/independent-hungarian/hungarianSubset.c:657-740) applied in one launch.
+// Independent swaps do not change each other's deltas, so the tracked score
+// stays exact.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "bm_internal.cuh"
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+double secs_since(clk::time_point t0) { return std::chrono::duration<double>(clk::now() - t0).count(); }
+
+// Device + pinned staging for one schedule call.
+struct SchedBufs {
+    int32_t* d_rows = nullptr;
+    int32_t* d_col = nullptr;
+    bm_row_result* d_res = nullptr;
+    int32_t* d_pairs = nullptr;
+    int32_t* h_rows = nullptr;
+    int32_t* h_col = nullptr;
+    bm_row_result* h_res = nullptr;
+    int32_t* h_pairs = nullptr;
+};
+
+bm_status sched_bufs(bm_ctx* ctx, int32_t kmax, SchedBufs* b) {
+    const size_t rb = ((size_t)kmax * sizeof(int32_t) + 255) & ~(size_t)255;
+    const size_t resb = ((size_t)kmax * sizeof(bm_row_result) + 255) & ~(size_t)255;
+    const size_t pb = ((size_t)kmax * 2 * sizeof(int32_t) + 255) & ~(size_t)255;
+    const size_t total = 2 * rb + resb + pb;
+    bm_status s = bm_stage(ctx, total);
+    if (s != BM_OK) return s;
+    s = bm_hstage(ctx, total);
+    if (s != BM_OK) return s;
+    char* d = (char*)ctx->stage;
+    char* h = (char*)ctx->hstage;
+    b->d_rows = (int32_t*)d;  b->h_rows = (int32_t*)h;
+    b->d_col = (int32_t*)(d + rb);  b->h_col = (int32_t*)(h + rb);
+    b->d_res = (bm_row_result*)(d + 2 * rb);  b->h_res = (bm_row_result*)(h + 2 * rb);
+    b->d_pairs = (int32_t*)(d + 2 * rb + resb);  b->h_pairs = (int32_t*)(h + 2 * rb + resb);
+    return BM_OK;
+}
+
+bm_status eval_rows(bm_ctx* ctx, SchedBufs& b, int32_t k, bool with_col) {
+    BM_CUDA(ctx, cudaMemcpyAsync(b.d_rows, b.h_rows, sizeof(int32_t) * k, cudaMemcpyHostToDevice, ctx->stream));
+    if (with_col)
+        BM_CUDA(ctx, cudaMemcpyAsync(b.d_col, b.h_col, sizeof(int32_t) * k, cudaMemcpyHostToDevice, ctx->stream));
+    bm_status s = bm_launch_rows(ctx, b.d_rows, with_col ? b.d_col : nullptr, k, nullptr, b.d_res);
+    if (s != BM_OK) return s;
+    BM_CUDA(ctx, cudaMemcpyAsync(b.h_res, b.d_res, sizeof(bm_row_result) * k, cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BM_OK;
+}
+
+bm_status apply_pairs(bm_ctx* ctx, SchedBufs& b, int32_t k) {
+    BM_CUDA(ctx, cudaMemcpyAsync(b.d_pairs, b.h_pairs, sizeof(int32_t) * 2 * k, cudaMemcpyHostToDevice, ctx->stream));
+    return bm_launch_apply(ctx, b.d_pairs, k);
+}
+
+bm_status verify_score(bm_ctx* ctx) {
+    int64_t full = 0;
+    bm_status s = bm_launch_score(ctx, &full);
+    if (s != BM_OK) return s;
+    if (full != ctx->score) {
+        bm_status r = bm_fail(ctx, BM_PARITY_FAIL, "tracked score %lld != recomputed score %lld", (long long)ctx->score,
+                              (long long)full);
+        ctx->score = full;  // trust the recomputation, as the reference does (:572-575)
+        return r;
+    }
+    return BM_OK;
+}
+
+bm_status load_order(bm_ctx* ctx, const int32_t* row_order, int32_t nrows, std::vector<int32_t>& order) {
+    const int32_t n = ctx->n;
+    if (!row_order) {
+        order.resize((size_t)n);
+        for (int32_t i = 0; i < n; i++) order[(size_t)i] = i + 1;
+        return BM_OK;
+    }
+    if (nrows <= 0) return bm_fail(ctx, BM_INVALID_ARG, "empty row order");
+    order.assign(row_order, row_order + nrows);
+    for (int32_t i = 0; i < nrows; i++)
+        if (order[(size_t)i] < 1 || order[(size_t)i] > n)
+            return bm_fail(ctx, BM_INVALID_ARG, "row_order[%d] = %d outside 1..%d", i, order[(size_t)i], n);
+    return BM_OK;
+}
+
+// Marks of closed A neighbourhoods, for the independence test.
+struct Marks {
+    std::vector<uint32_t> stamp;
+    uint32_t cur = 0;
+    void reset(int32_t n) {
+        if (stamp.size() != (size_t)n + 1) { stamp.assign((size_t)n + 1, 0); cur = 0; }
+        if (++cur == 0) { std::fill(stamp.begin(), stamp.end(), 0); cur = 1; }
+    }
+    bool marked(int32_t v) const { return stamp[(size_t)v] == cur; }
+    void mark_closed(const bm_ctx* ctx, int32_t v) {
+        stamp[(size_t)v] = cur;
+        for (int32_t j = ctx->hA_optr[(size_t)v]; j < ctx->hA_optr[(size_t)v + 1]; j++)
+            stamp[(size_t)bm_eid(ctx->hA_oent[(size_t)j])] = cur;
+        for (int32_t j = ctx->hA_iptr[(size_t)v]; j < ctx->hA_iptr[(size_t)v + 1]; j++)
+            stamp[(size_t)bm_eid(ctx->hA_ient[(size_t)j])] = cur;
+    }
+};
+
+}  // namespace
+
+extern "C" bm_status bm_apply_swaps(bm_ctx* ctx, const int32_t* pairs, const int64_t* deltas, int32_t k) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (k < 0 || (k > 0 && !pairs)) return bm_fail(ctx, BM_INVALID_ARG, "bad swap buffers");
+    if (k == 0) return BM_OK;
+    const int32_t n = ctx->n;
+    Marks mk;
+    mk.reset(n);
+    for (int32_t i = 0; i < k; i++) {
+        const int32_t a = pairs[2 * i], b = pairs[2 * i + 1];
+        if (a < 1 || a > n || b < 1 || b > n) return bm_fail(ctx, BM_INVALID_ARG, "swap %d: id outside 1..%d", i, n);
+        if (k > 1) {
+            if (a == b) return bm_fail(ctx, BM_INVALID_ARG, "swap %d: a == b in a batch", i);
+            if (mk.marked(a) || mk.marked(b))
+                return bm_fail(ctx, BM_INVALID_ARG, "swap %d (%d,%d) is not independent of an earlier swap", i, a, b);
+            mk.mark_closed(ctx, a);
+            mk.mark_closed(ctx, b);
+        }
+    }
+    SchedBufs bufs;
+    if ((s = sched_bufs(ctx, k, &bufs)) != BM_OK) return s;
+    memcpy(bufs.h_pairs, pairs, sizeof(int32_t) * 2 * (size_t)k);
+    if ((s = apply_pairs(ctx, bufs, k)) != BM_OK) return s;
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (deltas)
+        for (int32_t i = 0; i < k; i++) ctx->score += deltas[i];
+    return BM_OK;
+}
+
+extern "C" bm_status bm_sweep_parity(bm_ctx* ctx, const int32_t* row_order, int32_t nrows, int64_t max_accepts,
+                                     int32_t max_sweeps, double time_budget_s, bm_progress* prog) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (!prog) return bm_fail(ctx, BM_INVALID_ARG, "progress struct required");
+    if ((s = bm_rows_smem_check(ctx)) != BM_OK) return s;
+    std::vector<int32_t> order;
+    if ((s = load_order(ctx, row_order, nrows, order)) != BM_OK) return s;
+    const int32_t nr = (int32_t)order.size();
+    const int32_t n = ctx->n;
+    const int32_t kmax = std::max(1, std::min(nr, ctx->num_sms));
+    SchedBufs b;
+    if ((s = sched_bufs(ctx, kmax, &b)) != BM_OK) return s;
+
+    const auto t0 = clk::now();
+    int32_t pos = prog->next_row_pos, col = prog->next_col;
+    if (pos < 0 || pos >= nr) pos = 0;
+    if (col < 1 || col > n) col = 1;
+    bool pass_full = (pos == 0 && col == 1);
+    int64_t pass_accepts = 0, accepts0 = prog->accepts;
+    int32_t K = 1;
+    prog->converged = 0;
+    bm_status ret = BM_OK;
+    for (;;) {
+        if (max_accepts >= 0 && prog->accepts - accepts0 >= max_accepts) break;
+        if (time_budget_s > 0 && secs_since(t0) >= time_budget_s) { ret = BM_TIMEOUT; break; }
+        const int32_t k = std::min(K, nr - pos);
+        for (int32_t i = 0; i < k; i++) {
+            b.h_rows[i] = order[(size_t)(pos + i)];
+            b.h_col[i] = (i == 0) ? col : 1;
+        }
+        if ((s = eval_rows(ctx, b, k, true)) != BM_OK) return s;
+        prog->launches++;
+        prog->evaluated += (int64_t)k * (n - 1);
+        int32_t hit = -1;
+        for (int32_t i = 0; i < k; i++)
+            if (b.h_res[i].first_pos != 0) { hit = i; break; }
+        if (hit >= 0) {
+            const int32_t u = b.h_res[hit].row, v = b.h_res[hit].first_pos;
+            b.h_pairs[0] = u;
+            b.h_pairs[1] = v;
+            if ((s = apply_pairs(ctx, b, 1)) != BM_OK) return s;
+            ctx->score += b.h_res[hit].first_delta;
+            prog->accepts++;
+            pass_accepts++;
+            prog->rows_done += hit;
+            pos += hit;
+            col = v + 1;
+            if (col > n) { pos++; col = 1; prog->rows_done++; }
+            K = std::max(1, K / 2);
+        } else {
+            prog->rows_done += k;
+            pos += k;
+            col = 1;
+            K = std::min(kmax, K * 2);
+        }
+        if (pos >= nr) {
+            pos = 0;
+            col = 1;
+            if (pass_full) prog->sweeps++;
+            if (pass_full && pass_accepts == 0) { prog->converged = 1; break; }
+            pass_full = true;
+            pass_accepts = 0;
+            if (max_sweeps >= 0 && prog->sweeps >= max_sweeps) break;
+        }
+    }
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    prog->next_row_pos = pos;
+    prog->next_col = col;
+    prog->seconds += secs_since(t0);
+    s = verify_score(ctx);
+    prog->score = ctx->score;
+    if (s != BM_OK) return s;
+    return ret;
+}
+
+extern "C" bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, int32_t nrows, int32_t rows_per_batch,
+                                       int64_t max_accepts, int32_t max_sweeps, double time_budget_s,
+                                       int64_t target_score, bm_progress* prog) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (!prog) return bm_fail(ctx, BM_INVALID_ARG, "progress struct required");
+    if ((s = bm_rows_smem_check(ctx)) != BM_OK) return s;
+    std::vector<int32_t> order;
+    if ((s = load_order(ctx, row_order, nrows, order)) != BM_OK) return s;
+    const int32_t nr = (int32_t)order.size();
+    const int32_t n = ctx->n;
+    int32_t R = rows_per_batch > 0 ? rows_per_batch : 2 * ctx->num_sms;
+    R = std::min(R, nr);
+    SchedBufs b;
+    if ((s = sched_bufs(ctx, R, &b)) != BM_OK) return s;
+    std::vector<int32_t> cand;
+    Marks mk;
+    const auto t0 = clk::now();
+    int32_t pos = prog->next_row_pos;
+    if (pos < 0 || pos >= nr) pos = 0;
+    bool pass_full = (pos == 0);
+    int64_t pass_accepts = 0, accepts0 = prog->accepts;
+    prog->converged = 0;
+    bm_status ret = BM_OK;
+    for (;;) {
+        if (max_accepts >= 0 && prog->accepts - accepts0 >= max_accepts) break;
+        if (target_score > 0 && ctx->score >= target_score) break;
+        if (time_budget_s > 0 && secs_since(t0) >= time_budget_s) { ret = BM_TIMEOUT; break; }
+        const int32_t k = std::min(R, nr - pos);
+        for (int32_t i = 0; i < k; i++) b.h_rows[i] = order[(size_t)(pos + i)];
+        if ((s = eval_rows(ctx, b, k, false)) != BM_OK) return s;
+        prog->launches++;
+        prog->evaluated += (int64_t)k * (n - 1);
+        cand.clear();
+        for (int32_t i = 0; i < k; i++)
+            if (b.h_res[i].best_delta > 0) cand.push_back(i);
+        std::sort(cand.begin(), cand.end(), [&](int32_t x, int32_t y) {
+            if (b.h_res[x].best_delta != b.h_res[y].best_delta) return b.h_res[x].best_delta > b.h_res[y].best_delta;
+            return x < y;
+        });
+        mk.reset(n);
+        int32_t na = 0;
+        int64_t gain = 0;
+        for (int32_t i : cand) {
+            const int32_t u = b.h_res[i].row, v = b.h_res[i].best;
+            if (mk.marked(u) || mk.marked(v)) continue;
+            mk.mark_closed(ctx, u);
+            mk.mark_closed(ctx, v);
+            b.h_pairs[2 * na] = u;
+            b.h_pairs[2 * na + 1] = v;
+            gain += b.h_res[i].best_delta;
+            na++;
+        }
+        if (na > 0) {
+            if ((s = apply_pairs(ctx, b, na)) != BM_OK) return s;
+            ctx->score += gain;
+            prog->accepts += na;
+            pass_accepts += na;
+        }
+        prog->rows_done += k;
+        pos += k;
+        if (pos >= nr) {
+            pos = 0;
+            if (pass_full) prog->sweeps++;
+            if (pass_full && pass_accepts == 0) { prog->converged = 1; break; }
+            pass_full = true;
+            pass_accepts = 0;
+            if (max_sweeps >= 0 && prog->sweeps >= max_sweeps) break;
+        }
+    }
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    prog->next_row_pos = pos;
+    prog->next_col = 1;
+    prog->seconds += secs_since(t0);
+    s = verify_score(ctx);
+    prog->score = ctx->score;
+    if (s != BM_OK) return s;
+    return ret;
+}

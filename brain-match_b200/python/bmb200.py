@@ -1,0 +1,485 @@
+"""ctypes binding of the engine's C ABI (include/bm_cuda.h, include/bm_host.h).
+
+The engine is C/CUDA; this module only marshals numpy arrays across the ABI for
+tests and benchmarks.  It never computes deltas itself and has no CPU path:
+if libbmcuda.so is missing or no GPU is present, the calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REPO_DIR = os.path.dirname(PKG_DIR)
+LIB_DIR = os.path.join(PKG_DIR, "lib")
+BIN_DIR = os.path.join(PKG_DIR, "bin")
+INCLUDE_DIR = os.path.join(REPO_DIR, "include")
+
+BM_OK, BM_INVALID_ARG, BM_OOM, BM_CUDA_ERROR, BM_TIMEOUT, BM_PARITY_FAIL, BM_UNSUPPORTED, BM_NO_DEVICE = range(8)
+STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "CUDA_ERROR", "TIMEOUT", "PARITY_FAIL", "UNSUPPORTED", "NO_DEVICE"]
+SIDE_A, SIDE_B = 0, 1
+
+
+def build(jobs: int = 8) -> None:
+    """Compile libbmcuda.so (sm_100a), libbmhost.so and the CLIs in-tree."""
+    subprocess.run(["make", "-C", PKG_DIR, f"-j{jobs}"], check=True, stdout=subprocess.DEVNULL)
+
+
+def _lib(name: str) -> C.CDLL:
+    path = os.path.join(LIB_DIR, name)
+    if not os.path.exists(path):
+        build()
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing and could not be built")
+    return C.CDLL(path)
+
+
+class RowResult(C.Structure):
+    _fields_ = [("row", C.c_int32), ("first_pos", C.c_int32), ("best", C.c_int32), ("npos", C.c_int32),
+                ("first_delta", C.c_int64), ("best_delta", C.c_int64)]
+
+
+ROW_DTYPE = np.dtype([("row", np.int32), ("first_pos", np.int32), ("best", np.int32), ("npos", np.int32),
+                      ("first_delta", np.int64), ("best_delta", np.int64)])
+assert ROW_DTYPE.itemsize == C.sizeof(RowResult)
+
+
+class Progress(C.Structure):
+    _fields_ = [("rows_done", C.c_int64), ("evaluated", C.c_int64), ("accepts", C.c_int64), ("score", C.c_int64),
+                ("launches", C.c_int64), ("next_row_pos", C.c_int32), ("next_col", C.c_int32),
+                ("sweeps", C.c_int32), ("converged", C.c_int32), ("seconds", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GenParams(C.Structure):
+    _fields_ = [("n", C.c_int32), ("m_target", C.c_int64), ("degree_model", C.c_int32), ("alpha", C.c_double),
+                ("max_degree", C.c_int32), ("weight_model", C.c_int32), ("geo_p", C.c_double),
+                ("tail_frac", C.c_double), ("tail_max", C.c_int32), ("del_frac", C.c_double),
+                ("add_frac", C.c_double), ("jitter", C.c_int32), ("shuffle_frac", C.c_double),
+                ("init_mode", C.c_int32), ("seed", C.c_uint64)]
+
+
+class Edges(C.Structure):
+    _fields_ = [("n", C.c_int32), ("m", C.c_int64), ("src", C.POINTER(C.c_int32)), ("dst", C.POINTER(C.c_int32)),
+                ("w", C.POINTER(C.c_int32))]
+
+
+I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+I64P = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+_cuda = None
+_host = None
+
+
+def cuda_lib() -> C.CDLL:
+    global _cuda
+    if _cuda is None:
+        L = _lib("libbmcuda.so")
+        vp = C.c_void_p
+        sig = {
+            "bm_ctx_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+            "bm_ctx_destroy": (None, [vp]),
+            "bm_status_str": (C.c_char_p, [C.c_int]),
+            "bm_ctx_last_error": (C.c_char_p, [vp]),
+            "bm_ctx_stream": (vp, [vp]),
+            "bm_sync": (C.c_int, [vp]),
+            "bm_set_graph": (C.c_int, [vp, C.c_int, C.c_int32, C.c_int64, vp, vp, vp]),
+            "bm_graph_info": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+            "bm_set_mapping": (C.c_int, [vp, vp]),
+            "bm_get_mapping": (C.c_int, [vp, vp]),
+            "bm_score": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+            "bm_tracked_score": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+            "bm_get_overlap": (C.c_int, [vp, vp]),
+            "bm_delta_pairs": (C.c_int, [vp, vp, C.c_int64, vp]),
+            "bm_delta_pairs_dev": (C.c_int, [vp, vp, C.c_int64, vp]),
+            "bm_delta_rows": (C.c_int, [vp, vp, C.c_int32, vp]),
+            "bm_delta_rows_dev": (C.c_int, [vp, vp, C.c_int32, vp]),
+            "bm_rows_best": (C.c_int, [vp, vp, vp, C.c_int32, vp]),
+            "bm_rows_best_dev": (C.c_int, [vp, vp, vp, C.c_int32, vp]),
+            "bm_apply_swaps": (C.c_int, [vp, vp, vp, C.c_int32]),
+            "bm_sweep_parity": (C.c_int, [vp, vp, C.c_int32, C.c_int64, C.c_int32, C.c_double, C.POINTER(Progress)]),
+            "bm_search_batched": (C.c_int, [vp, vp, C.c_int32, C.c_int32, C.c_int64, C.c_int32, C.c_double,
+                                            C.c_int64, C.POINTER(Progress)]),
+            "bm_dev_alloc": (C.c_int, [vp, C.c_int64, C.POINTER(vp)]),
+            "bm_dev_free": (C.c_int, [vp, vp]),
+            "bm_memcpy_h2d": (C.c_int, [vp, vp, vp, C.c_int64]),
+            "bm_memcpy_d2h": (C.c_int, [vp, vp, vp, C.c_int64]),
+            "bm_host_alloc_pinned": (C.c_int, [C.c_int64, C.POINTER(vp)]),
+            "bm_host_free_pinned": (C.c_int, [vp]),
+            "bm_l2_flush": (C.c_int, [vp]),
+            "bm_event_create": (C.c_int, [vp, C.POINTER(vp)]),
+            "bm_event_destroy": (C.c_int, [vp, vp]),
+            "bm_event_record": (C.c_int, [vp, vp]),
+            "bm_event_elapsed_ms": (C.c_int, [vp, vp, vp, C.POINTER(C.c_float)]),
+            "bm_launch_count": (C.c_int64, [vp]),
+            "bm_set_row_tiling": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "bm_get_row_tiling": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _cuda = L
+    return _cuda
+
+
+def host_lib() -> C.CDLL:
+    global _host
+    if _host is None:
+        L = _lib("libbmhost.so")
+        vp = C.c_void_p
+        sig = {
+            "bm_edges_free": (None, [C.POINTER(Edges)]),
+            "bm_read_graph_csv": (C.c_int, [C.c_char_p, C.POINTER(Edges), C.POINTER(C.c_int64)]),
+            "bm_write_graph_csv": (C.c_int, [C.c_char_p, C.POINTER(Edges)]),
+            "bm_read_ordering": (C.c_int, [C.c_char_p, C.c_int32, vp]),
+            "bm_write_ordering": (C.c_int, [C.c_char_p, C.c_int32, vp]),
+            "bm_read_mapping": (C.c_int, [C.c_char_p, C.c_int32, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+            "bm_write_mapping": (C.c_int, [C.c_char_p, C.c_int32, vp]),
+            "bm_scan_mapping_max_id": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32)]),
+            "bm_gen_defaults": (C.c_int, [C.c_int, C.POINTER(GenParams)]),
+            "bm_gen_pair": (C.c_int, [C.POINTER(GenParams), C.POINTER(Edges), C.POINTER(Edges), vp, vp]),
+            "bm_ordering_by_weighted_degree": (None, [C.POINTER(Edges), vp]),
+            "bm_rows_from_ordering": (None, [C.c_int32, vp, vp]),
+            "bm_greedy_match": (C.c_int, [C.POINTER(Edges), C.POINTER(Edges), vp]),
+            "bm_host_score": (C.c_int64, [C.POINTER(Edges), C.POINTER(Edges), vp]),
+            "bm_check_bijection": (C.c_int32, [C.c_int32, vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _host = L
+    return _host
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+# ---------------------------------------------------------------- host side
+
+class Graph:
+    """An edge list with ids 1..n (numpy int32 arrays)."""
+
+    def __init__(self, n: int, src, dst, w):
+        self.n = int(n)
+        self.src, self.dst, self.w = _i32(src), _i32(dst), _i32(w)
+
+    @property
+    def m(self) -> int:
+        return int(self.src.shape[0])
+
+    def edges_struct(self) -> Edges:
+        e = Edges()
+        e.n, e.m = self.n, self.m
+        e.src = self.src.ctypes.data_as(C.POINTER(C.c_int32))
+        e.dst = self.dst.ctypes.data_as(C.POINTER(C.c_int32))
+        e.w = self.w.ctypes.data_as(C.POINTER(C.c_int32))
+        return e
+
+
+def _take_edges(e: Edges) -> Graph:
+    m = int(e.m)
+    g = Graph(e.n, np.ctypeslib.as_array(e.src, (m,)).copy() if m else np.zeros(0, np.int32),
+              np.ctypeslib.as_array(e.dst, (m,)).copy() if m else np.zeros(0, np.int32),
+              np.ctypeslib.as_array(e.w, (m,)).copy() if m else np.zeros(0, np.int32))
+    host_lib().bm_edges_free(C.byref(e))
+    return g
+
+
+def gen_params(config: int, **overrides) -> GenParams:
+    p = GenParams()
+    if host_lib().bm_gen_defaults(int(config), C.byref(p)) != 0:
+        raise ValueError(f"unknown workload config {config}")
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def gen_pair(config: int, **overrides):
+    """Synthetic pair: returns (A, B, pi_true, pi_init)."""
+    p = gen_params(config, **overrides)
+    a, b = Edges(), Edges()
+    truth = np.zeros(p.n + 1, np.int32)
+    init = np.zeros(p.n + 1, np.int32)
+    if host_lib().bm_gen_pair(C.byref(p), C.byref(a), C.byref(b), _ptr(truth), _ptr(init)) != 0:
+        raise RuntimeError("bm_gen_pair failed")
+    return _take_edges(a), _take_edges(b), truth, init
+
+
+def read_graph_csv(path: str):
+    e = Edges()
+    bad = C.c_int64(0)
+    if host_lib().bm_read_graph_csv(path.encode(), C.byref(e), C.byref(bad)) != 0:
+        raise OSError(f"cannot read {path}")
+    return _take_edges(e), int(bad.value)
+
+
+def write_graph_csv(path: str, g: Graph) -> None:
+    e = g.edges_struct()
+    if host_lib().bm_write_graph_csv(path.encode(), C.byref(e)) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def read_mapping(path: str, n: int):
+    pi = np.zeros(n + 1, np.int32)
+    cnt, mx = C.c_int64(0), C.c_int32(0)
+    if host_lib().bm_read_mapping(path.encode(), n, _ptr(pi), C.byref(cnt), C.byref(mx)) != 0:
+        raise OSError(f"cannot read {path}")
+    return pi, int(cnt.value), int(mx.value)
+
+
+def write_mapping(path: str, pi: np.ndarray) -> None:
+    pi = _i32(pi)
+    if host_lib().bm_write_mapping(path.encode(), pi.shape[0] - 1, _ptr(pi)) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def read_ordering(path: str, n: int) -> np.ndarray:
+    o = np.zeros(n + 1, np.int32)
+    if host_lib().bm_read_ordering(path.encode(), n, _ptr(o)) != 0:
+        raise OSError(f"cannot read {path}")
+    return o
+
+
+def write_ordering(path: str, order: np.ndarray) -> None:
+    order = _i32(order)
+    if host_lib().bm_write_ordering(path.encode(), order.shape[0] - 1, _ptr(order)) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def ordering_by_weighted_degree(g: Graph) -> np.ndarray:
+    o = np.zeros(g.n + 1, np.int32)
+    e = g.edges_struct()
+    host_lib().bm_ordering_by_weighted_degree(C.byref(e), _ptr(o))
+    return o
+
+
+def rows_from_ordering(order: np.ndarray) -> np.ndarray:
+    order = _i32(order)
+    n = order.shape[0] - 1
+    rows = np.zeros(n, np.int32)
+    host_lib().bm_rows_from_ordering(n, _ptr(order), _ptr(rows))
+    return rows
+
+
+def greedy_match(A: Graph, B: Graph) -> np.ndarray:
+    n = max(A.n, B.n)
+    pi = np.zeros(n + 1, np.int32)
+    a, b = A.edges_struct(), B.edges_struct()
+    if host_lib().bm_greedy_match(C.byref(a), C.byref(b), _ptr(pi)) != 0:
+        raise RuntimeError("bm_greedy_match failed")
+    return pi
+
+
+def host_score(A: Graph, B: Graph, pi: np.ndarray) -> int:
+    a, b = A.edges_struct(), B.edges_struct()
+    return int(host_lib().bm_host_score(C.byref(a), C.byref(b), _ptr(_i32(pi))))
+
+
+def check_bijection(pi: np.ndarray) -> int:
+    pi = _i32(pi)
+    return int(host_lib().bm_check_bijection(pi.shape[0] - 1, _ptr(pi)))
+
+
+# -------------------------------------------------------------- device side
+
+class BMError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        self.status = status
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"{name}: {msg}")
+
+
+class Engine:
+    """One device context: graphs, mapping and the search state."""
+
+    def __init__(self, device: int = 0):
+        self.L = cuda_lib()
+        h = C.c_void_p()
+        st = self.L.bm_ctx_create(device, C.byref(h))
+        if st != BM_OK:
+            raise BMError(st, f"bm_ctx_create({device})")
+        self.h = h
+        self.n = 0
+
+    def _chk(self, st: int, what: str, ok=(BM_OK,)) -> int:
+        if st not in ok:
+            raise BMError(st, f"{what}: {self.L.bm_ctx_last_error(self.h).decode()}")
+        return st
+
+    def close(self) -> None:
+        if self.h:
+            self.L.bm_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # graphs and mapping
+    def set_graph(self, side: int, g: Graph) -> None:
+        self._chk(self.L.bm_set_graph(self.h, side, g.n, g.m, _ptr(g.src), _ptr(g.dst), _ptr(g.w)), "bm_set_graph")
+        self.n = g.n
+
+    def set_graphs(self, A: Graph, B: Graph) -> None:
+        self.set_graph(SIDE_A, A)
+        self.set_graph(SIDE_B, B)
+
+    def graph_info(self, side: int) -> dict:
+        n, m, d, wd = C.c_int32(), C.c_int64(), C.c_int32(), C.c_int64()
+        self._chk(self.L.bm_graph_info(self.h, side, C.byref(n), C.byref(m), C.byref(d), C.byref(wd)), "bm_graph_info")
+        return {"n": n.value, "m": m.value, "max_degree": d.value, "max_weighted_degree": wd.value}
+
+    def set_mapping(self, pi) -> None:
+        pi = _i32(pi)
+        self._chk(self.L.bm_set_mapping(self.h, _ptr(pi)), "bm_set_mapping")
+
+    def get_mapping(self) -> np.ndarray:
+        pi = np.zeros(self.n + 1, np.int32)
+        self._chk(self.L.bm_get_mapping(self.h, _ptr(pi)), "bm_get_mapping")
+        return pi
+
+    def score(self) -> int:
+        s = C.c_int64()
+        self._chk(self.L.bm_score(self.h, C.byref(s)), "bm_score")
+        return s.value
+
+    def tracked_score(self) -> int:
+        s = C.c_int64()
+        self._chk(self.L.bm_tracked_score(self.h, C.byref(s)), "bm_tracked_score")
+        return s.value
+
+    def overlap(self) -> np.ndarray:
+        o = np.zeros(self.n + 1, np.int32)
+        self._chk(self.L.bm_get_overlap(self.h, _ptr(o)), "bm_get_overlap")
+        return o
+
+    # deltas
+    def delta_pairs(self, pairs) -> np.ndarray:
+        pairs = _i32(pairs).reshape(-1)
+        k = pairs.shape[0] // 2
+        out = np.zeros(k, np.int64)
+        self._chk(self.L.bm_delta_pairs(self.h, _ptr(pairs), k, _ptr(out)), "bm_delta_pairs")
+        return out
+
+    def delta_rows(self, rows) -> np.ndarray:
+        rows = _i32(rows).reshape(-1)
+        out = np.zeros((rows.shape[0], self.n + 1), np.int64)
+        self._chk(self.L.bm_delta_rows(self.h, _ptr(rows), rows.shape[0], _ptr(out)), "bm_delta_rows")
+        return out
+
+    def rows_best(self, rows, col_lo=None) -> np.ndarray:
+        rows = _i32(rows).reshape(-1)
+        out = np.zeros(rows.shape[0], ROW_DTYPE)
+        cl = None if col_lo is None else _i32(col_lo).reshape(-1)
+        self._chk(self.L.bm_rows_best(self.h, _ptr(rows), None if cl is None else _ptr(cl), rows.shape[0], _ptr(out)),
+                  "bm_rows_best")
+        return out
+
+    def apply_swaps(self, pairs, deltas=None) -> None:
+        pairs = _i32(pairs).reshape(-1)
+        d = None if deltas is None else np.ascontiguousarray(np.asarray(deltas, np.int64))
+        self._chk(self.L.bm_apply_swaps(self.h, _ptr(pairs), None if d is None else _ptr(d), pairs.shape[0] // 2),
+                  "bm_apply_swaps")
+
+    # schedules
+    def sweep_parity(self, rows=None, max_accepts=-1, max_sweeps=-1, time_budget=0.0, prog=None):
+        prog = prog or Progress()
+        r = None if rows is None else _i32(rows)
+        st = self.L.bm_sweep_parity(self.h, None if r is None else _ptr(r), 0 if r is None else r.shape[0],
+                                    max_accepts, max_sweeps, time_budget, C.byref(prog))
+        self._chk(st, "bm_sweep_parity", ok=(BM_OK, BM_TIMEOUT))
+        return prog, st
+
+    def search_batched(self, rows=None, rows_per_batch=0, max_accepts=-1, max_sweeps=-1, time_budget=0.0,
+                       target_score=0, prog=None):
+        prog = prog or Progress()
+        r = None if rows is None else _i32(rows)
+        st = self.L.bm_search_batched(self.h, None if r is None else _ptr(r), 0 if r is None else r.shape[0],
+                                      rows_per_batch, max_accepts, max_sweeps, time_budget, target_score,
+                                      C.byref(prog))
+        self._chk(st, "bm_search_batched", ok=(BM_OK, BM_TIMEOUT))
+        return prog, st
+
+    def set_row_tiling(self, ctas_per_row: int = 0, threads: int = 0) -> None:
+        self._chk(self.L.bm_set_row_tiling(self.h, ctas_per_row, threads), "bm_set_row_tiling")
+
+    def launch_count(self) -> int:
+        return int(self.L.bm_launch_count(self.h))
+
+    # device utilities
+    def dev_alloc(self, nbytes: int) -> int:
+        p = C.c_void_p()
+        self._chk(self.L.bm_dev_alloc(self.h, nbytes, C.byref(p)), "bm_dev_alloc")
+        return p.value
+
+    def dev_free(self, p: int) -> None:
+        self._chk(self.L.bm_dev_free(self.h, p), "bm_dev_free")
+
+    def h2d(self, dptr: int, a: np.ndarray) -> None:
+        self._chk(self.L.bm_memcpy_h2d(self.h, dptr, _ptr(a), a.nbytes), "bm_memcpy_h2d")
+
+    def d2h(self, a: np.ndarray, dptr: int) -> None:
+        self._chk(self.L.bm_memcpy_d2h(self.h, _ptr(a), dptr, a.nbytes), "bm_memcpy_d2h")
+
+    def sync(self) -> None:
+        self._chk(self.L.bm_sync(self.h), "bm_sync")
+
+    def l2_flush(self) -> None:
+        self._chk(self.L.bm_l2_flush(self.h), "bm_l2_flush")
+
+    def event(self) -> int:
+        e = C.c_void_p()
+        self._chk(self.L.bm_event_create(self.h, C.byref(e)), "bm_event_create")
+        return e.value
+
+    def record(self, ev: int) -> None:
+        self._chk(self.L.bm_event_record(self.h, ev), "bm_event_record")
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_float()
+        self._chk(self.L.bm_event_elapsed_ms(self.h, a, b, C.byref(ms)), "bm_event_elapsed_ms")
+        return ms.value
+
+    def rows_best_dev(self, d_rows: int, d_col: int | None, nrows: int, d_out: int) -> None:
+        self._chk(self.L.bm_rows_best_dev(self.h, d_rows, d_col, nrows, d_out), "bm_rows_best_dev")
+
+    def delta_rows_dev(self, d_rows: int, nrows: int, d_out: int) -> None:
+        self._chk(self.L.bm_delta_rows_dev(self.h, d_rows, nrows, d_out), "bm_delta_rows_dev")
+
+    def delta_pairs_dev(self, d_pairs: int, k: int, d_out: int) -> None:
+        self._chk(self.L.bm_delta_pairs_dev(self.h, d_pairs, k, d_out), "bm_delta_pairs_dev")
+
+
+def header_functions(header: str = "bm_cuda.h") -> list[str]:
+    """Names of the functions declared in include/<header>."""
+    import re
+    txt = open(os.path.join(INCLUDE_DIR, header)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = re.findall(r"\b(bm_[a-z0-9_]+)\s*\(", txt)
+    seen, out = set(), []
+    for nme in names:
+        if nme not in seen:
+            seen.add(nme)
+            out.append(nme)
+    return out

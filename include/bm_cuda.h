@@ -1,0 +1,213 @@
+/*
+ * bm_cuda.h — C ABI of the B200 swap-search engine (libbmcuda.so).
+ *
+ * Plain C types only: pointers, sizes and status codes.  Every entry point
+ * returns a bm_status; the library never calls exit().  One context owns one
+ * device and one CUDA stream; a context is not re-entrant, different contexts
+ * may be driven from different host threads.
+ *
+ * Problem: two weighted directed graphs A ("male", gm) and B ("female", gf)
+ * on vertex ids 1..n, and a bijection pi: A-vertex -> B-vertex stored 1-indexed
+ * in an int32 array of length n+1 (slot 0 unused), exactly like the `mapping`
+ * array of the reference tools.  The objective is the edge-overlap score
+ *     score(pi) = sum over A edges (x->y, w) of min(w, w_B(pi x, pi y))
+ * (w_B = 0 for absent edges), computed in int64.
+ *
+ * Semantics ("exact"): a swap delta is score(pi after swapping pi(u),pi(v))
+ * minus score(pi), with score as in calculate_alignment_score
+ * (src/graph-alignment-optimized.c:292-307): every A edge-list entry counts
+ * (duplicate A edges count once per entry), B is a matrix (the last duplicate
+ * weight wins, src/graph-alignment-optimized.c:185).  Self-loops are scored
+ * exactly; on graphs without self-loops this equals calculate_swap_delta
+ * (src/graph-alignment-optimized.c:321-408) for every pair.
+ *
+ * Limits: n <= 131071, 0 <= w <= 32767 (the reference stores B weights as
+ * int16), fewer than 2^31 edges per graph, at most one self-loop per A vertex.
+ * Inputs outside these limits are rejected with BM_INVALID_ARG.
+ */
+#ifndef BM_CUDA_H
+#define BM_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bm_status {
+    BM_OK = 0,
+    BM_INVALID_ARG = 1,   /* bad size, id, weight, non-bijective mapping, missing graph */
+    BM_OOM = 2,           /* device or host allocation failed */
+    BM_CUDA_ERROR = 3,    /* a CUDA runtime call or kernel launch failed */
+    BM_TIMEOUT = 4,       /* a time or iteration budget ran out before completion */
+    BM_PARITY_FAIL = 5,   /* a self-check (score re-verification) disagreed */
+    BM_UNSUPPORTED = 6,   /* the request exceeds what the chosen kernel supports */
+    BM_NO_DEVICE = 7      /* no CUDA device, or the requested ordinal does not exist */
+} bm_status;
+
+typedef struct bm_ctx bm_ctx;
+
+#define BM_SIDE_A 0   /* "male" graph gm: the graph whose edges are scored */
+#define BM_SIDE_B 1   /* "female" graph gf: the graph looked up at mapped ends */
+
+/* ---------------------------------------------------------------- lifecycle */
+
+/* Create a context on `device` (ordinal).  Replaces the implicit global state
+ * of the reference tools (main in src/graph-alignment-optimized.c:682-738,
+ * cudaSetDevice in src/graph-re-alignment-gpu.cu:1304). */
+bm_status bm_ctx_create(int device, bm_ctx** out);
+void bm_ctx_destroy(bm_ctx* ctx);
+const char* bm_status_str(bm_status s);
+/* Last error message recorded on this context ("" if none). */
+const char* bm_ctx_last_error(const bm_ctx* ctx);
+/* The context's cudaStream_t, as an opaque pointer. */
+void* bm_ctx_stream(bm_ctx* ctx);
+bm_status bm_sync(bm_ctx* ctx);
+
+/* ------------------------------------------------------------------- graphs */
+
+/* Upload one graph from an edge list (ids 1..n).  The library copies; the
+ * caller keeps ownership of the host arrays.  Replaces load_graph_from_csv +
+ * add_edge (src/graph-alignment-optimized.c:183-204, 635-679): A keeps every
+ * list entry, B keeps the last weight of a duplicated edge.  Both graphs must
+ * share the same n.  Setting a graph invalidates the mapping. */
+bm_status bm_set_graph(bm_ctx* ctx, int side, int32_t n, int64_t m,
+                       const int32_t* src, const int32_t* dst, const int32_t* w);
+
+/* Graph statistics after upload: n, non-self entries, max in+out degree. */
+bm_status bm_graph_info(bm_ctx* ctx, int side, int32_t* n, int64_t* m_nonself,
+                        int32_t* max_degree, int64_t* max_weighted_degree);
+
+/* ------------------------------------------------------------------ mapping */
+
+/* Set pi (host, n+1 entries, 1-indexed, slot 0 ignored).  pi must be a
+ * bijection of 1..n (the check of verify_mapping, src/verify-mapping.c:199-232).
+ * Recomputes the per-vertex overlap and the score on the device. */
+bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* pi);
+/* Copy the current pi back to the host (n+1 entries, slot 0 = 0). */
+bm_status bm_get_mapping(bm_ctx* ctx, int32_t* pi);
+
+/* ------------------------------------------------------------------- scoring */
+
+/* Full score of the current pi, recomputed from scratch on the device.
+ * Replaces calculate_alignment_score (src/graph-alignment-optimized.c:292-307)
+ * and score-matching's calculate_score_sparse (src/score-matching.c:558-597). */
+bm_status bm_score(bm_ctx* ctx, int64_t* score);
+/* Score tracked incrementally by the engine (sum of applied deltas). */
+bm_status bm_tracked_score(bm_ctx* ctx, int64_t* score);
+/* Per-vertex overlap S(v) = sum of min(w, w_B) over non-self A entries incident
+ * to v (each edge counts at both ends), host array of n+1 int32. */
+bm_status bm_get_overlap(bm_ctx* ctx, int32_t* ov);
+
+/* ------------------------------------------------------------ swap deltas */
+
+/* Exact deltas for k arbitrary pairs (u_i, v_i) = (pairs[2i], pairs[2i+1]).
+ * Host buffers.  Replaces calculate_swap_delta
+ * (src/graph-alignment-optimized.c:321-408) and the reference GPU kernels
+ * calculateSwapDeltasKernel(Quick) (src/graph-re-alignment-gpu.cu:46-248).
+ * u == v gives 0. */
+bm_status bm_delta_pairs(bm_ctx* ctx, const int32_t* pairs, int64_t k, int64_t* deltas);
+/* Same, device pointers, asynchronous on the context stream. */
+bm_status bm_delta_pairs_dev(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_deltas);
+
+/* Exact deltas of whole rows: for each row u = rows[r], delta(u, v) for
+ * v = 0..n is written to deltas[r*(n+1) + v] (v == 0 and v == u give 0).
+ * Host buffers.  This is the m2 sweep of one m1 row of optimize_mapping
+ * (src/graph-alignment-optimized.c:542-579) evaluated at once. */
+bm_status bm_delta_rows(bm_ctx* ctx, const int32_t* rows, int32_t nrows, int64_t* deltas);
+bm_status bm_delta_rows_dev(bm_ctx* ctx, const int32_t* d_rows, int32_t nrows, int64_t* d_deltas);
+
+/* Per-row reduction of whole-row deltas, without materialising them. */
+typedef struct bm_row_result {
+    int32_t row;         /* u */
+    int32_t first_pos;   /* smallest v >= col_lo, v != u, with delta > 0; 0 if none */
+    int32_t best;        /* v with the largest delta (smallest v on ties), v >= col_lo, v != u */
+    int32_t npos;        /* number of v >= col_lo with delta > 0 */
+    int64_t first_delta; /* delta(u, first_pos), 0 if none */
+    int64_t best_delta;  /* delta(u, best) */
+} bm_row_result;
+
+/* col_lo may be NULL (all columns); otherwise col_lo[r] is the first column
+ * considered for row r.  Host buffers. */
+bm_status bm_rows_best(bm_ctx* ctx, const int32_t* rows, const int32_t* col_lo,
+                       int32_t nrows, bm_row_result* out);
+bm_status bm_rows_best_dev(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo,
+                           int32_t nrows, bm_row_result* d_out);
+
+/* --------------------------------------------------------------- moves */
+
+/* Apply k swaps pi(a_i) <-> pi(b_i) that must be pairwise independent (no shared
+ * vertex and no A edge between the endpoint sets of two swaps; k == 1 is always
+ * independent), updating pi, the per-vertex overlap and the tracked score by
+ * the given deltas.  Host buffers.  Replaces the swap of optimize_mapping
+ * (src/graph-alignment-optimized.c:556-566). */
+bm_status bm_apply_swaps(bm_ctx* ctx, const int32_t* pairs, const int64_t* deltas, int32_t k);
+
+/* ------------------------------------------------------------- schedules */
+
+typedef struct bm_progress {
+    int64_t rows_done;       /* rows (m1 values) completed */
+    int64_t evaluated;       /* exact deltas evaluated (full rows count n-1) */
+    int64_t accepts;         /* swaps applied */
+    int64_t score;           /* tracked score at return */
+    int64_t launches;        /* kernel batches launched */
+    int32_t next_row_pos;    /* position in row_order to resume from */
+    int32_t next_col;        /* column to resume from in that row */
+    int32_t sweeps;          /* completed passes over row_order */
+    int32_t converged;       /* 1 if a full pass found no improving swap */
+    double seconds;          /* wall time spent */
+} bm_progress;
+
+/* Serial first-improvement hill-climb, bit-exact with the loop of
+ * optimize_mapping (src/graph-alignment-optimized.c:513-580): rows in
+ * row_order (NULL = 1..n), columns v = 1..n ascending, accept the first
+ * delta > 0 and continue from the next column under the new mapping.
+ * Stops at convergence (a full pass without an accept), after max_accepts
+ * accepts (<0: no limit), max_sweeps passes (<0: no limit) or time_budget_s
+ * seconds (<=0: no limit; BM_TIMEOUT is returned when it ran out).  `prog`
+ * may carry a resume position (next_row_pos, next_col) in; it is updated. */
+bm_status bm_sweep_parity(bm_ctx* ctx, const int32_t* row_order, int32_t nrows,
+                          int64_t max_accepts, int32_t max_sweeps, double time_budget_s,
+                          bm_progress* prog);
+
+/* Throughput search: batches of rows (row_order, cycled), best improving
+ * partner per row, then a deterministic conflict-free subset of those swaps
+ * (descending delta, ascending row) applied together.  Stops like
+ * bm_sweep_parity; target_score > 0 also stops once the score reaches it. */
+bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, int32_t nrows,
+                            int32_t rows_per_batch, int64_t max_accepts, int32_t max_sweeps,
+                            double time_budget_s, int64_t target_score, bm_progress* prog);
+
+/* ------------------------------------------------------- device utilities */
+
+/* Device memory, copies and events on the context stream, for callers that
+ * keep inputs resident (benchmarks, pipelines).  No PyTorch needed. */
+bm_status bm_dev_alloc(bm_ctx* ctx, int64_t bytes, void** d_ptr);
+bm_status bm_dev_free(bm_ctx* ctx, void* d_ptr);
+bm_status bm_memcpy_h2d(bm_ctx* ctx, void* d_dst, const void* h_src, int64_t bytes);
+bm_status bm_memcpy_d2h(bm_ctx* ctx, void* h_dst, const void* d_src, int64_t bytes);
+bm_status bm_host_alloc_pinned(int64_t bytes, void** h_ptr);
+bm_status bm_host_free_pinned(void* h_ptr);
+/* Write a device buffer larger than L2 so the next kernel starts cold. */
+bm_status bm_l2_flush(bm_ctx* ctx);
+bm_status bm_event_create(bm_ctx* ctx, void** ev);
+bm_status bm_event_destroy(bm_ctx* ctx, void* ev);
+bm_status bm_event_record(bm_ctx* ctx, void* ev);
+bm_status bm_event_elapsed_ms(bm_ctx* ctx, void* ev_start, void* ev_stop, float* ms);
+/* Kernel launches issued by this context since creation (all entry points). */
+int64_t bm_launch_count(const bm_ctx* ctx);
+
+/* Tuning knobs of the row kernel: CTAs per row (1, 2, 4 or 8: a thread-block
+ * cluster sharing the row through distributed shared memory) and threads per
+ * CTA (256 or 512).  0 keeps the current value. */
+bm_status bm_set_row_tiling(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads);
+bm_status bm_get_row_tiling(bm_ctx* ctx, int32_t* ctas_per_row, int32_t* threads);
+/* How many row clusters of the given shape can be resident at once on the
+ * device for the current n (cudaOccupancyMaxActiveClusters). */
+bm_status bm_rows_max_active_clusters(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads, int32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BM_CUDA_H */

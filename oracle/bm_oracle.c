@@ -1,0 +1,241 @@
+/*
+ * bm_oracle.c — CPU restatement of the reference's swap-search hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker the GPU kernels are
+ * compared against; it is loaded by tests/, by __graft_entry__.smoke() and by
+ * the CPU-baseline leg of bench.py, and by nothing else.  The engine
+ * (libbmcuda) never calls it and has no CPU fallback.
+ *
+ * Each function follows the named reference function line by line in
+ * behaviour (data layout differs: edge lists in insertion order as EdgeMap
+ * keeps them, and the dense int16 matrix replaced by a hash with the same
+ * last-write-wins rule):
+ *   orc_score       calculate_alignment_score  src/graph-alignment-optimized.c:292-307
+ *   orc_swap_delta  calculate_swap_delta       src/graph-alignment-optimized.c:321-408
+ *   orc_serial      optimize_mapping loop      src/graph-alignment-optimized.c:513-580
+ *                   (bounded: the reference loops forever)
+ *   orc_rows_omp    the OpenMP m2 sweep        src/graph-alignment-optimized-parallel.c:544
+ *                   (deltas only, no applies)
+ * Parity is pinned by tests/golden/ fixtures produced by the reference's own
+ * functions compiled from its sources (oracle/ref_harness.c).
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct {
+    int32_t n;
+    int64_t m;
+    int32_t* optr;  /* n+2: out-lists in insertion order (EdgeMap edges) */
+    int32_t* oto;
+    int32_t* ow;
+    int32_t* iptr;  /* n+2: in-lists (EdgeMap reverse_edges) */
+    int32_t* ifrom;
+    int32_t* iw;
+    /* matrix lookups: key (s,d) -> last weight */
+    uint64_t* hkey;
+    int32_t* hval;
+    uint64_t hmask;
+} orc_graph;
+
+static uint64_t orc_mix(uint64_t k) {
+    k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+    return k;
+}
+
+static int32_t mat(const orc_graph* g, int32_t s, int32_t d) {
+    uint64_t k = ((uint64_t)(uint32_t)s << 32) | (uint32_t)d;
+    uint64_t h = orc_mix(k) & g->hmask;
+    while (g->hkey[h] != ~0ull) {
+        if (g->hkey[h] == k) return g->hval[h];
+        h = (h + 1) & g->hmask;
+    }
+    return 0;
+}
+
+#define MIN(a, b) ((a) < (b) ? (a) : (b))
+
+void orc_graph_free(orc_graph* g) {
+    if (!g) return;
+    free(g->optr); free(g->oto); free(g->ow);
+    free(g->iptr); free(g->ifrom); free(g->iw);
+    free(g->hkey); free(g->hval);
+    free(g);
+}
+
+/* add_edge (src/graph-alignment-optimized.c:183-204): the edge goes to the
+ * end of from's out-list and to's in-list; the matrix keeps the last weight. */
+orc_graph* orc_graph_new(int32_t n, int64_t m, const int32_t* src, const int32_t* dst, const int32_t* w) {
+    orc_graph* g = (orc_graph*)calloc(1, sizeof(orc_graph));
+    if (!g) return NULL;
+    g->n = n;
+    g->m = m;
+    g->optr = (int32_t*)calloc((size_t)n + 2, sizeof(int32_t));
+    g->iptr = (int32_t*)calloc((size_t)n + 2, sizeof(int32_t));
+    g->oto = (int32_t*)malloc(sizeof(int32_t) * (size_t)(m + 1));
+    g->ow = (int32_t*)malloc(sizeof(int32_t) * (size_t)(m + 1));
+    g->ifrom = (int32_t*)malloc(sizeof(int32_t) * (size_t)(m + 1));
+    g->iw = (int32_t*)malloc(sizeof(int32_t) * (size_t)(m + 1));
+    uint64_t cap = 16;
+    while (cap < (uint64_t)(2 * m + 16)) cap <<= 1;
+    g->hkey = (uint64_t*)malloc(sizeof(uint64_t) * cap);
+    g->hval = (int32_t*)malloc(sizeof(int32_t) * cap);
+    if (!g->optr || !g->iptr || !g->oto || !g->ow || !g->ifrom || !g->iw || !g->hkey || !g->hval) {
+        orc_graph_free(g);
+        return NULL;
+    }
+    g->hmask = cap - 1;
+    memset(g->hkey, 0xff, sizeof(uint64_t) * cap);
+    for (int64_t e = 0; e < m; e++) { g->optr[src[e] + 1]++; g->iptr[dst[e] + 1]++; }
+    for (int32_t i = 1; i <= n + 1; i++) { g->optr[i] += g->optr[i - 1]; g->iptr[i] += g->iptr[i - 1]; }
+    int32_t* fo = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n + 1));
+    int32_t* fi = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n + 1));
+    memcpy(fo, g->optr, sizeof(int32_t) * ((size_t)n + 1));
+    memcpy(fi, g->iptr, sizeof(int32_t) * ((size_t)n + 1));
+    for (int64_t e = 0; e < m; e++) {
+        int32_t s = src[e], d = dst[e];
+        g->oto[fo[s]] = d; g->ow[fo[s]++] = w[e];
+        g->ifrom[fi[d]] = s; g->iw[fi[d]++] = w[e];
+        uint64_t k = ((uint64_t)(uint32_t)s << 32) | (uint32_t)d;
+        uint64_t h = orc_mix(k) & g->hmask;
+        while (g->hkey[h] != ~0ull && g->hkey[h] != k) h = (h + 1) & g->hmask;
+        g->hkey[h] = k;
+        g->hval[h] = (int32_t)(int16_t)w[e]; /* the matrix is short */
+    }
+    free(fo);
+    free(fi);
+    return g;
+}
+
+/* calculate_alignment_score, src/graph-alignment-optimized.c:292-307 */
+int64_t orc_score(const orc_graph* gm, const orc_graph* gf, const int32_t* mapping) {
+    int64_t score = 0;
+    for (int32_t s = 1; s <= gm->n; s++)
+        for (int32_t j = gm->optr[s]; j < gm->optr[s + 1]; j++) {
+            int32_t d = gm->oto[j];
+            score += MIN(gm->ow[j], mat(gf, mapping[s], mapping[d]));
+        }
+    return score;
+}
+
+/* calculate_swap_delta, src/graph-alignment-optimized.c:321-408 */
+int64_t orc_swap_delta(const orc_graph* gm, const orc_graph* gf, const int32_t* mapping, int32_t m1, int32_t m2) {
+    int32_t f1 = mapping[m1], f2 = mapping[m2];
+    int64_t delta = 0;
+    for (int32_t j = gm->optr[m1]; j < gm->optr[m1 + 1]; j++) {          /* out of m1 :327-340 */
+        int32_t d = gm->oto[j];
+        if (d == m2) continue;
+        int32_t w = gm->ow[j], df = mapping[d];
+        delta += MIN(w, mat(gf, f2, df)) - MIN(w, mat(gf, f1, df));
+    }
+    for (int32_t j = gm->iptr[m1]; j < gm->iptr[m1 + 1]; j++) {          /* into m1 :343-356 */
+        int32_t s = gm->ifrom[j];
+        if (s == m2) continue;
+        int32_t w = gm->iw[j], sf = mapping[s];
+        delta += MIN(w, mat(gf, sf, f2)) - MIN(w, mat(gf, sf, f1));
+    }
+    for (int32_t j = gm->optr[m2]; j < gm->optr[m2 + 1]; j++) {          /* out of m2 :359-372 */
+        int32_t d = gm->oto[j];
+        if (d == m1) continue;
+        int32_t w = gm->ow[j], df = mapping[d];
+        delta += MIN(w, mat(gf, f1, df)) - MIN(w, mat(gf, f2, df));
+    }
+    for (int32_t j = gm->iptr[m2]; j < gm->iptr[m2 + 1]; j++) {          /* into m2 :375-388 */
+        int32_t s = gm->ifrom[j];
+        if (s == m1) continue;
+        int32_t w = gm->iw[j], sf = mapping[s];
+        delta += MIN(w, mat(gf, sf, f1)) - MIN(w, mat(gf, sf, f2));
+    }
+    int32_t a = mat(gm, m1, m2);                                          /* m1 -> m2 :392-397 */
+    if (a > 0) delta += MIN(a, mat(gf, f2, f1)) - MIN(a, mat(gf, f1, f2));
+    int32_t b = mat(gm, m2, m1);                                          /* m2 -> m1 :400-405 */
+    if (b > 0) delta += MIN(b, mat(gf, f1, f2)) - MIN(b, mat(gf, f2, f1));
+    return delta;
+}
+
+/* Exact delta by re-scoring: score(pi with m1,m2 swapped) - score(pi).  The
+ * ground truth on graphs with self-loops, where calculate_swap_delta counts a
+ * self-loop twice against the old image. */
+int64_t orc_exact_delta(const orc_graph* gm, const orc_graph* gf, int32_t* mapping, int32_t m1, int32_t m2) {
+    int64_t before = orc_score(gm, gf, mapping);
+    int32_t t = mapping[m1]; mapping[m1] = mapping[m2]; mapping[m2] = t;
+    int64_t after = orc_score(gm, gf, mapping);
+    t = mapping[m1]; mapping[m1] = mapping[m2]; mapping[m2] = t;
+    return after - before;
+}
+
+/* Bounded serial first-improvement loop of optimize_mapping
+ * (src/graph-alignment-optimized.c:513-580): for m1 in rows, for m2 = 1..n,
+ * m2 != m1: accept the first delta > 0 and apply it at once.  Stops after a
+ * pass without accepts, after max_sweeps passes, or after max_accepts accepts.
+ * Accepted moves are logged (m1, m2, delta) up to log_cap entries.
+ * Returns the number of accepts; *score is updated by the deltas. */
+int64_t orc_serial(const orc_graph* gm, const orc_graph* gf, int32_t* mapping, const int32_t* rows, int32_t nrows,
+                   int64_t max_accepts, int32_t max_sweeps, int64_t* score, int32_t* log_m1, int32_t* log_m2,
+                   int64_t* log_delta, int64_t log_cap, int32_t* sweeps_done, int32_t* converged) {
+    int32_t n = gm->n;
+    int64_t accepts = 0;
+    int32_t sweeps = 0;
+    *converged = 0;
+    for (;;) {
+        int64_t pass_acc = 0;
+        for (int32_t r = 0; r < nrows; r++) {
+            int32_t m1 = rows ? rows[r] : r + 1;
+            for (int32_t m2 = 1; m2 <= n; m2++) {
+                if (m1 == m2) continue;
+                if (max_accepts >= 0 && accepts >= max_accepts) goto done;
+                int64_t delta = orc_swap_delta(gm, gf, mapping, m1, m2);
+                if (delta > 0) {
+                    int32_t f1 = mapping[m1], f2 = mapping[m2];
+                    mapping[m1] = f2;
+                    mapping[m2] = f1;
+                    *score += delta;
+                    if (accepts < log_cap) {
+                        log_m1[accepts] = m1;
+                        log_m2[accepts] = m2;
+                        log_delta[accepts] = delta;
+                    }
+                    accepts++;
+                    pass_acc++;
+                }
+            }
+        }
+        sweeps++;
+        if (pass_acc == 0) { *converged = 1; break; }
+        if (max_sweeps >= 0 && sweeps >= max_sweeps) break;
+    }
+done:
+    *sweeps_done = sweeps;
+    return accepts;
+}
+
+/* The OpenMP m2 sweep (src/graph-alignment-optimized-parallel.c:544) without
+ * applies: deltas of rows x all columns, out[r*(n+1)+m2]. */
+void orc_rows_omp(const orc_graph* gm, const orc_graph* gf, const int32_t* mapping, const int32_t* rows,
+                  int32_t nrows, int64_t* out, int32_t threads) {
+    int32_t n = gm->n;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+    for (int32_t r = 0; r < nrows; r++) {
+        int32_t m1 = rows[r];
+        int64_t* o = out + (size_t)r * ((size_t)n + 1);
+        o[0] = 0;
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int32_t m2 = 1; m2 <= n; m2++)
+            o[m2] = (m2 == m1) ? 0 : orc_swap_delta(gm, gf, mapping, m1, m2);
+    }
+}
+
+/* Deltas of arbitrary pairs. */
+void orc_pairs(const orc_graph* gm, const orc_graph* gf, const int32_t* mapping, const int32_t* pairs, int64_t k,
+               int64_t* out) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < k; i++) {
+        int32_t u = pairs[2 * i], v = pairs[2 * i + 1];
+        out[i] = (u == v) ? 0 : orc_swap_delta(gm, gf, mapping, u, v);
+    }
+}

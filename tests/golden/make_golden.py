@@ -1,0 +1,111 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own
+functions (calculate_alignment_score, calculate_swap_delta and the loop order
+of optimize_mapping), compiled from the reference sources into
+oracle/_ref/libref.so by oracle/Makefile.
+
+Run in a checkout where the reference sources are present:
+    make -C oracle && python tests/golden/make_golden.py
+
+Each fixture holds the graph pair itself (so it does not depend on the
+generator staying unchanged), the mappings, and the reference's outputs.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "brain-match_b200", "python"))
+sys.path.insert(0, os.path.join(REPO, "tests"))
+
+import bmb200 as bm  # noqa: E402
+from oracle_bind import Reference, ref_available  # noqa: E402
+
+
+def edges(g):
+    return g.src, g.dst, g.w
+
+
+def make_pair_case(name, config, seed, n, m, npairs, nrows, max_sweeps, log_cap, verify):
+    A, B, truth, init = bm.gen_pair(config, n=n, m_target=m, seed=seed)
+    ref = Reference(A.n, edges(A), edges(B))
+    rng = np.random.default_rng(seed)
+    pairs = rng.integers(1, A.n + 1, size=(npairs, 2)).astype(np.int32)
+    rows = rng.choice(np.arange(1, A.n + 1), size=nrows, replace=False).astype(np.int32)
+    out = {
+        "n": np.int64(A.n),
+        "a_src": A.src, "a_dst": A.dst, "a_w": A.w,
+        "b_src": B.src, "b_dst": B.dst, "b_w": B.w,
+        "pi_init": init, "pi_truth": truth,
+        "score_init": np.int64(ref.score(init)), "score_truth": np.int64(ref.score(truth)),
+        "pairs": pairs, "pair_deltas": ref.pairs(init, pairs),
+        "rows": rows, "row_deltas": ref.rows(init, rows),
+    }
+    pi_f, score_f, log, sweeps, conv = ref.serial(init, max_sweeps=max_sweeps, verify=verify)
+    out.update({
+        "serial_max_sweeps": np.int64(max_sweeps),
+        "serial_pi": pi_f, "serial_score": np.int64(score_f), "serial_accepts": np.int64(len(log)),
+        "serial_log": log[:log_cap], "serial_sweeps": np.int64(sweeps), "serial_converged": np.int64(conv),
+    })
+    # the first 100 accepts only, to pin the early order exactly
+    pi_k, score_k, log_k, _, _ = ref.serial(init, max_accepts=100, verify=verify)
+    out.update({"serial100_pi": pi_k, "serial100_score": np.int64(score_k)})
+    ref.close()
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, {k: (v if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items() if k in
+                 ("n", "score_init", "score_truth", "serial_score", "serial_accepts", "serial_sweeps",
+                  "serial_converged")})
+
+
+def make_selfloop_case(name, seed=17, n=40, m=400):
+    """A pair with self-loops, duplicate edges and zero weights.  The score is
+    well defined there; calculate_swap_delta is not exact (it counts a self-loop
+    twice against the old image), so the fixture records scores of mapping
+    pairs (pi, pi after one swap) and the reference's delta for comparison."""
+    rng = np.random.default_rng(seed)
+    s = rng.integers(1, n + 1, m).astype(np.int32)
+    d = rng.integers(1, n + 1, m).astype(np.int32)
+    w = rng.integers(0, 9, m).astype(np.int32)
+    seen, keep = set(), []
+    for i in range(m):  # at most one self-loop per A vertex
+        if s[i] == d[i]:
+            if s[i] in seen:
+                continue
+            seen.add(int(s[i]))
+        keep.append(i)
+    A = (s[keep], d[keep], w[keep])
+    B = (rng.integers(1, n + 1, m).astype(np.int32), rng.integers(1, n + 1, m).astype(np.int32),
+         rng.integers(0, 9, m).astype(np.int32))
+    ref = Reference(n, A, B)
+    pis, scores, swaps, swapped_scores, ref_deltas = [], [], [], [], []
+    for _ in range(8):
+        pi = np.concatenate([[0], rng.permutation(n) + 1]).astype(np.int32)
+        pis.append(pi)
+        scores.append(ref.score(pi))
+        u, v = rng.choice(np.arange(1, n + 1), 2, replace=False)
+        swaps.append((u, v))
+        q = pi.copy()
+        q[u], q[v] = q[v], q[u]
+        swapped_scores.append(ref.score(q))
+        ref_deltas.append(int(ref.pairs(pi, np.array([u, v], np.int32))[0]))
+    ref.close()
+    np.savez_compressed(os.path.join(HERE, name), n=np.int64(n), a_src=A[0], a_dst=A[1], a_w=A[2], b_src=B[0],
+                        b_dst=B[1], b_w=B[2], pis=np.array(pis), scores=np.array(scores, np.int64),
+                        swaps=np.array(swaps, np.int32), swapped_scores=np.array(swapped_scores, np.int64),
+                        ref_deltas=np.array(ref_deltas, np.int64))
+    print(name, "scores", scores[:3])
+
+
+def main():
+    if not ref_available():
+        raise SystemExit("oracle/_ref/libref.so missing: run make -C oracle where the reference sources exist")
+    make_pair_case("golden_small.npz", 1, 11, 300, 3000, 3000, 6, max_sweeps=-1, log_cap=1 << 16, verify=True)
+    make_pair_case("golden_cfg1.npz", 1, 1, 2000, 40000, 5000, 4, max_sweeps=1, log_cap=3000, verify=False)
+    make_selfloop_case("golden_selfloop.npz")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,75 @@
+"""The oracle (oracle/bm_oracle.c) pinned against the golden fixtures made by
+the reference's own functions, and against the compiled reference itself when
+it is present.  CPU only."""
+import numpy as np
+import pytest
+
+from conftest import golden_graphs
+from oracle_bind import Oracle, Reference, ref_available
+
+
+@pytest.mark.parametrize("case", ["golden_small", "golden_cfg1"])
+def test_oracle_score_and_deltas(case, request):
+    g = request.getfixturevalue(case)
+    n, A, B = golden_graphs(g)
+    orc = Oracle(n, A, B)
+    assert orc.score(g["pi_init"]) == int(g["score_init"])
+    assert orc.score(g["pi_truth"]) == int(g["score_truth"])
+    np.testing.assert_array_equal(orc.pairs(g["pi_init"], g["pairs"]), g["pair_deltas"])
+    np.testing.assert_array_equal(orc.rows(g["pi_init"], g["rows"]), g["row_deltas"])
+
+
+def test_oracle_serial_converges_like_reference(golden_small):
+    g = golden_small
+    n, A, B = golden_graphs(g)
+    orc = Oracle(n, A, B)
+    pi, score, log, sweeps, conv = orc.serial(g["pi_init"])
+    assert conv == int(g["serial_converged"]) == 1
+    assert sweeps == int(g["serial_sweeps"])
+    assert score == int(g["serial_score"])
+    np.testing.assert_array_equal(pi, g["serial_pi"])
+    np.testing.assert_array_equal(log, g["serial_log"])
+    assert orc.score(pi) == score
+
+
+def test_oracle_serial_first_sweep_cfg1(golden_cfg1):
+    g = golden_cfg1
+    n, A, B = golden_graphs(g)
+    orc = Oracle(n, A, B)
+    pi, score, log, sweeps, conv = orc.serial(g["pi_init"], max_sweeps=1)
+    assert len(log) == int(g["serial_accepts"])
+    np.testing.assert_array_equal(log[: len(g["serial_log"])], g["serial_log"])
+    np.testing.assert_array_equal(pi, g["serial_pi"])
+    assert score == int(g["serial_score"])
+    pi100, s100, _, _, _ = orc.serial(g["pi_init"], max_accepts=100)
+    np.testing.assert_array_equal(pi100, g["serial100_pi"])
+    assert s100 == int(g["serial100_score"])
+
+
+def test_oracle_selfloop_scores(golden_selfloop):
+    g = golden_selfloop
+    n, A, B = golden_graphs(g)
+    orc = Oracle(n, A, B)
+    for pi, s, (u, v), s2, rd in zip(g["pis"], g["scores"], g["swaps"], g["swapped_scores"], g["ref_deltas"]):
+        assert orc.score(pi) == s
+        assert orc.exact_delta(pi, u, v) == s2 - s
+        assert orc.delta(pi, u, v) == rd  # the reference's own (inexact here) delta, restated
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_oracle_matches_live_reference():
+    import bmb200 as bm
+    for seed in (21, 22):
+        Ag, Bg, truth, init = bm.gen_pair(1, n=500, m_target=6000, seed=seed)
+        A, B = (Ag.src, Ag.dst, Ag.w), (Bg.src, Bg.dst, Bg.w)
+        orc, ref = Oracle(Ag.n, A, B), Reference(Ag.n, A, B)
+        rng = np.random.default_rng(seed)
+        pairs = rng.integers(1, Ag.n + 1, size=(4000, 2)).astype(np.int32)
+        np.testing.assert_array_equal(orc.pairs(init, pairs), ref.pairs(init, pairs))
+        assert orc.score(truth) == ref.score(truth)
+        p1, s1, l1, _, _ = orc.serial(init, max_sweeps=1)
+        p2, s2, l2, _, _ = ref.serial(init, max_sweeps=1)
+        np.testing.assert_array_equal(p1, p2)
+        np.testing.assert_array_equal(l1, l2)
+        assert s1 == s2
+        ref.close()
