@@ -109,50 +109,50 @@ def algorithmic_bytes_per_row(A: bm.Graph, B: bm.Graph, pi: np.ndarray) -> np.nd
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clock and clock-event reasons of the engine's GPU, polled through NVML
+    every ~2 ms in a background thread while the timed region runs (read-only
+    queries; no GPU setting is changed)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, device: int):
-        self.path = tempfile.mktemp(suffix=".csv")
-        self.proc = None
+    def __init__(self, pci_bus_id: str):
+        import threading
+        self.samples, self.reasons, self.max_mhz = [], 0, 0.0
+        self.stop_ev = threading.Event()
+        self.thread = None
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(pci_bus_id.encode())
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nv = None
+            return
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                self.reasons |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+            except Exception:
+                pass
+            self.stop_ev.wait(0.002)
 
     def stop(self) -> dict | None:
-        if self.proc is None:
+        if self.thread is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.f.close()
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            p = [x.strip() for x in line.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx = max(mx, float(p[2]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, p[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        os.unlink(self.path)
-        if not sm:
+        self.stop_ev.set()
+        self.thread.join()
+        if not self.samples:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        names = sorted(k for k, bit in self.REASONS.items() if self.reasons & bit)
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples), "source": "NVML, 2 ms polling during the timed region"}
 
 
 def measured_peaks():
@@ -252,43 +252,43 @@ def run_ours(args, ws, rank, local, dist):
     score0 = eng.score()
     bytes_row = algorithmic_bytes_per_row(A, B, init)
 
-    d_rows = eng.dev_alloc(4 * R)
-    d_res = eng.dev_alloc(bm.ROW_DTYPE.itemsize * R)
-    ev0, ev1 = eng.event(), eng.event()
-    launches0 = eng.launch_count()
-
     starts = step_starts(n, args.warmup, 0.5) + step_starts(n, args.steps)
+    nsteps = args.warmup + args.steps
 
     def batch(step):
         idx = (starts[step] + rank * R + np.arange(R)) % n
         return np.ascontiguousarray(rows[idx])
 
+    # every batch's rows staged on the device before timing
+    all_rows = np.concatenate([batch(s) for s in range(nsteps)]).astype(np.int32)
+    d_rows = eng.dev_alloc(all_rows.nbytes)
+    eng.h2d(d_rows, all_rows)
+    d_res = eng.dev_alloc(bm.ROW_DTYPE.itemsize * R)
+    ev = [(eng.event(), eng.event()) for _ in range(nsteps)]
+
     def device_step(step):
-        b = batch(step)
-        eng.h2d(d_rows, b)
         eng.l2_flush()
-        eng.record(ev0)
-        eng.rows_best_dev(d_rows, None, R, d_res)
-        eng.record(ev1)
-        return eng.elapsed_ms(ev0, ev1), b
+        eng.record(ev[step][0])
+        eng.rows_best_dev(d_rows + 4 * R * step, None, R, d_res)
+        eng.record(ev[step][1])
 
     for s in range(args.warmup):
         device_step(s)
     eng.sync()
     barrier(dist)
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(eng.pci_bus_id())
     t_wall = time.perf_counter()
     launches_a = eng.launch_count()
-    total_ms, total_bytes = 0.0, 0
-    for s in range(args.warmup, args.warmup + args.steps):
-        ms, b = device_step(s)
-        total_ms += ms
-        total_bytes += int(bytes_row[b].sum())
+    for s in range(args.warmup, nsteps):
+        device_step(s)
     eng.sync()
-    launches_b = eng.launch_count()
     wall = time.perf_counter() - t_wall
+    launches_b = eng.launch_count()
     clk = clocks.stop()
     barrier(dist)
+    step_ms = [eng.elapsed_ms(*ev[s]) for s in range(args.warmup, nsteps)]
+    total_ms = float(sum(step_ms))
+    total_bytes = int(sum(int(bytes_row[batch(s)].sum()) for s in range(args.warmup, nsteps)))
 
     deltas_step = R * (n - 1)
     max_ms = dist_max(dist, total_ms)
@@ -358,8 +358,8 @@ def plain_search(eng, rows, seconds):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows-per-step", type=int, default=57)
     ap.add_argument("--ref-seconds", type=float, default=12.0)

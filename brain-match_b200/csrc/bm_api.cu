@@ -114,6 +114,12 @@ extern "C" bm_status bm_sync(bm_ctx* ctx) {
 
 extern "C" int64_t bm_launch_count(const bm_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+extern "C" bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len) {
+    if (!ctx || !buf || len < 13) return BM_INVALID_ARG;
+    BM_CUDA(ctx, cudaDeviceGetPCIBusId(buf, len, ctx->device));
+    return BM_OK;
+}
+
 bm_status bm_stage(bm_ctx* ctx, size_t bytes) {
     if (ctx->stage_bytes >= bytes) return BM_OK;
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -166,151 +172,48 @@ extern "C" bm_status bm_set_graph(bm_ctx* ctx, int side, int32_t n, int64_t m, c
                                   const int32_t* dst, const int32_t* w) {
     if (!ctx) return BM_INVALID_ARG;
     if (side != BM_SIDE_A && side != BM_SIDE_B) return bm_fail(ctx, BM_INVALID_ARG, "side must be 0 (A) or 1 (B)");
-    if (n < 1 || n > BM_MAX_N) return bm_fail(ctx, BM_INVALID_ARG, "n=%d outside 1..%d", n, BM_MAX_N);
-    if (m < 0 || m >= (int64_t)0x7fffffff) return bm_fail(ctx, BM_INVALID_ARG, "edge count %lld out of range", (long long)m);
-    if (m > 0 && (!src || !dst || !w)) return bm_fail(ctx, BM_INVALID_ARG, "null edge arrays");
     int other = 1 - side;
     if (ctx->g[other].loaded && ctx->g[other].n != n)
         return bm_fail(ctx, BM_INVALID_ARG, "n=%d differs from the other graph's n=%d", n, ctx->g[other].n);
-    for (int64_t e = 0; e < m; e++) {
-        if (src[e] < 1 || src[e] > n || dst[e] < 1 || dst[e] > n)
-            return bm_fail(ctx, BM_INVALID_ARG, "edge %lld: id outside 1..%d", (long long)e, n);
-        if (w[e] < 0 || w[e] > BM_MAX_W)
-            return bm_fail(ctx, BM_INVALID_ARG, "edge %lld: weight %d outside 0..%d", (long long)e, w[e], BM_MAX_W);
-    }
+    HostCsr H;
+    std::string err;
+    if (bm_build_host_csr(side == BM_SIDE_B, n, m, src, dst, w, H, err) != 0)
+        return bm_fail(ctx, BM_INVALID_ARG, "%s", err.c_str());
     BM_CUDA(ctx, cudaSetDevice(ctx->device));
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-
-    // Which entries survive: B keeps the last weight of a duplicated edge
-    // (the matrix store of add_edge); A keeps every entry.  Zero weights
-    // never contribute to min(w, .) and are dropped.
-    std::vector<int32_t> self((size_t)n + 1, 0);
-    std::vector<char> keep((size_t)m, 1);
-    int has_self = 0;
-    std::vector<unsigned long long> htab;
-    int hlog2 = 0;
-    if (side == BM_SIDE_B) {
-        int64_t cap = 1024;
-        hlog2 = 10;
-        while (cap * 3 < (m + 1) * 4) { cap <<= 1; hlog2++; }
-        // map key -> last edge index, in a temporary table
-        std::vector<unsigned long long> kk((size_t)cap, BM_HASH_EMPTY);
-        std::vector<int64_t> vi((size_t)cap, -1);
-        unsigned long long np1 = (unsigned long long)n + 1;
-        for (int64_t e = 0; e < m; e++) {
-            unsigned long long key = (unsigned long long)src[e] * np1 + (unsigned long long)dst[e];
-            unsigned long long s = bm_hash_slot0(key, hlog2);
-            while (kk[s] != BM_HASH_EMPTY && kk[s] != key) s = (s + 1) & (unsigned long long)(cap - 1);
-            if (kk[s] == key) keep[(size_t)vi[s]] = 0;
-            kk[s] = key;
-            vi[s] = e;
-        }
-        htab.assign((size_t)cap, BM_HASH_EMPTY);
-        for (int64_t e = 0; e < m; e++) {
-            if (!keep[e]) continue;
-            if (w[e] == 0) { keep[e] = 0; continue; }
-            if (src[e] == dst[e]) { self[src[e]] = w[e]; has_self = 1; keep[e] = 0; continue; }
-            unsigned long long key = (unsigned long long)src[e] * np1 + (unsigned long long)dst[e];
-            unsigned long long s = bm_hash_slot0(key, hlog2);
-            while (htab[s] != BM_HASH_EMPTY) s = (s + 1) & (unsigned long long)(cap - 1);
-            htab[s] = (key << 16) | (unsigned long long)w[e];
-        }
-    } else {
-        for (int64_t e = 0; e < m; e++) {
-            if (w[e] == 0) { keep[e] = 0; continue; }
-            if (src[e] == dst[e]) {
-                if (self[src[e]] != 0)
-                    return bm_fail(ctx, BM_INVALID_ARG, "vertex %d has more than one self-loop in graph A", src[e]);
-                self[src[e]] = w[e];
-                has_self = 1;
-                keep[e] = 0;
-            }
-        }
-    }
-
-    // CSR (out) sorted by (src, dst) and CSC (in) sorted by (dst, src), by
-    // two stable counting sorts each.
-    std::vector<int32_t> optr((size_t)n + 2, 0), iptr((size_t)n + 2, 0);
-    int64_t mk = 0;
-    for (int64_t e = 0; e < m; e++)
-        if (keep[e]) { optr[(size_t)src[e] + 1]++; iptr[(size_t)dst[e] + 1]++; mk++; }
-    for (int32_t i = 1; i <= n + 1; i++) { optr[i] += optr[i - 1]; iptr[i] += iptr[i - 1]; }
-    std::vector<int64_t> by_dst((size_t)mk), by_src((size_t)mk);
-    {
-        std::vector<int32_t> f(iptr.begin(), iptr.end() - 1);
-        for (int64_t e = 0; e < m; e++) if (keep[e]) by_dst[(size_t)f[dst[e]]++] = e;
-        std::vector<int32_t> g(optr.begin(), optr.end() - 1);
-        for (int64_t e = 0; e < m; e++) if (keep[e]) by_src[(size_t)g[src[e]]++] = e;
-    }
-    std::vector<uint32_t> oent((size_t)mk), ient((size_t)mk);
-    std::vector<int32_t> opos_of((size_t)(side == BM_SIDE_B ? m : 0));
-    std::vector<int32_t> ipos_of((size_t)(side == BM_SIDE_B ? m : 0));
-    {
-        // out: iterate edges in dst order, place by src (stable) -> rows sorted by dst
-        std::vector<int32_t> f(optr.begin(), optr.end() - 1);
-        for (int64_t k = 0; k < mk; k++) {
-            int64_t e = by_dst[(size_t)k];
-            int32_t p = f[src[e]]++;
-            oent[(size_t)p] = bm_pack((uint32_t)dst[e], (uint32_t)w[e]);
-            if (side == BM_SIDE_B) opos_of[(size_t)e] = p;
-        }
-        std::vector<int32_t> g(iptr.begin(), iptr.end() - 1);
-        for (int64_t k = 0; k < mk; k++) {
-            int64_t e = by_src[(size_t)k];
-            int32_t p = g[dst[e]]++;
-            ient[(size_t)p] = bm_pack((uint32_t)src[e], (uint32_t)w[e]);
-            if (side == BM_SIDE_B) ipos_of[(size_t)e] = p;
-        }
-    }
-    int32_t max_deg = 0;
-    int64_t max_wdeg = 0;
-    {
-        std::vector<int64_t> wd((size_t)n + 1, 0);
-        for (int64_t e = 0; e < m; e++)
-            if (keep[e]) { wd[src[e]] += w[e]; wd[dst[e]] += w[e]; }
-        for (int32_t v = 1; v <= n; v++) {
-            int32_t d = (optr[v + 1] - optr[v]) + (iptr[v + 1] - iptr[v]);
-            if (d > max_deg) max_deg = d;
-            if (wd[v] + self[v] > max_wdeg) max_wdeg = wd[v] + self[v];
-        }
-    }
-
-    if (side == BM_SIDE_A && max_wdeg >= ((int64_t)1 << 29))
-        return bm_fail(ctx, BM_INVALID_ARG, "weighted degree %lld of graph A is 2^29 or more", (long long)max_wdeg);
 
     // Replacing a graph drops the mapping state.
     ctx->mapped = false;
     free_graph(ctx->g[side]);
     DevGraph& G = ctx->g[side];
     G.n = n;
-    G.m = mk;
-    BM_TRY(upload(ctx, &G.out_ptr, optr.data(), optr.size()));
-    BM_TRY(upload(ctx, &G.in_ptr, iptr.data(), iptr.size()));
-    BM_TRY(upload(ctx, &G.out_ent, oent.data(), oent.size()));
-    BM_TRY(upload(ctx, &G.in_ent, ient.data(), ient.size()));
-    BM_TRY(upload(ctx, &G.self_w, self.data(), self.size()));
+    G.m_out = H.m_out();
+    G.m_in = H.m_in();
+    G.m_real = H.m_real;
+    BM_TRY(upload(ctx, &G.out_ptr, H.optr.data(), H.optr.size()));
+    BM_TRY(upload(ctx, &G.in_ptr, H.iptr.data(), H.iptr.size()));
+    BM_TRY(upload(ctx, &G.out_ent, H.oent.data(), H.oent.size()));
+    BM_TRY(upload(ctx, &G.in_ent, H.ient.data(), H.ient.size()));
+    BM_TRY(upload(ctx, &G.self_w, H.self.data(), H.self.size()));
     if (side == BM_SIDE_B) {
-        std::vector<int32_t> otw((size_t)mk), itw((size_t)mk);
-        for (int64_t e = 0; e < m; e++)
-            if (keep[e]) { otw[(size_t)opos_of[e]] = ipos_of[e]; itw[(size_t)ipos_of[e]] = opos_of[e]; }
-        BM_TRY(upload(ctx, &G.out_twin, otw.data(), otw.size()));
-        BM_TRY(upload(ctx, &G.in_twin, itw.data(), itw.size()));
-        BM_TRY(upload(ctx, &G.out_ent0, oent.data(), oent.size()));
-        BM_TRY(upload(ctx, &G.in_ent0, ient.data(), ient.size()));
-        BM_TRY(upload(ctx, &G.hash, htab.data(), htab.size()));
-        G.hash_log2 = hlog2;
+        BM_TRY(upload(ctx, &G.out_twin, H.otw.data(), H.otw.size()));
+        BM_TRY(upload(ctx, &G.in_twin, H.itw.data(), H.itw.size()));
+        BM_TRY(upload(ctx, &G.out_ent0, H.oent.data(), H.oent.size()));
+        BM_TRY(upload(ctx, &G.in_ent0, H.ient.data(), H.ient.size()));
+        BM_TRY(upload(ctx, &G.hash, H.htab.data(), H.htab.size()));
+        G.hash_log2 = H.hlog2;
+    } else {
+        ctx->hA_optr = H.optr;
+        ctx->hA_iptr = H.iptr;
+        ctx->hA_oent = H.oent;
+        ctx->hA_ient = H.ient;
     }
-    if (side == BM_SIDE_A) {
-        ctx->hA_optr = optr;
-        ctx->hA_iptr = iptr;
-        ctx->hA_oent = oent;
-        ctx->hA_ient = ient;
-    }
-    G.max_deg = max_deg;
-    G.max_wdeg = max_wdeg;
-    G.has_self = has_self;
+    G.max_deg = H.max_deg;
+    G.max_wdeg = H.max_wdeg;
+    G.has_self = H.has_self;
     G.loaded = true;
     ctx->n = n;
+    ctx->nvec = (n + 1 + 3) & ~3;
     return BM_OK;
 }
 
@@ -320,7 +223,7 @@ extern "C" bm_status bm_graph_info(bm_ctx* ctx, int side, int32_t* n, int64_t* m
     const DevGraph& G = ctx->g[side];
     if (!G.loaded) return bm_fail(ctx, BM_INVALID_ARG, "graph %d not set", side);
     if (n) *n = G.n;
-    if (m_nonself) *m_nonself = G.m;
+    if (m_nonself) *m_nonself = G.m_real;
     if (max_degree) *max_degree = G.max_deg;
     if (max_weighted_degree) *max_weighted_degree = G.max_wdeg;
     return BM_OK;
@@ -345,7 +248,7 @@ extern "C" bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* pi) {
     if (!ctx->pi) {
         BM_CUDA(ctx, cudaMalloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
         BM_CUDA(ctx, cudaMalloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
-        BM_CUDA(ctx, cudaMalloc(&ctx->ov, sizeof(int32_t) * ((size_t)n + 1)));
+        BM_CUDA(ctx, cudaMalloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
     } else {
         // sizes may have changed with a new graph
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -353,7 +256,7 @@ extern "C" bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* pi) {
         ctx->pi = ctx->pinv = ctx->ov = nullptr;
         BM_CUDA(ctx, cudaMalloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
         BM_CUDA(ctx, cudaMalloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
-        BM_CUDA(ctx, cudaMalloc(&ctx->ov, sizeof(int32_t) * ((size_t)n + 1)));
+        BM_CUDA(ctx, cudaMalloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
     }
     BM_CUDA(ctx, cudaMemcpyAsync(ctx->pi, h.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
     BM_CUDA(ctx, cudaMemcpyAsync(ctx->pinv, hinv.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));

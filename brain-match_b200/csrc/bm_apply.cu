@@ -38,6 +38,7 @@ __device__ __forceinline__ void relabel_twins(const int32_t* __restrict__ ptr, c
     const int32_t b = ptr[img], e = ptr[img + 1];
     for (int32_t j = b + threadIdx.x; j < e; j += kApplyThreads) {
         const int32_t t = twin[j];
+        if (t < 0) continue;  // list padding
         const uint32_t old = other_ent[t];
         other_ent[t] = (old & ~BM_ID_MASK) | new_id;
     }
@@ -56,6 +57,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(ApplyArgs a, const
             const int32_t b = a.A.out_ptr[me], e = a.A.out_ptr[me + 1];
             for (int32_t j = b + threadIdx.x; j < e; j += kApplyThreads) {
                 const uint32_t ent = a.A.out_ent[j];
+                if (ent == 0) continue;  // list padding
                 const int32_t x = bm_eid(ent), w = bm_ew(ent);
                 if (x == other) {
                     // edge me -> other: (fme, fnew) before, (fnew, fme) after
@@ -73,6 +75,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(ApplyArgs a, const
             const int32_t b = a.A.in_ptr[me], e = a.A.in_ptr[me + 1];
             for (int32_t j = b + threadIdx.x; j < e; j += kApplyThreads) {
                 const uint32_t ent = a.A.in_ent[j];
+                if (ent == 0) continue;
                 const int32_t x = bm_eid(ent), w = bm_ew(ent);
                 if (x == other) continue;
                 const int32_t gx = a.pi[x];

@@ -2,13 +2,15 @@
 //
 // HBM layout of one graph (ids 1..n, slot 0 unused):
 //   out_ptr[n+2], in_ptr[n+2]   int32 row offsets (CSR of out-lists, CSC of in-lists)
-//   out_ent[m], in_ent[m]       uint32 packed entries: neighbour id in bits 0..16,
-//                               weight in bits 17..31 (n <= 131071, w <= 32767)
+//   out_ent, in_ent             uint32 packed entries: neighbour id in bits 0..16,
+//                               weight in bits 17..31 (n <= 131071, w <= 32767);
+//                               each list padded to a multiple of 4 entries with
+//                               null entries (0), so every list is 16-byte aligned
 //   self_w[n+1]                 self-loop weight (0 if none); self-loops are kept
 //                               out of the lists and scored separately
 // Graph B additionally holds
-//   out_twin[m], in_twin[m]     index of the same edge in the other direction
-//   out_ent0[m], in_ent0[m]     the entries with B ids (immutable)
+//   out_twin, in_twin           index of the same edge in the other direction
+//   out_ent0, in_ent0           the entries with B ids (immutable)
 //   hash[2^k]                   open-addressing table (g*(n+1)+h) -> w of B edges
 // and its live out_ent/in_ent carry neighbour ids relabelled into A space
 // (id = pi^-1(B id)), so B'-out(x) = B-out(pi x) lists A vertices directly.
@@ -20,20 +22,13 @@
 #include <vector>
 
 #include "../../include/bm_cuda.h"
-
-#define BM_ID_BITS 17
-#define BM_ID_MASK ((1u << BM_ID_BITS) - 1u)
-#define BM_MAX_N ((int32_t)BM_ID_MASK)
-#define BM_MAX_W 32767
-#define BM_HASH_EMPTY 0xFFFFFFFFFFFFFFFFull
-
-__host__ __device__ __forceinline__ uint32_t bm_pack(uint32_t id, uint32_t w) { return id | (w << BM_ID_BITS); }
-__host__ __device__ __forceinline__ int32_t bm_eid(uint32_t e) { return (int32_t)(e & BM_ID_MASK); }
-__host__ __device__ __forceinline__ int32_t bm_ew(uint32_t e) { return (int32_t)(e >> BM_ID_BITS); }
+#include "bm_csr.hpp"
 
 struct DevGraph {
     int32_t n = 0;
-    int64_t m = 0;  // non-self list entries
+    int64_t m_out = 0;   // out-list slots, including the null entries padding each list to 4
+    int64_t m_in = 0;    // in-list slots
+    int64_t m_real = 0;  // non-self edges
     int32_t* out_ptr = nullptr;
     int32_t* in_ptr = nullptr;
     uint32_t* out_ent = nullptr;
@@ -75,6 +70,7 @@ struct bm_ctx {
     size_t smem_optin = 0;
     DevGraph g[2];
     int32_t n = 0;
+    int32_t nvec = 0;               // n+1 rounded up to a multiple of 4 (vectorised per-vertex arrays)
     // mapping state (device)
     int32_t* pi = nullptr;
     int32_t* pinv = nullptr;
@@ -125,22 +121,27 @@ inline HashView hview(const DevGraph& g) { return HashView{g.hash, g.hash_log2, 
 
 // ------------------------------------------------------------------ device
 
-__host__ __device__ __forceinline__ unsigned long long bm_hash_slot0(unsigned long long key, int log2) {
-    return (key * 0x9E3779B97F4A7C15ull) >> (64 - log2);
-}
-
-// Weight of B edge g->h (B ids), 0 if absent.  The table is at most 3/4 full,
-// so an empty slot ends every probe sequence; the loop is also bounded by the
-// table size.
+// Weight of B edge g->h (B ids), 0 if absent.  Linear probing read two slots
+// (16 bytes) at a time from the even slot at or below the home slot; in the
+// first pair a slot before the home slot is not part of the probe sequence.
+// The table is at most 3/4 full, so an empty slot ends every sequence; the
+// loop is also bounded by the table size.
 __device__ __forceinline__ int32_t bm_hash_get(const HashView& hv, int32_t g, int32_t h) {
-    unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;
-    unsigned long long mask = (1ull << hv.log2) - 1ull;
-    unsigned long long s = bm_hash_slot0(key, hv.log2);
-    for (unsigned long long it = 0; it <= mask; it++) {
-        unsigned long long v = __ldg(hv.tab + s);
-        if (v == BM_HASH_EMPTY) return 0;
-        if ((v >> 16) == key) return (int32_t)(v & 0xFFFFull);
-        s = (s + 1) & mask;
+    const unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;
+    const unsigned long long mask = (1ull << hv.log2) - 1ull;
+    const unsigned long long s0 = bm_hash_slot0(key, hv.log2);
+    unsigned long long base = s0 & ~1ull;
+    bool skip_first = (s0 & 1ull) != 0;
+    for (unsigned long long it = 0; it <= mask; it += 2) {
+        const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(hv.tab + base));
+        if (!skip_first) {
+            if (v.x == BM_HASH_EMPTY) return 0;
+            if ((v.x >> 16) == key) return (int32_t)(v.x & 0xFFFFull);
+        }
+        skip_first = false;
+        if (v.y == BM_HASH_EMPTY) return 0;
+        if ((v.y >> 16) == key) return (int32_t)(v.y & 0xFFFFull);
+        base = (base + 2) & mask;
     }
     return 0;
 }

@@ -37,6 +37,7 @@ __device__ __forceinline__ int64_t pair_delta_warp(const PairArgs& a, int32_t u,
         const int32_t b = __ldg(a.A.out_ptr + u), e = __ldg(a.A.out_ptr + u + 1);
         for (int32_t j = b + lane; j < e; j += 32) {
             const uint32_t ent = __ldg(a.A.out_ent + j);
+            if (ent == 0) continue;  // list padding
             const int32_t x = bm_eid(ent), w = bm_ew(ent);
             s += imin(w, bm_hash_get(a.hb, fv, __ldg(a.pi + x)));
             if (x == v) corr_w += imin(w, bm_hash_get(a.hb, fu, fv)) + imin(w, bm_hash_get(a.hb, fv, fu));
@@ -46,6 +47,7 @@ __device__ __forceinline__ int64_t pair_delta_warp(const PairArgs& a, int32_t u,
         const int32_t b = __ldg(a.A.in_ptr + u), e = __ldg(a.A.in_ptr + u + 1);
         for (int32_t j = b + lane; j < e; j += 32) {
             const uint32_t ent = __ldg(a.A.in_ent + j);
+            if (ent == 0) continue;
             const int32_t x = bm_eid(ent), w = bm_ew(ent);
             s += imin(w, bm_hash_get(a.hb, __ldg(a.pi + x), fv));
             if (x == v) corr_w += imin(w, bm_hash_get(a.hb, fu, fv)) + imin(w, bm_hash_get(a.hb, fv, fu));
@@ -55,6 +57,7 @@ __device__ __forceinline__ int64_t pair_delta_warp(const PairArgs& a, int32_t u,
         const int32_t b = __ldg(a.A.out_ptr + v), e = __ldg(a.A.out_ptr + v + 1);
         for (int32_t j = b + lane; j < e; j += 32) {
             const uint32_t ent = __ldg(a.A.out_ent + j);
+            if (ent == 0) continue;
             s += imin(bm_ew(ent), bm_hash_get(a.hb, fu, __ldg(a.pi + bm_eid(ent))));
         }
     }
@@ -62,6 +65,7 @@ __device__ __forceinline__ int64_t pair_delta_warp(const PairArgs& a, int32_t u,
         const int32_t b = __ldg(a.A.in_ptr + v), e = __ldg(a.A.in_ptr + v + 1);
         for (int32_t j = b + lane; j < e; j += 32) {
             const uint32_t ent = __ldg(a.A.in_ent + j);
+            if (ent == 0) continue;
             s += imin(bm_ew(ent), bm_hash_get(a.hb, __ldg(a.pi + bm_eid(ent)), fu));
         }
     }

@@ -12,6 +12,8 @@
 //   T3  (y, b) in B'-out(u):      for (v, w) in A-in(y):    acc[v] += min(w, b)
 //   T4  (y, b) in B'-in(u):       for (v, w) in A-out(y):   acc[v] += min(w, b)
 //   C   x in out_A(u) or in_A(u), weight a:  acc[x] += min(a, B(pi u, pi x)) + min(a, B(pi x, pi u))
+//       (through shared memory: B's row and column at pi u are written into
+//       the empty accumulator and read back, no per-entry lookups)
 //
 // where B'-out(x) = B-out(pi x) with neighbour ids relabelled into A space
 // (maintained by the apply kernel).  Then
@@ -40,6 +42,7 @@ namespace {
 constexpr int kItemChunk = 1024;  // first-hop items staged per pass
 constexpr int kSeg = 512;         // second-hop entries per work unit
 constexpr int kMaxCluster = 8;
+constexpr int kSideCap = 4096;    // A entries of u whose corrections go through shared memory
 
 struct RowArgs {
     const int32_t* Aout_ptr;
@@ -75,12 +78,14 @@ struct Partial {
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
+__host__ __device__ inline int32_t nvec_of(int32_t n) { return (n + 1 + 3) & ~3; }
+
 __host__ __device__ inline size_t rows_smem_bytes(int32_t n) {
-    return align16(sizeof(int32_t) * ((size_t)n + 1))  // acc
+    return align16(sizeof(int32_t) * (size_t)nvec_of(n))  // acc
            + sizeof(void*) * kItemChunk                  // item base
            + sizeof(int32_t) * kItemChunk * 2            // len, cap
            + sizeof(int32_t) * (kItemChunk + 4)          // unit prefix
-           + sizeof(int32_t) * 32                        // scan scratch
+           + sizeof(int32_t) * 32                        // scan scratch + unit counter
            + sizeof(Partial) * (kMaxCluster + 32);       // cluster partials + warp partials
 }
 
@@ -104,21 +109,26 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     const int32_t n = a.n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
+    const int32_t nv = nvec_of(n);
     int32_t* acc = (int32_t*)smem;
-    unsigned char* p = smem + align16(sizeof(int32_t) * ((size_t)n + 1));
+    unsigned char* p = smem + align16(sizeof(int32_t) * (size_t)nv);
     const uint32_t** it_base = (const uint32_t**)p;
     p += sizeof(void*) * kItemChunk;
     int32_t* it_len = (int32_t*)p;
     int32_t* it_cap = it_len + kItemChunk;
     int32_t* it_upre = it_cap + kItemChunk;
-    int32_t* scan_tmp = it_upre + kItemChunk + 4;
+    int32_t* scan_tmp = it_upre + kItemChunk + 4;  // [0..15] warp offsets, [31] unit counter
+    int* unit_ctr = scan_tmp + 31;
     Partial* parts = (Partial*)(scan_tmp + 32);  // [kMaxCluster] cluster partials
     Partial* wparts = parts + kMaxCluster;       // [32] warp partials
 
     const int32_t u = (r < a.nrows) ? __ldg(a.rows + r) : 0;
     const bool valid = (u >= 1 && u <= n);
 
-    for (int32_t i = tid; i <= n; i += THREADS) acc[i] = 0;
+    {
+        int4* acc4 = reinterpret_cast<int4*>(acc);
+        for (int32_t i = tid; i < (nv >> 2); i += THREADS) acc4[i] = make_int4(0, 0, 0, 0);
+    }
     __syncthreads();
 
     int32_t fu = 0;
@@ -129,50 +139,104 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
         const int32_t bo = __ldg(a.Bout_ptr + fu), d3 = __ldg(a.Bout_ptr + fu + 1) - bo;
         const int32_t bi = __ldg(a.Bin_ptr + fu), d4 = __ldg(a.Bin_ptr + fu + 1) - bi;
         const int32_t F = d1 + d2 + d3 + d4;
+        const int32_t dA = d1 + d2;
+        // ---- direct-edge corrections C, for A entries (x, w) of u:
+        //   acc[x] += min(w, B(pi u, pi x)) + min(w, B(pi x, pi u)).
+        // The B weights at pi u are written packed (out | in << 16) into the
+        // still-empty accumulator, read back for u's A entries into a side
+        // buffer (the item table's storage), cleared, then added.  Rows with
+        // more than kSideCap A entries use hash lookups, spread over the
+        // cluster's CTAs.
+        const bool side_path = dA <= kSideCap;
+        if (side_path && crank == 0) {
+            int32_t* side = reinterpret_cast<int32_t*>(it_base);
+            for (int32_t j = tid; j < d3; j += THREADS) {
+                const uint32_t e = __ldg(a.Bout_ent + bo + j);
+                if (e) atomicAdd(acc + bm_eid(e), bm_ew(e));
+            }
+            for (int32_t j = tid; j < d4; j += THREADS) {
+                const uint32_t e = __ldg(a.Bin_ent + bi + j);
+                if (e) atomicAdd(acc + bm_eid(e), bm_ew(e) << 16);
+            }
+            __syncthreads();
+            for (int32_t j = tid; j < dA; j += THREADS) {
+                const uint32_t e = (j < d1) ? __ldg(a.Aout_ent + ao + j) : __ldg(a.Ain_ent + ai + (j - d1));
+                int32_t c = 0;
+                if (e) {
+                    const uint32_t pq = (uint32_t)acc[bm_eid(e)];
+                    const int32_t w = bm_ew(e);
+                    c = imin(w, (int32_t)(pq & 0xFFFFu)) + imin(w, (int32_t)(pq >> 16));
+                }
+                side[j] = c;
+            }
+            __syncthreads();
+            for (int32_t j = tid; j < d3; j += THREADS) {
+                const uint32_t e = __ldg(a.Bout_ent + bo + j);
+                if (e) acc[bm_eid(e)] = 0;
+            }
+            for (int32_t j = tid; j < d4; j += THREADS) {
+                const uint32_t e = __ldg(a.Bin_ent + bi + j);
+                if (e) acc[bm_eid(e)] = 0;
+            }
+            __syncthreads();
+            for (int32_t j = tid; j < dA; j += THREADS) {
+                const int32_t c = side[j];
+                if (c) {
+                    const uint32_t e = (j < d1) ? __ldg(a.Aout_ent + ao + j) : __ldg(a.Ain_ent + ai + (j - d1));
+                    atomicAdd(acc + bm_eid(e), c);
+                }
+            }
+            __syncthreads();
+        }
         for (int32_t c0 = 0; c0 < F; c0 += kItemChunk) {
             const int32_t cnt = min(kItemChunk, F - c0);
-            // ---- build this thread's IPT consecutive items
+            // ---- build this thread's IPT consecutive items (null padding
+            // entries give empty items)
             int32_t tsum = 0;
 #pragma unroll
             for (int k = 0; k < IPT; k++) {
                 const int32_t li = tid * IPT + k;
                 const int32_t i = c0 + li;
                 if (li >= cnt) break;
-                const uint32_t* base;
-                int32_t len, cap;
+                const uint32_t* base = a.Aout_ent;
+                int32_t len = 0, cap = 0;
                 if (i < d1 + d2) {
                     const uint32_t ent = (i < d1) ? __ldg(a.Aout_ent + ao + i) : __ldg(a.Ain_ent + ai + (i - d1));
-                    const int32_t x = bm_eid(ent), w = bm_ew(ent);
-                    const int32_t g = __ldg(a.pi + x);
-                    if (i < d1) {
-                        const int32_t o = __ldg(a.Bin_ptr + g);
-                        base = a.Bin_ent + o;
-                        len = __ldg(a.Bin_ptr + g + 1) - o;
-                    } else {
-                        const int32_t o = __ldg(a.Bout_ptr + g);
-                        base = a.Bout_ent + o;
-                        len = __ldg(a.Bout_ptr + g + 1) - o;
-                    }
-                    cap = w;
-                    if (crank == 0) {
-                        const int32_t c = imin(w, bm_hash_get(a.hb, fu, g)) + imin(w, bm_hash_get(a.hb, g, fu));
-                        if (c) atomicAdd(acc + x, c);
+                    if (ent != 0) {
+                        const int32_t x = bm_eid(ent), w = bm_ew(ent);
+                        const int32_t g = __ldg(a.pi + x);
+                        if (i < d1) {
+                            const int32_t o = __ldg(a.Bin_ptr + g);
+                            base = a.Bin_ent + o;
+                            len = __ldg(a.Bin_ptr + g + 1) - o;
+                        } else {
+                            const int32_t o = __ldg(a.Bout_ptr + g);
+                            base = a.Bout_ent + o;
+                            len = __ldg(a.Bout_ptr + g + 1) - o;
+                        }
+                        cap = w;
+                        if (!side_path && (i % CL) == crank) {
+                            const int32_t c = imin(w, bm_hash_get(a.hb, fu, g)) + imin(w, bm_hash_get(a.hb, g, fu));
+                            if (c) atomicAdd(acc + x, c);
+                        }
                     }
                 } else {
                     const bool outb = i < d1 + d2 + d3;
                     const uint32_t ent = outb ? __ldg(a.Bout_ent + bo + (i - d1 - d2))
                                               : __ldg(a.Bin_ent + bi + (i - d1 - d2 - d3));
-                    const int32_t y = bm_eid(ent);
-                    if (outb) {
-                        const int32_t o = __ldg(a.Ain_ptr + y);
-                        base = a.Ain_ent + o;
-                        len = __ldg(a.Ain_ptr + y + 1) - o;
-                    } else {
-                        const int32_t o = __ldg(a.Aout_ptr + y);
-                        base = a.Aout_ent + o;
-                        len = __ldg(a.Aout_ptr + y + 1) - o;
+                    if (ent != 0) {
+                        const int32_t y = bm_eid(ent);
+                        if (outb) {
+                            const int32_t o = __ldg(a.Ain_ptr + y);
+                            base = a.Ain_ent + o;
+                            len = __ldg(a.Ain_ptr + y + 1) - o;
+                        } else {
+                            const int32_t o = __ldg(a.Aout_ptr + y);
+                            base = a.Aout_ent + o;
+                            len = __ldg(a.Aout_ptr + y + 1) - o;
+                        }
+                        cap = bm_ew(ent);
                     }
-                    cap = bm_ew(ent);
                 }
                 it_base[li] = base;
                 it_len[li] = len;
@@ -197,6 +261,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                     if (lane >= o) wi += t;
                 }
                 if (lane < NW) scan_tmp[lane] = wi - wv;  // exclusive warp offsets
+                if (lane == 0) *unit_ctr = 0;
             }
             __syncthreads();
             {
@@ -211,30 +276,38 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 if (tid * IPT < cnt && (tid + 1) * IPT >= cnt) it_upre[cnt] = run;
             }
             __syncthreads();
-            // ---- scatter: units k = crank, crank+CL, ... over this CTA's warps
+            // ---- scatter: this CTA owns units crank, crank+CL, ...; its warps
+            // take them one at a time from a shared counter.  A unit is at most
+            // kSeg entries of one list, read as 16-byte vectors (lists are
+            // padded to multiples of 4 entries and start 16-byte aligned).
             const int32_t U = it_upre[cnt];
-            for (int32_t k = crank + CL * warp; k < U; k += CL * NW) {
-                int32_t lo = 0, hi = cnt;  // last i with it_upre[i] <= k
+            for (;;) {
+                int32_t k = 0;
+                if (lane == 0) k = atomicAdd(unit_ctr, 1);
+                k = __shfl_sync(0xffffffffu, k, 0);
+                const int32_t unit = crank + CL * k;
+                if (unit >= U) break;
+                int32_t lo = 0, hi = cnt;  // last i with it_upre[i] <= unit
                 while (hi - lo > 1) {
                     const int32_t mid = (lo + hi) >> 1;
-                    if (it_upre[mid] <= k) lo = mid; else hi = mid;
+                    if (it_upre[mid] <= unit) lo = mid; else hi = mid;
                 }
-                const uint32_t* base = it_base[lo];
                 const int32_t cap = it_cap[lo];
-                const int32_t s = (k - it_upre[lo]) * kSeg;
-                const int32_t e = min(it_len[lo], s + kSeg);
-                int32_t j = s + lane;
-                for (; j + 96 < e; j += 128) {
-                    const uint32_t e0 = __ldg(base + j), e1 = __ldg(base + j + 32);
-                    const uint32_t e2 = __ldg(base + j + 64), e3 = __ldg(base + j + 96);
-                    atomicAdd(acc + bm_eid(e0), imin(cap, bm_ew(e0)));
-                    atomicAdd(acc + bm_eid(e1), imin(cap, bm_ew(e1)));
-                    atomicAdd(acc + bm_eid(e2), imin(cap, bm_ew(e2)));
-                    atomicAdd(acc + bm_eid(e3), imin(cap, bm_ew(e3)));
+                const int32_t s0 = (unit - it_upre[lo]) * kSeg;
+                const int32_t nq = (min(it_len[lo], s0 + kSeg) - s0) >> 2;
+                const uint4* b4 = reinterpret_cast<const uint4*>(it_base[lo] + s0);
+                uint4 q[kSeg / 128];
+#pragma unroll
+                for (int t = 0; t < kSeg / 128; t++) {
+                    const int qi = lane + 32 * t;
+                    q[t] = (qi < nq) ? __ldg(b4 + qi) : make_uint4(0u, 0u, 0u, 0u);
                 }
-                for (; j < e; j += 32) {
-                    const uint32_t e0 = __ldg(base + j);
-                    atomicAdd(acc + bm_eid(e0), imin(cap, bm_ew(e0)));
+#pragma unroll
+                for (int t = 0; t < kSeg / 128; t++) {
+                    const uint32_t e4[4] = {q[t].x, q[t].y, q[t].z, q[t].w};
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        if (e4[c] != 0) atomicAdd(acc + bm_eid(e4[c]), imin(cap, bm_ew(e4[c])));
                 }
             }
             __syncthreads();
@@ -242,10 +315,11 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     }
     cluster.sync();
 
-    // ---- finalise this CTA's slice of v
-    const int32_t slice = (n + CL - 1) / CL;
-    const int32_t vlo = 1 + crank * slice;
-    const int32_t vhi = min(n + 1, vlo + slice);
+    // ---- finalise this CTA's slice of v, four consecutive v per thread
+    const int32_t groups = nv >> 2;
+    const int32_t gslice = (groups + CL - 1) / CL;
+    const int32_t glo = crank * gslice;
+    const int32_t ghi = min(groups, glo + gslice);
     const int32_t collo = (valid && a.col_lo) ? __ldg(a.col_lo + r) : 1;
     int32_t first_v = INT_MAX, best_v = INT_MAX, npos = 0;
     long long first_d = 0, best_d = LLONG_MIN;
@@ -253,29 +327,37 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     int32_t sAu = 0, sBu = 0;
     if (valid && a.has_self) { sAu = __ldg(a.selfA + u); sBu = __ldg(a.selfB + fu); }
     int64_t* frow = a.full ? a.full + (size_t)r * ((size_t)n + 1) : nullptr;
-    if (frow && crank == 0 && tid == 0) frow[0] = 0;
-    for (int32_t v = vlo + tid; v < vhi; v += THREADS) {
-        long long d = 0;
-        if (valid && v != u) {
-            long long s = acc[v];
-            for (int q = 1; q < CL; q++) {
-                const int rr = (crank + q) % CL;
-                s += *cluster.map_shared_rank(acc + v, rr);
-            }
-            d = s - ovu - (long long)__ldg(a.ov + v);
-            if (a.has_self) {
-                const int32_t sAv = __ldg(a.selfA + v), sBv = __ldg(a.selfB + __ldg(a.pi + v));
-                d += imin(sAu, sBv) - imin(sAu, sBu) + imin(sAv, sBu) - imin(sAv, sBv);
-            }
-            if (v >= collo) {
-                if (d > 0) {
-                    npos++;
-                    if (v < first_v) { first_v = v; first_d = d; }
-                }
-                better_best(best_v, best_d, v, d);
-            }
+    const int4* ov4 = reinterpret_cast<const int4*>(a.ov);
+    for (int32_t gi = glo + tid; gi < ghi; gi += THREADS) {
+        int4 s4 = reinterpret_cast<const int4*>(acc)[gi];
+        for (int q = 1; q < CL; q++) {
+            const int4 t4 = *reinterpret_cast<const int4*>(cluster.map_shared_rank(acc + 4 * gi, (crank + q) % CL));
+            s4.x += t4.x; s4.y += t4.y; s4.z += t4.z; s4.w += t4.w;
         }
-        if (frow) frow[v] = d;
+        const int4 o4 = __ldg(ov4 + gi);
+        const int32_t sv[4] = {s4.x, s4.y, s4.z, s4.w};
+        const int32_t ovv[4] = {o4.x, o4.y, o4.z, o4.w};
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int32_t v = 4 * gi + c;
+            if (v > n) break;
+            long long d = 0;
+            if (valid && v != u && v >= 1) {
+                d = (long long)sv[c] - ovu - (long long)ovv[c];
+                if (a.has_self) {
+                    const int32_t sAv = __ldg(a.selfA + v), sBv = __ldg(a.selfB + __ldg(a.pi + v));
+                    d += imin(sAu, sBv) - imin(sAu, sBu) + imin(sAv, sBu) - imin(sAv, sBv);
+                }
+                if (v >= collo) {
+                    if (d > 0) {
+                        npos++;
+                        if (v < first_v) { first_v = v; first_d = d; }
+                    }
+                    better_best(best_v, best_d, v, d);
+                }
+            }
+            if (frow) frow[v] = d;
+        }
     }
     if (a.res) {
         // warp, then block reduction
@@ -408,7 +490,7 @@ bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_co
     args.res = d_res;
     int cl = ctx->row_ctas;
     if (cl == 0) {
-        // fill about two CTAs per SM: the largest cluster size with nrows*cl <= 2*SMs
+        // two CTAs fit per SM: the largest cluster size with nrows*cl <= 2*SMs
         cl = 1;
         while (cl < kMaxCluster && (int64_t)nrows * cl * 2 <= (int64_t)ctx->num_sms * 2) cl *= 2;
     }

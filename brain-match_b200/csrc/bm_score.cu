@@ -26,6 +26,7 @@ score_kernel(GView A, HashView hb, const int32_t* __restrict__ selfB, const int3
         int32_t s = 0;
         for (int32_t j = b + lane; j < e; j += 32) {
             const uint32_t ent = __ldg(A.out_ent + j);
+            if (ent == 0) continue;  // list padding
             const int32_t x = bm_eid(ent);
             const int32_t c = imin(bm_ew(ent), bm_hash_get(hb, fu, __ldg(pi + x)));
             if (c) atomicAdd(ov + x, c);
@@ -59,7 +60,7 @@ __global__ void relabel_kernel(const uint32_t* __restrict__ ent0, uint32_t* __re
 
 bm_status bm_launch_score(bm_ctx* ctx, int64_t* score_out) {
     const int32_t n = ctx->n;
-    BM_CUDA(ctx, cudaMemsetAsync(ctx->ov, 0, sizeof(int32_t) * ((size_t)n + 1), ctx->stream));
+    BM_CUDA(ctx, cudaMemsetAsync(ctx->ov, 0, sizeof(int32_t) * (size_t)ctx->nvec, ctx->stream));
     BM_CUDA(ctx, cudaMemsetAsync(ctx->d_score, 0, sizeof(unsigned long long), ctx->stream));
     int blocks = ctx->num_sms * 8;
     int need = (n + (kScoreThreads / 32) - 1) / (kScoreThreads / 32);
@@ -76,11 +77,14 @@ bm_status bm_launch_score(bm_ctx* ctx, int64_t* score_out) {
 
 bm_status bm_launch_relabel(bm_ctx* ctx) {
     const DevGraph& B = ctx->g[1];
-    if (B.m == 0) return BM_OK;
     int blocks = ctx->num_sms * 4;
-    relabel_kernel<<<blocks, 256, 0, ctx->stream>>>(B.out_ent0, B.out_ent, ctx->pinv, B.m);
-    BM_LAUNCH_CHECK(ctx, "relabel_kernel(out)");
-    relabel_kernel<<<blocks, 256, 0, ctx->stream>>>(B.in_ent0, B.in_ent, ctx->pinv, B.m);
-    BM_LAUNCH_CHECK(ctx, "relabel_kernel(in)");
+    if (B.m_out > 0) {
+        relabel_kernel<<<blocks, 256, 0, ctx->stream>>>(B.out_ent0, B.out_ent, ctx->pinv, B.m_out);
+        BM_LAUNCH_CHECK(ctx, "relabel_kernel(out)");
+    }
+    if (B.m_in > 0) {
+        relabel_kernel<<<blocks, 256, 0, ctx->stream>>>(B.in_ent0, B.in_ent, ctx->pinv, B.m_in);
+        BM_LAUNCH_CHECK(ctx, "relabel_kernel(in)");
+    }
     return BM_OK;
 }

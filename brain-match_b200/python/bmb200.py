@@ -118,6 +118,8 @@ def cuda_lib() -> C.CDLL:
             "bm_event_record": (C.c_int, [vp, vp]),
             "bm_event_elapsed_ms": (C.c_int, [vp, vp, vp, C.POINTER(C.c_float)]),
             "bm_launch_count": (C.c_int64, [vp]),
+            "bm_device_pci_bus_id": (C.c_int, [vp, C.c_char_p, C.c_int32]),
+            "bm_rows_max_active_clusters": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
             "bm_set_row_tiling": (C.c_int, [vp, C.c_int32, C.c_int32]),
             "bm_get_row_tiling": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         }
@@ -426,6 +428,17 @@ class Engine:
 
     def launch_count(self) -> int:
         return int(self.L.bm_launch_count(self.h))
+
+    def pci_bus_id(self) -> str:
+        buf = C.create_string_buffer(64)
+        self._chk(self.L.bm_device_pci_bus_id(self.h, buf, 64), "bm_device_pci_bus_id")
+        return buf.value.decode()
+
+    def max_active_clusters(self, ctas_per_row: int, threads: int) -> int:
+        v = C.c_int32()
+        self._chk(self.L.bm_rows_max_active_clusters(self.h, ctas_per_row, threads, C.byref(v)),
+                  "bm_rows_max_active_clusters")
+        return v.value
 
     # device utilities
     def dev_alloc(self, nbytes: int) -> int:

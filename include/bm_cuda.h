@@ -196,6 +196,8 @@ bm_status bm_event_record(bm_ctx* ctx, void* ev);
 bm_status bm_event_elapsed_ms(bm_ctx* ctx, void* ev_start, void* ev_stop, float* ms);
 /* Kernel launches issued by this context since creation (all entry points). */
 int64_t bm_launch_count(const bm_ctx* ctx);
+/* PCI bus id of the context's device ("0000:1b:00.0"), for NVML queries. */
+bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len);
 
 /* Tuning knobs of the row kernel: CTAs per row (1, 2, 4 or 8: a thread-block
  * cluster sharing the row through distributed shared memory) and threads per
