@@ -43,6 +43,7 @@ constexpr int kItemChunk = 1024;  // first-hop items staged per pass
 constexpr int kSeg = 512;         // second-hop entries per work unit
 constexpr int kMaxCluster = 8;
 constexpr int kSideCap = 4096;    // A entries of u whose corrections go through shared memory
+constexpr int kMaxUnits = 4096;   // units per chunk with a unit -> item table (else binary search)
 
 struct RowArgs {
     const int32_t* Aout_ptr;
@@ -85,6 +86,7 @@ __host__ __device__ inline size_t rows_smem_bytes(int32_t n) {
            + sizeof(void*) * kItemChunk                  // item base
            + sizeof(int32_t) * kItemChunk * 2            // len, cap
            + sizeof(int32_t) * (kItemChunk + 4)          // unit prefix
+           + sizeof(int16_t) * kMaxUnits                 // unit -> item
            + sizeof(int32_t) * 32                        // scan scratch + unit counter
            + sizeof(Partial) * (kMaxCluster + 32);       // cluster partials + warp partials
 }
@@ -117,7 +119,8 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     int32_t* it_len = (int32_t*)p;
     int32_t* it_cap = it_len + kItemChunk;
     int32_t* it_upre = it_cap + kItemChunk;
-    int32_t* scan_tmp = it_upre + kItemChunk + 4;  // [0..15] warp offsets, [31] unit counter
+    int16_t* unit_item = reinterpret_cast<int16_t*>(it_upre + kItemChunk + 4);
+    int32_t* scan_tmp = reinterpret_cast<int32_t*>(unit_item + kMaxUnits);  // [0..15] warp offsets, [31] unit counter
     int* unit_ctr = scan_tmp + 31;
     Partial* parts = (Partial*)(scan_tmp + 32);  // [kMaxCluster] cluster partials
     Partial* wparts = parts + kMaxCluster;       // [32] warp partials
@@ -276,39 +279,70 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 if (tid * IPT < cnt && (tid + 1) * IPT >= cnt) it_upre[cnt] = run;
             }
             __syncthreads();
+            // ---- unit -> item table (one shared load per unit instead of a
+            // binary search), when the chunk's units fit
+            const int32_t U = it_upre[cnt];
+            const bool table = U <= kMaxUnits;
+            if (table) {
+#pragma unroll
+                for (int k = 0; k < IPT; k++) {
+                    const int32_t li = tid * IPT + k;
+                    if (li >= cnt) break;
+                    for (int32_t x = it_upre[li]; x < it_upre[li + 1]; x++) unit_item[x] = (int16_t)li;
+                }
+                __syncthreads();
+            }
             // ---- scatter: this CTA owns units crank, crank+CL, ...; its warps
             // take them one at a time from a shared counter.  A unit is at most
             // kSeg entries of one list, read as 16-byte vectors (lists are
-            // padded to multiples of 4 entries and start 16-byte aligned).
-            const int32_t U = it_upre[cnt];
-            for (;;) {
+            // padded to multiples of 4 entries and start 16-byte aligned).  The
+            // loop is software-pipelined: the next unit's loads are issued
+            // before the current unit's shared-memory atomics.
+            auto grab = [&]() -> int32_t {
                 int32_t k = 0;
                 if (lane == 0) k = atomicAdd(unit_ctr, 1);
-                k = __shfl_sync(0xffffffffu, k, 0);
-                const int32_t unit = crank + CL * k;
-                if (unit >= U) break;
-                int32_t lo = 0, hi = cnt;  // last i with it_upre[i] <= unit
-                while (hi - lo > 1) {
-                    const int32_t mid = (lo + hi) >> 1;
-                    if (it_upre[mid] <= unit) lo = mid; else hi = mid;
+                return crank + CL * __shfl_sync(0xffffffffu, k, 0);
+            };
+            auto load_unit = [&](int32_t unit, uint4 (&q)[kSeg / 128], int32_t& cap) {
+                int32_t it;
+                if (table) {
+                    it = unit_item[unit];
+                } else {
+                    int32_t lo = 0, hi = cnt;  // last i with it_upre[i] <= unit
+                    while (hi - lo > 1) {
+                        const int32_t mid = (lo + hi) >> 1;
+                        if (it_upre[mid] <= unit) lo = mid; else hi = mid;
+                    }
+                    it = lo;
                 }
-                const int32_t cap = it_cap[lo];
-                const int32_t s0 = (unit - it_upre[lo]) * kSeg;
-                const int32_t nq = (min(it_len[lo], s0 + kSeg) - s0) >> 2;
-                const uint4* b4 = reinterpret_cast<const uint4*>(it_base[lo] + s0);
-                uint4 q[kSeg / 128];
+                cap = it_cap[it];
+                const int32_t s0 = (unit - it_upre[it]) * kSeg;
+                const int32_t nq = (min(it_len[it], s0 + kSeg) - s0) >> 2;
+                const uint4* b4 = reinterpret_cast<const uint4*>(it_base[it] + s0);
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) {
                     const int qi = lane + 32 * t;
                     q[t] = (qi < nq) ? __ldg(b4 + qi) : make_uint4(0u, 0u, 0u, 0u);
                 }
+            };
+            uint4 qa[kSeg / 128], qb[kSeg / 128];
+            int32_t capa = 0, capb = 0;
+            int32_t ua = grab();
+            if (ua < U) load_unit(ua, qa, capa);
+            while (ua < U) {
+                const int32_t ub = grab();
+                if (ub < U) load_unit(ub, qb, capb);
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) {
-                    const uint32_t e4[4] = {q[t].x, q[t].y, q[t].z, q[t].w};
+                    const uint32_t e4[4] = {qa[t].x, qa[t].y, qa[t].z, qa[t].w};
 #pragma unroll
                     for (int c = 0; c < 4; c++)
-                        if (e4[c] != 0) atomicAdd(acc + bm_eid(e4[c]), imin(cap, bm_ew(e4[c])));
+                        if (e4[c] != 0) atomicAdd(acc + bm_eid(e4[c]), imin(capa, bm_ew(e4[c])));
                 }
+#pragma unroll
+                for (int t = 0; t < kSeg / 128; t++) qa[t] = qb[t];
+                capa = capb;
+                ua = ub;
             }
             __syncthreads();
         }
