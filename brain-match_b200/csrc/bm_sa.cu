@@ -1,0 +1,532 @@
+// bm_sa.cu — batched simulated-annealing chains over many graph pairs.
+//
+// Follows the annealing of src/best-swap/score-lookup.c:346-408: a proposal is
+// a random pair (nodeM1, nodeM2), accepted if delta >= 0 or u < exp(delta/T),
+// with the geometric schedule T_i = Tmax * exp(ln(Tmin/Tmax) * i / iters).
+// Differences, deliberate: the deltas are exact int64 (pair form of
+// bm_pairs.cu) instead of an int16 lookup table; the RNG is Philox4x32-10
+// keyed per chain with the step as counter (instead of xoshiro256** seeded
+// from time), and exp is the project's own bm_exp, so a chain replays bit for
+// bit on the CPU; every chain ends on its final mapping and score, like the
+// reference's return value (:407).
+//
+// One CTA runs one chain.  Its K warps evaluate the K proposals of steps
+// s..s+K-1 under the current mapping; the first accepted one in step order is
+// applied and the rest are discarded, so the chain is exactly the one-at-a-
+// time chain for every K (the step counter moves past the accepted proposal,
+// or by K when none is accepted).  K and the block size are the tuning knobs.
+// A launch advances every chain by at most `chunk` proposals; the launch is
+// captured once in a CUDA graph and replayed until all chains finish.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bm_internal.cuh"
+#include "bm_rng.hpp"
+
+namespace {
+
+struct PairDev {
+    int32_t n;
+    int32_t has_self;
+    const int32_t* Aout_ptr;
+    const int32_t* Ain_ptr;
+    const uint32_t* Aout_ent;
+    const uint32_t* Ain_ent;
+    const int32_t* selfA;
+    const int32_t* selfB;
+    HashView hb;
+};
+
+struct ChainDev {
+    int32_t pair;
+    int32_t status;
+    int32_t* pi;    // n+1
+    int32_t* ov;    // n+1, per-vertex overlap (scratch)
+    uint64_t key;
+    uint64_t step;  // next proposal index
+    long long score;
+    long long accepts;
+};
+
+struct SaArgs {
+    const PairDev* pairs;
+    ChainDev* chains;
+    int32_t nchains;
+    uint64_t steps;
+    uint64_t chunk;
+    double t0;
+    double log_ratio;
+};
+
+// Exact delta of swapping pi(u), pi(v) for one chain, computed by one warp
+// (the per-pair identity of bm_pairs.cu).
+// pi and ov are written by the same kernel (chain_apply_block), so they are
+// read with plain coherent loads, never through the read-only path.
+__device__ long long chain_delta_warp(const PairDev& P, const int32_t* pi, const int32_t* ov, int32_t u, int32_t v,
+                                      int lane) {
+    const int32_t fu = pi[u], fv = pi[v];
+    long long s = 0;
+    int32_t corr = 0;
+    for (int side = 0; side < 2; side++) {
+        const int32_t me = side ? v : u, other = side ? u : v;
+        const int32_t fnew = side ? fu : fv;
+        {
+            const int32_t b = __ldg(P.Aout_ptr + me), e = __ldg(P.Aout_ptr + me + 1);
+            for (int32_t j = b + lane; j < e; j += 32) {
+                const uint32_t ent = __ldg(P.Aout_ent + j);
+                if (ent == 0) continue;
+                const int32_t x = bm_eid(ent), w = bm_ew(ent);
+                s += imin(w, bm_hash_get(P.hb, fnew, pi[x]));
+                if (side == 0 && x == other) corr += imin(w, bm_hash_get(P.hb, fu, fv)) + imin(w, bm_hash_get(P.hb, fv, fu));
+            }
+        }
+        {
+            const int32_t b = __ldg(P.Ain_ptr + me), e = __ldg(P.Ain_ptr + me + 1);
+            for (int32_t j = b + lane; j < e; j += 32) {
+                const uint32_t ent = __ldg(P.Ain_ent + j);
+                if (ent == 0) continue;
+                const int32_t x = bm_eid(ent), w = bm_ew(ent);
+                s += imin(w, bm_hash_get(P.hb, pi[x], fnew));
+                if (side == 0 && x == other) corr += imin(w, bm_hash_get(P.hb, fu, fv)) + imin(w, bm_hash_get(P.hb, fv, fu));
+            }
+        }
+    }
+    s += corr;
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    s -= (long long)ov[u] + (long long)ov[v];
+    if (P.has_self) {
+        const int32_t su = __ldg(P.selfA + u), sv = __ldg(P.selfA + v);
+        const int32_t bu = __ldg(P.selfB + fu), bv = __ldg(P.selfB + fv);
+        s += imin(su, bv) - imin(su, bu) + imin(sv, bu) - imin(sv, bv);
+    }
+    return s;
+}
+
+// Apply the swap pi(a) <-> pi(b) of one chain with the whole CTA: S updates of
+// every A entry incident to a or b (as apply_kernel in bm_apply.cu), then pi.
+__device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* ov, int32_t sa, int32_t sb) {
+    const int32_t fa = pi[sa], fb = pi[sb];
+    for (int side = 0; side < 2; side++) {
+        const int32_t me = side ? sb : sa, other = side ? sa : sb;
+        const int32_t fme = side ? fb : fa, fnew = side ? fa : fb;
+        {
+            const int32_t b = __ldg(P.Aout_ptr + me), e = __ldg(P.Aout_ptr + me + 1);
+            for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+                const uint32_t ent = __ldg(P.Aout_ent + j);
+                if (ent == 0) continue;
+                const int32_t x = bm_eid(ent), w = bm_ew(ent);
+                if (x == other) {
+                    const int32_t d = imin(w, bm_hash_get(P.hb, fnew, fme)) - imin(w, bm_hash_get(P.hb, fme, fnew));
+                    if (d) { atomicAdd(ov + me, d); atomicAdd(ov + other, d); }
+                } else {
+                    const int32_t gx = pi[x];
+                    const int32_t d = imin(w, bm_hash_get(P.hb, fnew, gx)) - imin(w, bm_hash_get(P.hb, fme, gx));
+                    if (d) { atomicAdd(ov + me, d); atomicAdd(ov + x, d); }
+                }
+            }
+        }
+        {
+            const int32_t b = __ldg(P.Ain_ptr + me), e = __ldg(P.Ain_ptr + me + 1);
+            for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+                const uint32_t ent = __ldg(P.Ain_ent + j);
+                if (ent == 0) continue;
+                const int32_t x = bm_eid(ent), w = bm_ew(ent);
+                if (x == other) continue;
+                const int32_t gx = pi[x];
+                const int32_t d = imin(w, bm_hash_get(P.hb, gx, fnew)) - imin(w, bm_hash_get(P.hb, gx, fme));
+                if (d) { atomicAdd(ov + me, d); atomicAdd(ov + x, d); }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        pi[sa] = fb;
+        pi[sb] = fa;
+    }
+    __syncthreads();
+}
+
+__global__ void sa_chain_kernel(SaArgs a) {
+    const int c = blockIdx.x;
+    if (c >= a.nchains) return;
+    __shared__ long long s_delta[32];
+    __shared__ int s_acc[32];
+    __shared__ int s_u[32], s_v[32];
+    ChainDev& ch = a.chains[c];
+    const PairDev P = a.pairs[ch.pair];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, K = blockDim.x >> 5;
+    uint64_t step = ch.step;
+    const uint64_t end = min(a.steps, step + a.chunk);
+    long long score = ch.score, accepts = ch.accepts;
+    int32_t* pi = ch.pi;
+    int32_t* ov = ch.ov;
+    while (step < end) {
+        const uint64_t s = step + (uint64_t)warp;
+        int acc = 0;
+        long long d = 0;
+        int32_t pu = 0, pv = 0;
+        if (s < end) {
+            const bm_proposal pr = bm_sa_proposal(ch.key, s, P.n);
+            pu = pr.u;
+            pv = pr.v;
+            d = chain_delta_warp(P, pi, ov, pu, pv, lane);
+            acc = bm_sa_accept(d, pr.uni, bm_sa_temperature(a.t0, a.log_ratio, s, a.steps)) ? 1 : 0;
+        }
+        if (lane == 0) {
+            s_delta[warp] = d;
+            s_acc[warp] = acc;
+            s_u[warp] = pu;
+            s_v[warp] = pv;
+        }
+        __syncthreads();
+        int first = -1;
+        for (int w = 0; w < K; w++)
+            if (s_acc[w]) { first = w; break; }
+        if (first >= 0) {
+            chain_apply_block(P, pi, ov, s_u[first], s_v[first]);
+            score += s_delta[first];
+            accepts++;
+            step += (uint64_t)first + 1;
+        } else {
+            step = min(end, step + (uint64_t)K);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ch.step = step;
+        ch.score = score;
+        ch.accepts = accepts;
+    }
+}
+
+// Initial S(v) and score of every chain: a warp per (chain, A vertex).
+__global__ void sa_init_kernel(const PairDev* pairs, ChainDev* chains, int32_t nchains) {
+    const int c = blockIdx.y;
+    if (c >= nchains) return;
+    ChainDev& ch = chains[c];
+    const PairDev P = pairs[ch.pair];
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int32_t u = 1 + blockIdx.x * wpb + (threadIdx.x >> 5); u <= P.n; u += gridDim.x * wpb) {
+        const int32_t fu = ch.pi[u];
+        int32_t s = 0;
+        for (int32_t j = __ldg(P.Aout_ptr + u) + lane; j < __ldg(P.Aout_ptr + u + 1); j += 32) {
+            const uint32_t ent = __ldg(P.Aout_ent + j);
+            if (ent == 0) continue;
+            const int32_t x = bm_eid(ent);
+            const int32_t cc = imin(bm_ew(ent), bm_hash_get(P.hb, fu, ch.pi[x]));
+            if (cc) atomicAdd(ch.ov + x, cc);
+            s += cc;
+        }
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            if (s) atomicAdd(ch.ov + u, s);
+            const long long t = (long long)s + imin(__ldg(P.selfA + u), __ldg(P.selfB + fu));
+            if (t) atomicAdd(reinterpret_cast<unsigned long long*>(&ch.score), (unsigned long long)t);
+        }
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ batches
+
+struct bm_batch {
+    bm_ctx* ctx = nullptr;
+    int device = 0;  // kept so that destruction does not need the context
+    struct Pair {
+        int32_t n = 0;
+        int64_t m_real_a = 0;
+        int32_t* d[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // Aoptr, Aiptr, selfA, selfB
+        uint32_t* e[2] = {nullptr, nullptr};                                   // Aoent, Aient
+        unsigned long long* hash = nullptr;
+        int hlog2 = 0;
+        int has_self = 0;
+    };
+    std::vector<Pair> pairs;
+    PairDev* d_pairs = nullptr;
+    bool dirty = true;
+};
+
+static void free_pair(bm_batch::Pair& p) {
+    for (auto* x : p.d) cudaFree(x);
+    for (auto* x : p.e) cudaFree(x);
+    cudaFree(p.hash);
+    p = bm_batch::Pair();
+}
+
+extern "C" bm_status bm_batch_create(bm_ctx* ctx, bm_batch** out) {
+    if (!ctx || !out) return BM_INVALID_ARG;
+    *out = new (std::nothrow) bm_batch();
+    if (!*out) return BM_OOM;
+    (*out)->ctx = ctx;
+    (*out)->device = ctx->device;
+    return BM_OK;
+}
+
+extern "C" void bm_batch_destroy(bm_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
+    for (auto& p : b->pairs) free_pair(p);
+    cudaFree(b->d_pairs);
+    delete b;
+}
+
+template <typename T>
+static bm_status up(bm_ctx* ctx, T** d, const std::vector<T>& h) {
+    BM_CUDA(ctx, cudaMalloc((void**)d, sizeof(T) * (h.empty() ? 1 : h.size())));
+    if (!h.empty()) BM_CUDA(ctx, cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_add_pair(bm_batch* b, int32_t n, int64_t mA, const int32_t* srcA, const int32_t* dstA,
+                                       const int32_t* wA, int64_t mB, const int32_t* srcB, const int32_t* dstB,
+                                       const int32_t* wB, int32_t* pair_index) {
+    if (!b) return BM_INVALID_ARG;
+    bm_ctx* ctx = b->ctx;
+    HostCsr HA, HB;
+    std::string err;
+    if (bm_build_host_csr(false, n, mA, srcA, dstA, wA, HA, err) != 0) return bm_fail(ctx, BM_INVALID_ARG, "A: %s", err.c_str());
+    if (bm_build_host_csr(true, n, mB, srcB, dstB, wB, HB, err) != 0) return bm_fail(ctx, BM_INVALID_ARG, "B: %s", err.c_str());
+    if (n < 2) return bm_fail(ctx, BM_INVALID_ARG, "annealing needs n >= 2");
+    BM_CUDA(ctx, cudaSetDevice(ctx->device));
+    bm_batch::Pair p;
+    p.n = n;
+    p.m_real_a = HA.m_real;
+    bm_status s;
+    if ((s = up(ctx, &p.d[0], HA.optr)) != BM_OK || (s = up(ctx, &p.d[1], HA.iptr)) != BM_OK ||
+        (s = up(ctx, &p.d[2], HA.self)) != BM_OK || (s = up(ctx, &p.d[3], HB.self)) != BM_OK ||
+        (s = up(ctx, &p.e[0], HA.oent)) != BM_OK || (s = up(ctx, &p.e[1], HA.ient)) != BM_OK ||
+        (s = up(ctx, &p.hash, HB.htab)) != BM_OK) {
+        free_pair(p);
+        return s;
+    }
+    p.hlog2 = HB.hlog2;
+    p.has_self = HA.has_self && HB.has_self;
+    b->pairs.push_back(p);
+    b->dirty = true;
+    if (pair_index) *pair_index = (int32_t)b->pairs.size() - 1;
+    return BM_OK;
+}
+
+// ------------------------------------------------------------- autotuning
+
+namespace {
+
+struct Tuning {
+    int32_t candidates = 8;
+    int32_t threads_unused = 0;
+};
+
+std::string tune_cache_path() {
+    const char* p = getenv("BM_TUNE_CACHE");
+    if (p && *p) return p;
+    const char* h = getenv("HOME");
+    return std::string(h && *h ? h : "/tmp") + "/.bm_b200_tune.txt";
+}
+
+// One line per key: "<device name>|<total n>|<chains> <candidates>"
+bool tune_lookup(const std::string& key, int32_t* cand) {
+    FILE* f = fopen(tune_cache_path().c_str(), "r");
+    if (!f) return false;
+    char line[512];
+    bool found = false;
+    while (fgets(line, sizeof line, f)) {
+        char* sp = strrchr(line, ' ');
+        if (!sp) continue;
+        *sp = 0;
+        if (key == line) { *cand = atoi(sp + 1); found = true; }
+    }
+    fclose(f);
+    return found;
+}
+
+void tune_store(const std::string& key, int32_t cand) {
+    FILE* f = fopen(tune_cache_path().c_str(), "a");
+    if (!f) return;
+    fprintf(f, "%s %d\n", key.c_str(), cand);
+    fclose(f);
+}
+
+}  // namespace
+
+extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chain_pair, const uint64_t* chain_key,
+                               const int32_t* init_pi, const bm_sa_params* prm, int32_t* final_pi,
+                               int64_t* final_score, int64_t* accepts, bm_sa_stats* stats) {
+    if (!b || !prm || nchains < 1 || !chain_pair || !chain_key || !init_pi) return BM_INVALID_ARG;
+    bm_ctx* ctx = b->ctx;
+    if (prm->steps < 0 || !(prm->t0 > 0) || !(prm->t_end > 0))
+        return bm_fail(ctx, BM_INVALID_ARG, "need steps >= 0 and positive temperatures");
+    if (prm->candidates < 0 || prm->candidates > 16)
+        return bm_fail(ctx, BM_INVALID_ARG, "candidates must be 0 (tuned) or 1..16");
+    BM_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int32_t np = (int32_t)b->pairs.size();
+    // chain layout and validation
+    std::vector<int64_t> off((size_t)nchains + 1, 0);
+    for (int32_t c = 0; c < nchains; c++) {
+        if (chain_pair[c] < 0 || chain_pair[c] >= np) return bm_fail(ctx, BM_INVALID_ARG, "chain %d: bad pair", c);
+        const int32_t n = b->pairs[(size_t)chain_pair[c]].n;
+        off[(size_t)c + 1] = off[(size_t)c] + (int64_t)n + 1;
+    }
+    for (int32_t c = 0; c < nchains; c++) {
+        const int32_t n = b->pairs[(size_t)chain_pair[c]].n;
+        const int32_t* p = init_pi + off[(size_t)c];
+        std::vector<char> seen((size_t)n + 1, 0);
+        for (int32_t i = 1; i <= n; i++) {
+            const int32_t f = p[i];
+            if (f < 1 || f > n || seen[(size_t)f]) return bm_fail(ctx, BM_INVALID_ARG, "chain %d: pi is not a bijection", c);
+            seen[(size_t)f] = 1;
+        }
+    }
+    // pair table
+    if (b->dirty) {
+        std::vector<PairDev> hp((size_t)np);
+        for (int32_t i = 0; i < np; i++) {
+            const auto& p = b->pairs[(size_t)i];
+            hp[(size_t)i] = PairDev{p.n, p.has_self, p.d[0], p.d[1], p.e[0], p.e[1], p.d[2], p.d[3],
+                                    HashView{p.hash, p.hlog2, p.n + 1}};
+        }
+        cudaFree(b->d_pairs);
+        b->d_pairs = nullptr;
+        BM_CUDA(ctx, cudaMalloc(&b->d_pairs, sizeof(PairDev) * (size_t)np));
+        BM_CUDA(ctx, cudaMemcpy(b->d_pairs, hp.data(), sizeof(PairDev) * (size_t)np, cudaMemcpyHostToDevice));
+        b->dirty = false;
+    }
+    // per-chain state: mapping (input/output) and the per-vertex overlap (scratch)
+    const int64_t tot = off[(size_t)nchains];
+    int32_t* d_pi = nullptr;
+    int32_t* d_ov = nullptr;
+    ChainDev* d_ch = nullptr;
+    BM_CUDA(ctx, cudaMalloc(&d_pi, sizeof(int32_t) * (size_t)tot));
+    BM_CUDA(ctx, cudaMalloc(&d_ov, sizeof(int32_t) * (size_t)tot));
+    BM_CUDA(ctx, cudaMalloc(&d_ch, sizeof(ChainDev) * (size_t)nchains));
+    struct Guard {
+        void* p[3];
+        ~Guard() { for (void* x : p) cudaFree(x); }
+    } guard{{d_pi, d_ov, d_ch}};
+    BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
+    BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
+    std::vector<ChainDev> hc((size_t)nchains);
+    for (int32_t c = 0; c < nchains; c++) {
+        hc[(size_t)c] = ChainDev{chain_pair[c], 0, d_pi + off[(size_t)c], d_ov + off[(size_t)c], chain_key[c], 0ull, 0, 0};
+    }
+    BM_CUDA(ctx, cudaMemcpyAsync(d_ch, hc.data(), sizeof(ChainDev) * (size_t)nchains, cudaMemcpyHostToDevice, ctx->stream));
+    {
+        dim3 g(64, (unsigned)nchains);
+        sa_init_kernel<<<g, 256, 0, ctx->stream>>>(b->d_pairs, d_ch, nchains);
+        BM_LAUNCH_CHECK(ctx, "sa_init_kernel");
+    }
+    SaArgs args;
+    args.pairs = b->d_pairs;
+    args.chains = d_ch;
+    args.nchains = nchains;
+    args.steps = (uint64_t)prm->steps;
+    args.t0 = prm->t0;
+    args.log_ratio = log(prm->t_end / prm->t0);
+    args.chunk = prm->chunk > 0 ? (uint64_t)prm->chunk : (uint64_t)65536;
+    cudaFuncAttributes fa;
+    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel));
+    const int32_t kmax = std::max(1, std::min(16, fa.maxThreadsPerBlock / 32));
+    int32_t K = prm->candidates;
+    if (K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates %d above this build's limit %d", K, kmax);
+    if (K == 0) {
+        int64_t ntot = 0;
+        for (int32_t c = 0; c < nchains; c++) ntot += b->pairs[(size_t)chain_pair[c]].n;
+        cudaDeviceProp prop;
+        cudaGetDeviceProperties(&prop, ctx->device);
+        const std::string key = std::string(prop.name) + "|" + std::to_string(ntot) + "|" + std::to_string(nchains);
+        if (!tune_lookup(key, &K)) {
+            // time a short prefix of the real run for each K and keep the
+            // fastest; the chain does not depend on K, so the prefix is
+            // simply replayed by the real run below
+            float best_ms = 1e30f;
+            int32_t best_k = 8;
+            std::vector<ChainDev> snap = hc;
+            for (int32_t cand : {1, 2, 4, 8, 16}) {
+                if (cand > kmax) break;
+                BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
+                BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
+                BM_CUDA(ctx, cudaMemcpyAsync(d_ch, snap.data(), sizeof(ChainDev) * (size_t)nchains, cudaMemcpyHostToDevice, ctx->stream));
+                sa_init_kernel<<<dim3(64, (unsigned)nchains), 256, 0, ctx->stream>>>(b->d_pairs, d_ch, nchains);
+                BM_LAUNCH_CHECK(ctx, "sa_init_kernel");
+                SaArgs t = args;
+                t.chunk = std::min<uint64_t>(4096, args.steps > 0 ? args.steps : 1);
+                struct Events {
+                    cudaEvent_t a = nullptr, b = nullptr;
+                    ~Events() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+                } ev;
+                BM_CUDA(ctx, cudaEventCreate(&ev.a));
+                BM_CUDA(ctx, cudaEventCreate(&ev.b));
+                BM_CUDA(ctx, cudaEventRecord(ev.a, ctx->stream));
+                sa_chain_kernel<<<nchains, 32 * cand, 0, ctx->stream>>>(t);
+                BM_LAUNCH_CHECK(ctx, "sa_chain_kernel(tune)");
+                BM_CUDA(ctx, cudaEventRecord(ev.b, ctx->stream));
+                BM_CUDA(ctx, cudaEventSynchronize(ev.b));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ev.a, ev.b);
+                if (ms < best_ms) { best_ms = ms; best_k = cand; }
+            }
+            K = best_k;
+            tune_store(key, K);
+            // restart from the initial state
+            BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
+            BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
+            BM_CUDA(ctx, cudaMemcpyAsync(d_ch, snap.data(), sizeof(ChainDev) * (size_t)nchains, cudaMemcpyHostToDevice, ctx->stream));
+            sa_init_kernel<<<dim3(64, (unsigned)nchains), 256, 0, ctx->stream>>>(b->d_pairs, d_ch, nchains);
+            BM_LAUNCH_CHECK(ctx, "sa_init_kernel");
+        }
+    }
+    // capture one chunk launch in a graph and replay it
+    const uint64_t launches = args.steps == 0 ? 0 : (args.steps + args.chunk - 1) / args.chunk;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (launches > 0) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        BM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        sa_chain_kernel<<<nchains, 32 * K, 0, ctx->stream>>>(args);
+        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (ce != cudaSuccess) return bm_cuda_fail(ctx, ce, "cudaStreamEndCapture");
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        if (ce != cudaSuccess) { cudaGraphDestroy(graph); return bm_cuda_fail(ctx, ce, "cudaGraphInstantiate"); }
+        for (uint64_t l = 0; l < launches; l++) {
+            ce = cudaGraphLaunch(exec, ctx->stream);
+            if (ce != cudaSuccess) break;
+            ctx->launches++;
+        }
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return bm_cuda_fail(ctx, ce, "cudaGraphLaunch");
+    }
+    BM_CUDA(ctx, cudaMemcpyAsync(hc.data(), d_ch, sizeof(ChainDev) * (size_t)nchains, cudaMemcpyDeviceToHost, ctx->stream));
+    if (final_pi)
+        BM_CUDA(ctx, cudaMemcpyAsync(final_pi, d_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int32_t c = 0; c < nchains; c++) {
+        if (final_score) final_score[c] = hc[(size_t)c].score;
+        if (accepts) accepts[c] = hc[(size_t)c].accepts;
+    }
+    if (stats) {
+        stats->candidates = K;
+        stats->launches = (int64_t)launches;
+        stats->seconds = secs;
+    }
+    return BM_OK;
+}
+
+extern "C" int64_t bm_sa_layout_size(bm_batch* b, int32_t nchains, const int32_t* chain_pair) {
+    if (!b || !chain_pair || nchains < 0) return -1;
+    int64_t tot = 0;
+    for (int32_t c = 0; c < nchains; c++) {
+        if (chain_pair[c] < 0 || chain_pair[c] >= (int32_t)b->pairs.size()) return -1;
+        tot += b->pairs[(size_t)chain_pair[c]].n + 1;
+    }
+    return tot;
+}

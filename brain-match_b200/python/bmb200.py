@@ -56,6 +56,15 @@ class Progress(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SaParams(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("t0", C.c_double), ("t_end", C.c_double), ("candidates", C.c_int32),
+                ("chunk", C.c_int64)]
+
+
+class SaStats(C.Structure):
+    _fields_ = [("candidates", C.c_int32), ("launches", C.c_int64), ("seconds", C.c_double)]
+
+
 class GenParams(C.Structure):
     _fields_ = [("n", C.c_int32), ("m_target", C.c_int64), ("degree_model", C.c_int32), ("alpha", C.c_double),
                 ("max_degree", C.c_int32), ("weight_model", C.c_int32), ("geo_p", C.c_double),
@@ -121,6 +130,12 @@ def cuda_lib() -> C.CDLL:
             "bm_device_pci_bus_id": (C.c_int, [vp, C.c_char_p, C.c_int32]),
             "bm_rows_max_active_clusters": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
             "bm_set_row_tiling": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "bm_batch_create": (C.c_int, [vp, C.POINTER(vp)]),
+            "bm_batch_destroy": (None, [vp]),
+            "bm_batch_add_pair": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, vp, C.c_int64, vp, vp, vp,
+                                            C.POINTER(C.c_int32)]),
+            "bm_sa_run": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.POINTER(SaParams), vp, vp, vp, C.POINTER(SaStats)]),
+            "bm_sa_layout_size": (C.c_int64, [vp, C.c_int32, vp]),
             "bm_get_row_tiling": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         }
         for name, (res, args) in sig.items():
@@ -315,6 +330,7 @@ class Engine:
             raise BMError(st, f"bm_ctx_create({device})")
         self.h = h
         self.n = 0
+        self._children = []  # weak references to batches, closed before the context
 
     def _chk(self, st: int, what: str, ok=(BM_OK,)) -> int:
         if st not in ok:
@@ -322,6 +338,11 @@ class Engine:
         return st
 
     def close(self) -> None:
+        for ref in self._children:
+            child = ref()
+            if child is not None:
+                child.close()
+        self._children = []
         if self.h:
             self.L.bm_ctx_destroy(self.h)
             self.h = None
@@ -482,6 +503,60 @@ class Engine:
 
     def delta_pairs_dev(self, d_pairs: int, k: int, d_out: int) -> None:
         self._chk(self.L.bm_delta_pairs_dev(self.h, d_pairs, k, d_out), "bm_delta_pairs_dev")
+
+
+class Batch:
+    """Graph pairs of uneven size for batched annealing chains (bm_batch)."""
+
+    def __init__(self, eng: Engine):
+        self.eng = eng
+        self.L = eng.L
+        h = C.c_void_p()
+        eng._chk(self.L.bm_batch_create(eng.h, C.byref(h)), "bm_batch_create")
+        self.h = h
+        self.ns = []
+        import weakref
+        eng._children.append(weakref.ref(self))
+
+    def add_pair(self, A: Graph, B: Graph) -> int:
+        idx = C.c_int32()
+        n = max(A.n, B.n)
+        self.eng._chk(self.L.bm_batch_add_pair(self.h, n, A.m, _ptr(A.src), _ptr(A.dst), _ptr(A.w), B.m, _ptr(B.src),
+                                               _ptr(B.dst), _ptr(B.w), C.byref(idx)), "bm_batch_add_pair")
+        self.ns.append(n)
+        return idx.value
+
+    def sa_run(self, chain_pair, keys, init_pis, steps, t0=5.0, t_end=0.01, candidates=0, chunk=0):
+        """Run chains; init_pis is a list of n+1 arrays.  Returns (final_pis,
+        scores, accepts, stats)."""
+        cp = _i32(chain_pair)
+        k = np.ascontiguousarray(np.asarray(keys, dtype=np.uint64))
+        flat = np.ascontiguousarray(np.concatenate([_i32(p) for p in init_pis]))
+        out = np.zeros_like(flat)
+        nch = cp.shape[0]
+        scores = np.zeros(nch, np.int64)
+        acc = np.zeros(nch, np.int64)
+        prm = SaParams(steps, t0, t_end, candidates, chunk)
+        st = SaStats()
+        self.eng._chk(self.L.bm_sa_run(self.h, nch, _ptr(cp), _ptr(k), _ptr(flat), C.byref(prm), _ptr(out),
+                                       _ptr(scores), _ptr(acc), C.byref(st)), "bm_sa_run")
+        pis, o = [], 0
+        for c in range(nch):
+            n = self.ns[int(cp[c])]
+            pis.append(out[o:o + n + 1].copy())
+            o += n + 1
+        return pis, scores, acc, st
+
+    def close(self):
+        if self.h:
+            self.L.bm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def header_functions(header: str = "bm_cuda.h") -> list[str]:

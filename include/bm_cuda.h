@@ -178,6 +178,48 @@ bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, int32_t nrows
                             int32_t rows_per_batch, int64_t max_accepts, int32_t max_sweeps,
                             double time_budget_s, int64_t target_score, bm_progress* prog);
 
+/* ------------------------------------------------- annealing chains */
+
+/* A batch of graph pairs of uneven size, for many independent annealing
+ * chains in one persistent kernel.  Pairs are added like bm_set_graph (same
+ * limits and duplicate rules); each gets an index 0, 1, ...  A batch runs on
+ * its context's device and stream; destroy it before the context. */
+typedef struct bm_batch bm_batch;
+bm_status bm_batch_create(bm_ctx* ctx, bm_batch** out);
+void bm_batch_destroy(bm_batch* b);
+bm_status bm_batch_add_pair(bm_batch* b, int32_t n,
+                            int64_t mA, const int32_t* srcA, const int32_t* dstA, const int32_t* wA,
+                            int64_t mB, const int32_t* srcB, const int32_t* dstB, const int32_t* wB,
+                            int32_t* pair_index);
+
+typedef struct bm_sa_params {
+    int64_t steps;       /* proposals per chain */
+    double t0;           /* starting temperature */
+    double t_end;        /* final temperature: T_i = t0 * exp(ln(t_end/t0) * i / steps) */
+    int32_t candidates;  /* proposals evaluated together per iteration, 1..16; 0 = autotuned */
+    int64_t chunk;       /* proposals per chain per kernel launch (0 = 65536) */
+} bm_sa_params;
+
+typedef struct bm_sa_stats {
+    int32_t candidates;  /* value used */
+    int64_t launches;    /* graph replays */
+    double seconds;      /* wall time of the chain launches */
+} bm_sa_stats;
+
+/* Simulated annealing, the loop of simulated_annealing in
+ * src/best-swap/score-lookup.c:346-408 with exact int64 deltas.  Chain c runs
+ * on pair chain_pair[c]; its proposals come from Philox4x32-10 keyed by
+ * chain_key[c] with the step as counter, and the acceptance test
+ * u < exp(delta/T) uses the library's own exp, so every chain is
+ * deterministic and independent of `candidates`.  init_pi and final_pi hold
+ * the chains' mappings back to back, n_c + 1 ints each (slot 0 ignored);
+ * bm_sa_layout_size gives the total.  final_score and accepts have nchains
+ * entries.  Any output pointer may be NULL. */
+bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chain_pair, const uint64_t* chain_key,
+                    const int32_t* init_pi, const bm_sa_params* params, int32_t* final_pi,
+                    int64_t* final_score, int64_t* accepts, bm_sa_stats* stats);
+int64_t bm_sa_layout_size(bm_batch* b, int32_t nchains, const int32_t* chain_pair);
+
 /* ------------------------------------------------------- device utilities */
 
 /* Device memory, copies and events on the context stream, for callers that

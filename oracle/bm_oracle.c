@@ -19,9 +19,15 @@
  * Parity is pinned by tests/golden/ fixtures produced by the reference's own
  * functions compiled from its sources (oracle/ref_harness.c).
  */
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+
+/* The chains' RNG (Philox4x32-10) and exp are defined by the engine; the
+ * replay below uses the same definitions so a chain can be checked step by
+ * step.  Both are pinned separately (known-answer vectors, error bounds). */
+#include "../brain-match_b200/csrc/bm_rng.hpp"
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -239,3 +245,33 @@ void orc_pairs(const orc_graph* gm, const orc_graph* gf, const int32_t* mapping,
         out[i] = (u == v) ? 0 : orc_swap_delta(gm, gf, mapping, u, v);
     }
 }
+
+/* Simulated-annealing chain of simulated_annealing
+ * (src/best-swap/score-lookup.c:346-408), restated with the engine's chain
+ * definition: proposal s from Philox4x32-10(key, s) (bm_sa_proposal), the
+ * exact delta (calculate_swap_delta, exact on graphs without self-loops),
+ * acceptance delta >= 0 or u < exp(delta / T_s) with T_s of the geometric
+ * schedule, immediate apply.  log_ratio = log(t_end / t0).  Returns accepts;
+ * mapping and *score are updated in place. */
+int64_t orc_sa_run(const orc_graph* gm, const orc_graph* gf, int32_t* mapping, uint64_t key, int64_t steps,
+                   double t0, double t_end, int64_t* score) {
+    const double lr = log(t_end / t0);
+    int64_t accepts = 0;
+    for (int64_t s = 0; s < steps; s++) {
+        bm_proposal p = bm_sa_proposal(key, (uint64_t)s, gm->n);
+        int64_t d = orc_swap_delta(gm, gf, mapping, p.u, p.v);
+        if (bm_sa_accept(d, p.uni, bm_sa_temperature(t0, lr, (uint64_t)s, (uint64_t)steps))) {
+            int32_t t = mapping[p.u];
+            mapping[p.u] = mapping[p.v];
+            mapping[p.v] = t;
+            *score += d;
+            accepts++;
+        }
+    }
+    return accepts;
+}
+
+/* Philox4x32-10 and exp as seen from the CPU, for known-answer and
+ * error-bound tests. */
+void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) { bm_philox4x32_10(ctr, key, out); }
+double orc_exp(double x) { return bm_exp(x); }

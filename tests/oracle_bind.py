@@ -49,6 +49,8 @@ def oracle_lib() -> C.CDLL:
         L.orc_rows_omp.argtypes = [vp, vp, vp, vp, C.c_int32, vp, C.c_int32]
         L.orc_pairs.restype = None
         L.orc_pairs.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
+        L.orc_sa_run.restype = C.c_int64
+        L.orc_sa_run.argtypes = [vp, vp, vp, C.c_uint64, C.c_int64, C.c_double, C.c_double, C.POINTER(C.c_int64)]
         _orc = L
     return _orc
 
@@ -130,6 +132,14 @@ class Oracle:
         out = np.zeros((rows.shape[0], self.n + 1), np.int64)
         self.L.orc_rows_omp(self.gm, self.gf, _p(pi), _p(rows), rows.shape[0], _p(out), threads)
         return out
+
+    def sa(self, pi, key, steps, t0=5.0, t_end=0.01):
+        """Replay of one annealing chain; returns (pi, score, accepts)."""
+        pi = _i32(pi).copy()
+        score = C.c_int64(self.score(pi))
+        acc = self.L.orc_sa_run(self.gm, self.gf, _p(pi), int(key), int(steps), float(t0), float(t_end),
+                                C.byref(score))
+        return pi, int(score.value), int(acc)
 
     def serial(self, pi, rows=None, max_accepts=-1, max_sweeps=-1, log_cap=1 << 20):
         """Bounded serial first-improvement loop; returns (pi, score, log, sweeps, converged)."""
