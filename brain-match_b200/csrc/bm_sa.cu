@@ -19,6 +19,7 @@
 // captured once in a CUDA graph and replayed until all chains finish.
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -529,4 +530,171 @@ extern "C" int64_t bm_sa_layout_size(bm_batch* b, int32_t nchains, const int32_t
         tot += b->pairs[(size_t)chain_pair[c]].n + 1;
     }
     return tot;
+}
+
+// --------------------------------------------------- allocation-free variant
+//
+// bm_sa_run_noalloc runs the same chains as bm_sa_run without allocating any
+// device memory.  It is for callers that cannot call cudaMalloc/cudaFree while
+// they run: a process whose device memory is owned by its own pool allocator
+// under a fixed budget, or a serving path that must not pay the implicit
+// device-wide synchronisation of cudaFree while other streams are busy.
+//
+// Its scratch is the file-scope array below: the pair table, the chain states,
+// and every chain's mapping and per-vertex overlap.  Every GPU that loads this
+// library holds the array until the process exits.  Host code must not use the
+// symbol's name as a device address; the address is obtained once per device
+// with cudaGetSymbolAddress (first call on that device, with the device
+// current) and passed to the kernels.  All calls share the array and it keeps
+// the last call's contents, so each call rewrites what it reads and clears the
+// overlap arrays; calls whose work overlaps on the GPU (two host threads, or
+// two contexts on one device) race and must be serialised by the caller.
+
+namespace {
+
+constexpr int64_t kNoAllocMaxPairs = 256;
+constexpr int64_t kNoAllocMaxChains = 1024;
+constexpr int64_t kNoAllocMaxInts = 1 << 20;  // sum over chains of (n + 1)
+constexpr size_t kNoAllocPairBytes = 128;
+constexpr size_t kNoAllocChainBytes = 64;
+constexpr size_t kNoAllocOffChains = kNoAllocMaxPairs * kNoAllocPairBytes;
+constexpr size_t kNoAllocOffPi = kNoAllocOffChains + kNoAllocMaxChains * kNoAllocChainBytes;
+constexpr size_t kNoAllocOffOv = kNoAllocOffPi + sizeof(int32_t) * kNoAllocMaxInts;
+constexpr size_t kNoAllocBytes = kNoAllocOffOv + sizeof(int32_t) * kNoAllocMaxInts;  // 8,486,912 bytes
+static_assert(sizeof(PairDev) <= kNoAllocPairBytes, "pair slot too small");
+static_assert(sizeof(ChainDev) <= kNoAllocChainBytes, "chain slot too small");
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_sa_noalloc_scratch[kNoAllocBytes];
+
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_addr[64] = {nullptr};
+
+// Device address of the scratch array on ctx's device (set up on first use).
+static bm_status noalloc_scratch(bm_ctx* ctx, unsigned char** out) {
+    if (ctx->device < 0 || ctx->device >= 64) return bm_fail(ctx, BM_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[ctx->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_sa_noalloc_scratch);
+        if (e != cudaSuccess) return bm_cuda_fail(ctx, e, "cudaGetSymbolAddress(g_sa_noalloc_scratch)");
+        g_noalloc_addr[ctx->device] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[ctx->device];
+    return BM_OK;
+}
+
+extern "C" bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32_t* chain_pair,
+                                       const uint64_t* chain_key, const int32_t* init_pi,
+                                       const bm_sa_params* prm, int32_t* final_pi, int64_t* final_score,
+                                       int64_t* accepts) {
+    if (!b || !prm || nchains < 1 || !chain_pair || !chain_key || !init_pi) return BM_INVALID_ARG;
+    bm_ctx* ctx = b->ctx;
+    const int64_t np = (int64_t)b->pairs.size();
+    if (np > kNoAllocMaxPairs)
+        return bm_fail(ctx, BM_INVALID_ARG, "batch holds %lld pairs; the allocation-free entry point takes at most %lld",
+                       (long long)np, (long long)kNoAllocMaxPairs);
+    if (nchains > kNoAllocMaxChains)
+        return bm_fail(ctx, BM_INVALID_ARG, "%d chains; the allocation-free entry point takes at most %lld", nchains,
+                       (long long)kNoAllocMaxChains);
+    if (prm->steps < 0 || !(prm->t0 > 0) || !(prm->t_end > 0))
+        return bm_fail(ctx, BM_INVALID_ARG, "need steps >= 0 and positive temperatures");
+    int64_t tot = 0;
+    for (int32_t c = 0; c < nchains; c++) {
+        if (chain_pair[c] < 0 || chain_pair[c] >= np) return bm_fail(ctx, BM_INVALID_ARG, "chain %d: bad pair", c);
+        tot += (int64_t)b->pairs[(size_t)chain_pair[c]].n + 1;
+    }
+    if (tot > kNoAllocMaxInts)
+        return bm_fail(ctx, BM_INVALID_ARG,
+                       "chains need %lld mapping entries; the allocation-free entry point holds at most %lld",
+                       (long long)tot, (long long)kNoAllocMaxInts);
+    // bijection check with a fixed bitset (n <= 131071)
+    {
+        uint64_t seen[(BM_MAX_N + 64) / 64];
+        int64_t o = 0;
+        for (int32_t c = 0; c < nchains; c++) {
+            const int32_t n = b->pairs[(size_t)chain_pair[c]].n;
+            memset(seen, 0, sizeof(uint64_t) * (size_t)((n + 64) / 64));
+            for (int32_t i = 1; i <= n; i++) {
+                const int32_t f = init_pi[o + i];
+                if (f < 1 || f > n || ((seen[f >> 6] >> (f & 63)) & 1ull))
+                    return bm_fail(ctx, BM_INVALID_ARG, "chain %d: pi is not a bijection", c);
+                seen[f >> 6] |= 1ull << (f & 63);
+            }
+            o += n + 1;
+        }
+    }
+    BM_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaFuncAttributes fa;
+    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel));
+    const int32_t kmax = std::max(1, std::min(16, fa.maxThreadsPerBlock / 32));
+    int32_t K = prm->candidates == 0 ? std::min(8, kmax) : prm->candidates;
+    if (K < 1 || K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates must be 0 or 1..%d", kmax);
+    unsigned char* base = nullptr;
+    bm_status st = noalloc_scratch(ctx, &base);
+    if (st != BM_OK) return st;
+    PairDev* d_pairs = reinterpret_cast<PairDev*>(base);
+    ChainDev* d_ch = reinterpret_cast<ChainDev*>(base + kNoAllocOffChains);
+    int32_t* d_pi = reinterpret_cast<int32_t*>(base + kNoAllocOffPi);
+    int32_t* d_ov = reinterpret_cast<int32_t*>(base + kNoAllocOffOv);
+    // pair table and chain states, staged through small host arrays on the stack
+    {
+        PairDev hp[16];
+        for (int64_t i0 = 0; i0 < np; i0 += 16) {
+            const int64_t k = std::min<int64_t>(16, np - i0);
+            for (int64_t j = 0; j < k; j++) {
+                const auto& p = b->pairs[(size_t)(i0 + j)];
+                hp[j] = PairDev{p.n, p.has_self, p.d[0], p.d[1], p.e[0], p.e[1], p.d[2], p.d[3],
+                                HashView{p.hash, p.hlog2, p.n + 1}};
+            }
+            BM_CUDA(ctx, cudaMemcpyAsync(d_pairs + i0, hp, sizeof(PairDev) * (size_t)k, cudaMemcpyHostToDevice, ctx->stream));
+            BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+        ChainDev hc[32];
+        int64_t o = 0;
+        for (int32_t c0 = 0; c0 < nchains; c0 += 32) {
+            const int32_t k = std::min(32, nchains - c0);
+            for (int32_t j = 0; j < k; j++) {
+                const int32_t c = c0 + j;
+                hc[j] = ChainDev{chain_pair[c], 0, d_pi + o, d_ov + o, chain_key[c], 0ull, 0, 0};
+                o += (int64_t)b->pairs[(size_t)chain_pair[c]].n + 1;
+            }
+            BM_CUDA(ctx, cudaMemcpyAsync(d_ch + c0, hc, sizeof(ChainDev) * (size_t)k, cudaMemcpyHostToDevice, ctx->stream));
+            BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+    }
+    BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
+    BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
+    sa_init_kernel<<<dim3(64, (unsigned)nchains), 256, 0, ctx->stream>>>(d_pairs, d_ch, nchains);
+    BM_LAUNCH_CHECK(ctx, "sa_init_kernel");
+    SaArgs args;
+    args.pairs = d_pairs;
+    args.chains = d_ch;
+    args.nchains = nchains;
+    args.steps = (uint64_t)prm->steps;
+    args.t0 = prm->t0;
+    args.log_ratio = log(prm->t_end / prm->t0);
+    args.chunk = prm->chunk > 0 ? (uint64_t)prm->chunk : (uint64_t)65536;
+    const uint64_t launches = args.steps == 0 ? 0 : (args.steps + args.chunk - 1) / args.chunk;
+    for (uint64_t l = 0; l < launches; l++) {
+        sa_chain_kernel<<<nchains, 32 * K, 0, ctx->stream>>>(args);
+        BM_LAUNCH_CHECK(ctx, "sa_chain_kernel");
+    }
+    if (final_pi)
+        BM_CUDA(ctx, cudaMemcpyAsync(final_pi, d_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyDeviceToHost, ctx->stream));
+    {
+        ChainDev hc[32];
+        for (int32_t c0 = 0; c0 < nchains; c0 += 32) {
+            const int32_t k = std::min(32, nchains - c0);
+            BM_CUDA(ctx, cudaMemcpyAsync(hc, d_ch + c0, sizeof(ChainDev) * (size_t)k, cudaMemcpyDeviceToHost, ctx->stream));
+            BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            for (int32_t j = 0; j < k; j++) {
+                if (final_score) final_score[c0 + j] = hc[j].score;
+                if (accepts) accepts[c0 + j] = hc[j].accepts;
+            }
+        }
+    }
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BM_OK;
 }

@@ -220,6 +220,24 @@ bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chain_pair, con
                     int64_t* final_score, int64_t* accepts, bm_sa_stats* stats);
 int64_t bm_sa_layout_size(bm_batch* b, int32_t nchains, const int32_t* chain_pair);
 
+/* The chains of bm_sa_run, computed without allocating any device memory.
+ * No counterpart in the reference.  For callers that cannot call
+ * cudaMalloc/cudaFree while they run (device memory owned by their own pool
+ * under a fixed budget, or a serving path that must not take cudaFree's
+ * device-wide synchronisation).  The batch itself is built beforehand with
+ * bm_batch_add_pair, which does allocate.  All scratch lives in one static
+ * device array of 8,486,912 bytes that every GPU loading the library holds
+ * until exit; it limits a call to 256 pairs, 1,024 chains and a total of
+ * 2^20 mapping entries (sum over chains of n + 1); larger requests return
+ * BM_INVALID_ARG.  The first call on a device looks up the array's device
+ * address and should come before any stream capture on that device.  Calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller.  candidates == 0 uses 8 (no autotuning: the tuner would
+ * allocate).  Arguments and outputs as bm_sa_run, without stats. */
+bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32_t* chain_pair, const uint64_t* chain_key,
+                            const int32_t* init_pi, const bm_sa_params* params, int32_t* final_pi,
+                            int64_t* final_score, int64_t* accepts);
+
 /* ------------------------------------------------------- device utilities */
 
 /* Device memory, copies and events on the context stream, for callers that
