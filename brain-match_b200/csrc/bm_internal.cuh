@@ -156,3 +156,6 @@ bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_co
                          int64_t* d_full, bm_row_result* d_res);
 bm_status bm_launch_apply(bm_ctx* ctx, const int32_t* d_pairs, int32_t k);
 bm_status bm_rows_smem_check(bm_ctx* ctx);
+bm_status bm_launch_kset(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t nsets, long long* d_best,
+                         int32_t* d_perm, long long* d_all, int32_t* d_status);
+bm_status bm_launch_apply_sets(bm_ctx* ctx, int32_t k, const int32_t* d_sets, const int32_t* d_perms, int32_t nsets);

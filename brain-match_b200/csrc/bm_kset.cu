@@ -1,0 +1,389 @@
+// bm_kset.cu — exact deltas of permutations of small vertex sets (k <= 8):
+// the 3-vertex moves of src/graph-re-alignment-gpu-3-swap.cu:43-305 (best of
+// the non-identity permutations of a triple, applied by apply_permutation
+// :925-956) and the permutation sets of
+// src/graph-alignment-permset-parallel.c:304-363,625-746 (all k! permutations
+// of a random k-subset, the best one applied).  The reference's group delta
+// counts an edge inside the group twice and is repaired by a full re-score
+// (:698-730); here the delta is exact.
+//
+// For a set T = {t_0..t_{k-1}} with images f_i = pi(t_i) and a permutation
+// sigma (member i takes the image of member sigma(i)):
+//
+//   delta(sigma) = sum_i (g[i][sigma i] - S(t_i)) + sum over A entries e = (t_i -> t_j, w)
+//                  inside T of [h(si, sj) + h(i, j) - h(si, j) - h(i, sj)] + self-loop terms
+//
+// with g[i][q] = G_{t_i}(f_q) = sum_{x in out(t_i)} min(w, B(f_q, pi x)) +
+// sum_{x in in(t_i)} min(w, B(pi x, f_q)) (old images everywhere, so
+// g[i][i] = S(t_i)), h(p, q) = min(w, B(f_p, f_q)) and h(p, p) = 0.  The first
+// sum moves every member's external and internal edges as if the other end
+// stayed; the second repairs each internal edge to its true new value.
+//
+// One CTA per set: the members' lists are scanned once with k-1 B lookups per
+// entry (atomics into g in shared memory), then the k! permutations are
+// enumerated in lexicographic order, each thread a contiguous block stepped by
+// next-permutation, and reduced to the best (largest delta, lowest index).
+#include <climits>
+#include <vector>
+
+#include "bm_internal.cuh"
+
+namespace {
+
+constexpr int kKThreads = 256;
+constexpr int kMaxK = 8;
+constexpr int kMaxInternal = 256;
+
+struct KsetArgs {
+    GView A;
+    HashView hb;
+    const int32_t* selfB;
+    int has_self;
+    const int32_t* pi;
+    const int32_t* ov;
+    int32_t n;
+    int32_t k;
+    int32_t kfact;
+    const int32_t* sets;
+    int64_t nsets;
+    long long* best_delta;
+    int32_t* best_perm;  // nsets * k
+    long long* all;      // nsets * kfact, optional
+    int32_t* status;     // nonzero: some set was rejected (see bm_kset_eval)
+};
+
+__device__ __forceinline__ void decode_perm(int32_t p, int k, int32_t* s) {
+    int32_t avail[kMaxK];
+    int32_t f = 1;
+    for (int i = 0; i < k; i++) avail[i] = i;
+    for (int i = 2; i < k; i++) f *= i;  // (k-1)!
+    for (int i = 0; i < k; i++) {
+        const int32_t idx = (k - 1 - i) > 0 ? p / f : 0;
+        if (k - 1 - i > 0) p -= idx * f;
+        s[i] = avail[idx];
+        for (int j = idx; j < k - 1 - i; j++) avail[j] = avail[j + 1];
+        if (k - 1 - i > 0) f /= (k - 1 - i);
+    }
+}
+
+__device__ __forceinline__ void next_perm(int k, int32_t* s) {
+    int i = k - 2;
+    while (i >= 0 && s[i] >= s[i + 1]) i--;
+    if (i < 0) return;
+    int j = k - 1;
+    while (s[j] <= s[i]) j--;
+    int32_t t = s[i]; s[i] = s[j]; s[j] = t;
+    for (int a = i + 1, b = k - 1; a < b; a++, b--) { t = s[a]; s[a] = s[b]; s[b] = t; }
+}
+
+__global__ void __launch_bounds__(kKThreads) kset_kernel(KsetArgs a) {
+    __shared__ int32_t t[kMaxK], f[kMaxK], sA[kMaxK], sB[kMaxK];
+    __shared__ int32_t g[kMaxK * kMaxK], Bsub[kMaxK * kMaxK];
+    __shared__ int32_t n_int, bad;
+    __shared__ int32_t ie_i[kMaxInternal], ie_j[kMaxInternal], ie_w[kMaxInternal];
+    __shared__ long long red_d[kKThreads / 32];
+    __shared__ int32_t red_p[kKThreads / 32];
+    const int k = a.k, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int64_t set = blockIdx.x; set < a.nsets; set += gridDim.x) {
+        if (tid == 0) { n_int = 0; bad = 0; }
+        if (tid < k) {
+            const int32_t v = a.sets[set * k + tid];
+            t[tid] = v;
+            if (v < 1 || v > a.n) bad = 1;
+        }
+        if (tid < k * k) g[tid] = 0;
+        __syncthreads();
+        if (tid == 0)
+            for (int i = 0; i < k; i++)
+                for (int j = i + 1; j < k; j++)
+                    if (t[i] == t[j]) bad = 1;
+        __syncthreads();
+        if (bad) {
+            if (tid < k) a.best_perm[set * k + tid] = tid;
+            if (tid == 0) { a.best_delta[set] = 0; atomicOr(a.status, 1); }
+            if (a.all)
+                for (int32_t p = tid; p < a.kfact; p += kKThreads) a.all[set * a.kfact + p] = 0;
+            __syncthreads();
+            continue;
+        }
+        if (tid < k) {
+            f[tid] = a.pi[t[tid]];
+            sA[tid] = a.has_self ? a.A.self_w[t[tid]] : 0;
+        }
+        __syncthreads();
+        if (tid < k) sB[tid] = a.has_self ? a.selfB[f[tid]] : 0;
+        if (tid < k * k) {
+            const int p = tid / k, q = tid % k;
+            Bsub[tid] = (p == q) ? 0 : bm_hash_get(a.hb, f[p], f[q]);
+        }
+        // ---- gains and internal entries: scan each member's out- and in-list
+        for (int i = 0; i < k; i++) {
+            for (int dir = 0; dir < 2; dir++) {
+                const int32_t* ptr = dir ? a.A.in_ptr : a.A.out_ptr;
+                const uint32_t* ent = dir ? a.A.in_ent : a.A.out_ent;
+                const int32_t b = ptr[t[i]], e = ptr[t[i] + 1];
+                for (int32_t j = b + tid; j < e; j += kKThreads) {
+                    const uint32_t en = ent[j];
+                    if (en == 0) continue;
+                    const int32_t x = bm_eid(en), w = bm_ew(en);
+                    const int32_t gx = a.pi[x];
+                    if (dir == 0) {
+                        for (int q = 0; q < k; q++)
+                            if (t[q] == x) {
+                                const int32_t slot = atomicAdd(&n_int, 1);
+                                if (slot < kMaxInternal) { ie_i[slot] = i; ie_j[slot] = q; ie_w[slot] = w; }
+                            }
+                    }
+                    for (int q = 0; q < k; q++) {
+                        if (q == i) continue;
+                        const int32_t bw = dir ? bm_hash_get(a.hb, gx, f[q]) : bm_hash_get(a.hb, f[q], gx);
+                        const int32_t c = imin(w, bw);
+                        if (c) atomicAdd(&g[i * k + q], c);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < k) g[tid * k + tid] = a.ov[t[tid]];
+        if (tid == 0 && n_int > kMaxInternal) { bad = 1; atomicOr(a.status, 2); }
+        __syncthreads();
+        const int32_t ni = bad ? 0 : n_int;
+        // ---- enumerate permutations
+        const int32_t per = (a.kfact + kKThreads - 1) / kKThreads;
+        const int32_t p0 = tid * per, p1 = min(a.kfact, p0 + per);
+        long long bd = LLONG_MIN;
+        int32_t bp = INT_MAX;
+        if (!bad && p0 < p1) {
+            int32_t s[kMaxK];
+            decode_perm(p0, k, s);
+            for (int32_t p = p0; p < p1; p++) {
+                long long d = 0;
+                for (int i = 0; i < k; i++) d += (long long)g[i * k + s[i]] - g[i * k + i];
+                for (int32_t e = 0; e < ni; e++) {
+                    const int i = ie_i[e], j = ie_j[e], w = ie_w[e];
+                    const int si = s[i], sj = s[j];
+                    d += imin(w, Bsub[si * k + sj]) + imin(w, Bsub[i * k + j]) - imin(w, Bsub[si * k + j]) -
+                         imin(w, Bsub[i * k + sj]);
+                }
+                if (a.has_self)
+                    for (int i = 0; i < k; i++) d += imin(sA[i], sB[s[i]]) - imin(sA[i], sB[i]);
+                if (a.all) a.all[set * a.kfact + p] = d;
+                if (d > bd) { bd = d; bp = p; }
+                next_perm(k, s);
+            }
+        }
+        if (bad && a.all)
+            for (int32_t p = tid; p < a.kfact; p += kKThreads) a.all[set * a.kfact + p] = 0;
+        // ---- block argmax (largest delta, lowest index)
+        for (int o = 16; o; o >>= 1) {
+            const long long d2 = __shfl_xor_sync(0xffffffffu, bd, o);
+            const int32_t p2 = __shfl_xor_sync(0xffffffffu, bp, o);
+            if (d2 > bd || (d2 == bd && p2 < bp)) { bd = d2; bp = p2; }
+        }
+        if (lane == 0) { red_d[warp] = bd; red_p[warp] = bp; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < kKThreads / 32; w++)
+                if (red_d[w] > red_d[0] || (red_d[w] == red_d[0] && red_p[w] < red_p[0])) {
+                    red_d[0] = red_d[w];
+                    red_p[0] = red_p[w];
+                }
+            if (bad) { red_d[0] = 0; red_p[0] = 0; }
+            a.best_delta[set] = red_d[0];
+            int32_t s[kMaxK];
+            decode_perm(red_p[0], k, s);
+            for (int i = 0; i < k; i++) a.best_perm[set * k + i] = s[i];
+        }
+        __syncthreads();
+    }
+}
+
+// Apply permutations of independent sets: member i of set takes the image of
+// member perm[i].  S updates of every A entry touching a member (entries
+// inside a set once, from the out-lists), relabelled B entries, then pi.
+struct ApplySetsArgs {
+    GView A;
+    const int32_t* Bout_ptr;
+    const int32_t* Bin_ptr;
+    uint32_t* Bout_ent;
+    uint32_t* Bin_ent;
+    const int32_t* Bout_twin;
+    const int32_t* Bin_twin;
+    HashView hb;
+    int32_t* pi;
+    int32_t* pinv;
+    int32_t* ov;
+    int32_t k;
+    const int32_t* sets;
+    const int32_t* perms;
+};
+
+__global__ void __launch_bounds__(kKThreads) apply_sets_kernel(ApplySetsArgs a) {
+    __shared__ int32_t t[kMaxK], f[kMaxK], fn[kMaxK];
+    const int k = a.k;
+    const int64_t set = blockIdx.x;
+    if (threadIdx.x < k) {
+        t[threadIdx.x] = a.sets[set * k + threadIdx.x];
+        f[threadIdx.x] = a.pi[t[threadIdx.x]];
+    }
+    __syncthreads();
+    if (threadIdx.x < k) fn[threadIdx.x] = f[a.perms[set * k + threadIdx.x]];
+    __syncthreads();
+    for (int i = 0; i < k; i++) {
+        for (int dir = 0; dir < 2; dir++) {
+            const int32_t* ptr = dir ? a.A.in_ptr : a.A.out_ptr;
+            const uint32_t* ent = dir ? a.A.in_ent : a.A.out_ent;
+            const int32_t b = ptr[t[i]], e = ptr[t[i] + 1];
+            for (int32_t j = b + threadIdx.x; j < e; j += kKThreads) {
+                const uint32_t en = ent[j];
+                if (en == 0) continue;
+                const int32_t x = bm_eid(en), w = bm_ew(en);
+                int xq = -1;
+                for (int q = 0; q < k; q++)
+                    if (t[q] == x) xq = q;
+                if (dir == 1 && xq >= 0) continue;  // inside the set: counted from the out-list
+                const int32_t gx_old = a.pi[x];
+                const int32_t gx_new = xq >= 0 ? fn[xq] : gx_old;
+                int32_t d;
+                if (dir == 0)
+                    d = imin(w, bm_hash_get(a.hb, fn[i], gx_new)) - imin(w, bm_hash_get(a.hb, f[i], gx_old));
+                else
+                    d = imin(w, bm_hash_get(a.hb, gx_new, fn[i])) - imin(w, bm_hash_get(a.hb, gx_old, f[i]));
+                if (d) { atomicAdd(a.ov + t[i], d); atomicAdd(a.ov + x, d); }
+            }
+        }
+    }
+    // image f[q] is now held by the member i with fn[i] == f[q]
+    for (int i = 0; i < k; i++) {
+        const int32_t img = fn[i];
+        const uint32_t label = (uint32_t)t[i];
+        for (int dir = 0; dir < 2; dir++) {
+            const int32_t* ptr = dir ? a.Bout_ptr : a.Bin_ptr;
+            const int32_t* twin = dir ? a.Bout_twin : a.Bin_twin;
+            uint32_t* other = dir ? a.Bin_ent : a.Bout_ent;
+            const int32_t b = ptr[img], e = ptr[img + 1];
+            for (int32_t j = b + threadIdx.x; j < e; j += kKThreads) {
+                const int32_t tw = twin[j];
+                if (tw < 0) continue;
+                other[tw] = (other[tw] & ~BM_ID_MASK) | label;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < k; i++) {
+            a.pi[t[i]] = fn[i];
+            a.pinv[fn[i]] = t[i];
+        }
+}
+
+int32_t factorial(int k) {
+    int32_t f = 1;
+    for (int i = 2; i <= k; i++) f *= i;
+    return f;
+}
+
+}  // namespace
+
+bm_status bm_launch_kset(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t nsets, long long* d_best,
+                         int32_t* d_perm, long long* d_all, int32_t* d_status) {
+    if (nsets <= 0) return BM_OK;
+    KsetArgs a;
+    a.A = gview(ctx->g[0]);
+    a.hb = hview(ctx->g[1]);
+    a.selfB = ctx->g[1].self_w;
+    a.has_self = ctx->g[0].has_self && ctx->g[1].has_self;
+    a.pi = ctx->pi;
+    a.ov = ctx->ov;
+    a.n = ctx->n;
+    a.k = k;
+    a.kfact = factorial(k);
+    a.sets = d_sets;
+    a.nsets = nsets;
+    a.best_delta = d_best;
+    a.best_perm = d_perm;
+    a.all = d_all;
+    a.status = d_status;
+    int64_t blocks = nsets < (int64_t)ctx->num_sms * 8 ? nsets : (int64_t)ctx->num_sms * 8;
+    kset_kernel<<<(unsigned)blocks, kKThreads, 0, ctx->stream>>>(a);
+    BM_LAUNCH_CHECK(ctx, "kset_kernel");
+    return BM_OK;
+}
+
+bm_status bm_launch_apply_sets(bm_ctx* ctx, int32_t k, const int32_t* d_sets, const int32_t* d_perms, int32_t nsets) {
+    if (nsets <= 0) return BM_OK;
+    const DevGraph& B = ctx->g[1];
+    ApplySetsArgs a;
+    a.A = gview(ctx->g[0]);
+    a.Bout_ptr = B.out_ptr;
+    a.Bin_ptr = B.in_ptr;
+    a.Bout_ent = B.out_ent;
+    a.Bin_ent = B.in_ent;
+    a.Bout_twin = B.out_twin;
+    a.Bin_twin = B.in_twin;
+    a.hb = hview(B);
+    a.pi = ctx->pi;
+    a.pinv = ctx->pinv;
+    a.ov = ctx->ov;
+    a.k = k;
+    a.sets = d_sets;
+    a.perms = d_perms;
+    apply_sets_kernel<<<nsets, kKThreads, 0, ctx->stream>>>(a);
+    BM_LAUNCH_CHECK(ctx, "apply_sets_kernel");
+    return BM_OK;
+}
+
+extern "C" bm_status bm_kset_eval(bm_ctx* ctx, int32_t k, const int32_t* sets, int64_t nsets, int64_t* best_delta,
+                                  int32_t* best_perm, int64_t* all_deltas) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (k < 2 || k > kMaxK) return bm_fail(ctx, BM_INVALID_ARG, "k must be 2..%d", kMaxK);
+    if (nsets < 0 || (nsets > 0 && (!sets || !best_delta || !best_perm)))
+        return bm_fail(ctx, BM_INVALID_ARG, "bad set buffers");
+    if (nsets == 0) return BM_OK;
+    for (int64_t i = 0; i < nsets; i++)
+        for (int a = 0; a < k; a++) {
+            const int32_t v = sets[i * k + a];
+            if (v < 1 || v > ctx->n) return bm_fail(ctx, BM_INVALID_ARG, "set %lld: id %d outside 1..%d", (long long)i, v, ctx->n);
+            for (int b = 0; b < a; b++)
+                if (sets[i * k + b] == v) return bm_fail(ctx, BM_INVALID_ARG, "set %lld repeats vertex %d", (long long)i, v);
+        }
+    const int32_t kf = factorial(k);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t b_sets = al(sizeof(int32_t) * (size_t)(nsets * k));
+    const size_t b_best = al(sizeof(long long) * (size_t)nsets);
+    const size_t b_perm = al(sizeof(int32_t) * (size_t)(nsets * k));
+    const size_t b_stat = 256;
+    const size_t b_all = all_deltas ? al(sizeof(long long) * (size_t)nsets * (size_t)kf) : 0;
+    if ((s = bm_stage(ctx, b_sets + b_best + b_perm + b_stat + b_all)) != BM_OK) return s;
+    char* base = (char*)ctx->stage;
+    int32_t* d_sets = (int32_t*)base;
+    long long* d_best = (long long*)(base + b_sets);
+    int32_t* d_perm = (int32_t*)(base + b_sets + b_best);
+    int32_t* d_stat = (int32_t*)(base + b_sets + b_best + b_perm);
+    long long* d_all = all_deltas ? (long long*)(base + b_sets + b_best + b_perm + b_stat) : nullptr;
+    BM_CUDA(ctx, cudaMemcpyAsync(d_sets, sets, sizeof(int32_t) * (size_t)(nsets * k), cudaMemcpyHostToDevice, ctx->stream));
+    BM_CUDA(ctx, cudaMemsetAsync(d_stat, 0, sizeof(int32_t), ctx->stream));
+    if ((s = bm_launch_kset(ctx, k, d_sets, nsets, d_best, d_perm, d_all, d_stat)) != BM_OK) return s;
+    int32_t hstat = 0;
+    BM_CUDA(ctx, cudaMemcpyAsync(best_delta, d_best, sizeof(long long) * (size_t)nsets, cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaMemcpyAsync(best_perm, d_perm, sizeof(int32_t) * (size_t)(nsets * k), cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaMemcpyAsync(&hstat, d_stat, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    if (all_deltas)
+        BM_CUDA(ctx, cudaMemcpyAsync(all_deltas, d_all, sizeof(long long) * (size_t)nsets * (size_t)kf,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hstat & 2)
+        return bm_fail(ctx, BM_UNSUPPORTED, "a set has more than %d A entries between its members", kMaxInternal);
+    return BM_OK;
+}
+
+extern "C" bm_status bm_kset_eval_dev(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t nsets,
+                                      int64_t* d_best_delta, int32_t* d_best_perm, int32_t* d_status) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (k < 2 || k > kMaxK) return bm_fail(ctx, BM_INVALID_ARG, "k must be 2..%d", kMaxK);
+    if (nsets < 0 || (nsets > 0 && (!d_sets || !d_best_delta || !d_best_perm || !d_status)))
+        return bm_fail(ctx, BM_INVALID_ARG, "bad set buffers");
+    return bm_launch_kset(ctx, k, d_sets, nsets, (long long*)d_best_delta, d_best_perm, nullptr, d_status);
+}

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "bm_internal.cuh"
+#include "bm_rng.hpp"
 
 namespace {
 
@@ -302,6 +303,182 @@ extern "C" bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, in
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     prog->next_row_pos = pos;
     prog->next_col = 1;
+    prog->seconds += secs_since(t0);
+    s = verify_score(ctx);
+    prog->score = ctx->score;
+    if (s != BM_OK) return s;
+    return ret;
+}
+
+// ------------------------------------------------------------- k-set moves
+
+extern "C" bm_status bm_apply_sets(bm_ctx* ctx, int32_t k, const int32_t* sets, const int32_t* perms,
+                                   const int64_t* deltas, int32_t nsets) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (k < 2 || k > 8) return bm_fail(ctx, BM_INVALID_ARG, "k must be 2..8");
+    if (nsets < 0 || (nsets > 0 && (!sets || !perms))) return bm_fail(ctx, BM_INVALID_ARG, "bad set buffers");
+    if (nsets == 0) return BM_OK;
+    const int32_t n = ctx->n;
+    Marks mk;
+    mk.reset(n);
+    for (int32_t i = 0; i < nsets; i++) {
+        int used = 0;
+        for (int a = 0; a < k; a++) {
+            const int32_t v = sets[(size_t)i * k + a], p = perms[(size_t)i * k + a];
+            if (v < 1 || v > n) return bm_fail(ctx, BM_INVALID_ARG, "set %d: id outside 1..%d", i, n);
+            if (p < 0 || p >= k || (used >> p & 1)) return bm_fail(ctx, BM_INVALID_ARG, "set %d: not a permutation", i);
+            used |= 1 << p;
+            for (int b = 0; b < a; b++)
+                if (sets[(size_t)i * k + b] == v) return bm_fail(ctx, BM_INVALID_ARG, "set %d repeats vertex %d", i, v);
+            if (mk.marked(v))
+                return bm_fail(ctx, BM_INVALID_ARG, "set %d is not independent of an earlier set", i);
+        }
+        for (int a = 0; a < k; a++) mk.mark_closed(ctx, sets[(size_t)i * k + a]);
+    }
+    const size_t b1 = ((size_t)nsets * k * sizeof(int32_t) + 255) & ~(size_t)255;
+    if ((s = bm_stage(ctx, 2 * b1)) != BM_OK) return s;
+    int32_t* d_sets = (int32_t*)ctx->stage;
+    int32_t* d_perms = (int32_t*)((char*)ctx->stage + b1);
+    BM_CUDA(ctx, cudaMemcpyAsync(d_sets, sets, sizeof(int32_t) * (size_t)nsets * k, cudaMemcpyHostToDevice, ctx->stream));
+    BM_CUDA(ctx, cudaMemcpyAsync(d_perms, perms, sizeof(int32_t) * (size_t)nsets * k, cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = bm_launch_apply_sets(ctx, k, d_sets, d_perms, nsets)) != BM_OK) return s;
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (deltas)
+        for (int32_t i = 0; i < nsets; i++) ctx->score += deltas[i];
+    return BM_OK;
+}
+
+namespace {
+
+// Candidate sets for bm_search_ksets: k distinct random vertices (mode 0), or
+// for k == 3 a path u - x - y of A (mode 1: x a neighbour of u, y a neighbour
+// of x).  Counter-based, so a (seed, launch, set) triple fixes the set.
+void draw_set(const bm_ctx* ctx, int32_t k, int32_t mode, uint64_t seed, uint64_t launch, uint64_t idx, int32_t* out) {
+    const int32_t n = ctx->n;
+    uint64_t ctr = (launch << 32) ^ idx;
+    uint32_t word[4];
+    int have = 0;
+    auto next = [&]() -> uint32_t {
+        if (have == 0) {
+            const uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), 0x6B657473u, 0u};
+            const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+            bm_philox4x32_10(c, key, word);
+            ctr += 1;
+            have = 4;
+        }
+        return word[--have];
+    };
+    auto neighbour = [&](int32_t v, int32_t* w) -> bool {
+        const int32_t d_out = ctx->hA_optr[(size_t)v + 1] - ctx->hA_optr[(size_t)v];
+        const int32_t d_in = ctx->hA_iptr[(size_t)v + 1] - ctx->hA_iptr[(size_t)v];
+        if (d_out + d_in == 0) return false;
+        for (int tries = 0; tries < 8; tries++) {
+            const uint32_t r = next() % (uint32_t)(d_out + d_in);
+            const uint32_t e = (int32_t)r < d_out ? ctx->hA_oent[(size_t)ctx->hA_optr[(size_t)v] + r]
+                                                   : ctx->hA_ient[(size_t)ctx->hA_iptr[(size_t)v] + (r - d_out)];
+            if (e != 0) { *w = bm_eid(e); return true; }
+        }
+        return false;
+    };
+    for (;;) {
+        int32_t m = 0;
+        if (mode == 1 && k == 3) {
+            const int32_t u = 1 + (int32_t)(next() % (uint32_t)n);
+            int32_t x, y;
+            if (neighbour(u, &x) && neighbour(x, &y) && y != u && y != x) {
+                out[0] = u; out[1] = x; out[2] = y;
+                return;
+            }
+            continue;
+        }
+        while (m < k) {
+            const int32_t v = 1 + (int32_t)(next() % (uint32_t)n);
+            bool dup = false;
+            for (int32_t j = 0; j < m; j++) dup |= out[j] == v;
+            if (!dup) out[m++] = v;
+        }
+        return;
+    }
+}
+
+}  // namespace
+
+extern "C" bm_status bm_search_ksets(bm_ctx* ctx, int32_t k, int32_t sets_per_launch, int32_t mode, uint64_t seed,
+                                     int64_t max_launches, double time_budget_s, bm_progress* prog) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (!prog) return bm_fail(ctx, BM_INVALID_ARG, "progress struct required");
+    if (k < 2 || k > 8) return bm_fail(ctx, BM_INVALID_ARG, "k must be 2..8");
+    if (mode == 1 && k != 3) return bm_fail(ctx, BM_INVALID_ARG, "path sets need k == 3");
+    if (sets_per_launch < 1 || ctx->n < k) return bm_fail(ctx, BM_INVALID_ARG, "need sets_per_launch >= 1 and n >= k");
+    const int64_t S = sets_per_launch;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t b_sets = al(sizeof(int32_t) * (size_t)(S * k)), b_best = al(sizeof(long long) * (size_t)S);
+    const size_t total = 2 * b_sets + b_best + 256;
+    if ((s = bm_stage(ctx, total)) != BM_OK) return s;
+    if ((s = bm_hstage(ctx, total)) != BM_OK) return s;
+    char* d = (char*)ctx->stage;
+    char* h = (char*)ctx->hstage;
+    int32_t* d_sets = (int32_t*)d;
+    int32_t* d_perm = (int32_t*)(d + b_sets);
+    long long* d_best = (long long*)(d + 2 * b_sets);
+    int32_t* d_stat = (int32_t*)(d + 2 * b_sets + b_best);
+    int32_t* h_sets = (int32_t*)h;
+    int32_t* h_perm = (int32_t*)(h + b_sets);
+    long long* h_best = (long long*)(h + 2 * b_sets);
+    std::vector<int32_t> order((size_t)S), ap_sets, ap_perms;
+    Marks mk;
+    const auto t0 = clk::now();
+    bm_status ret = BM_OK;
+    for (int64_t l = 0; max_launches < 0 || l < max_launches; l++) {
+        if (time_budget_s > 0 && secs_since(t0) >= time_budget_s) { ret = BM_TIMEOUT; break; }
+        const uint64_t launch = (uint64_t)prog->launches;
+        for (int64_t i = 0; i < S; i++) draw_set(ctx, k, mode, seed, launch, (uint64_t)i, h_sets + i * k);
+        BM_CUDA(ctx, cudaMemcpyAsync(d_sets, h_sets, sizeof(int32_t) * (size_t)(S * k), cudaMemcpyHostToDevice, ctx->stream));
+        BM_CUDA(ctx, cudaMemsetAsync(d_stat, 0, sizeof(int32_t), ctx->stream));
+        if ((s = bm_launch_kset(ctx, k, d_sets, S, d_best, d_perm, nullptr, d_stat)) != BM_OK) return s;
+        BM_CUDA(ctx, cudaMemcpyAsync(h_best, d_best, sizeof(long long) * (size_t)S, cudaMemcpyDeviceToHost, ctx->stream));
+        BM_CUDA(ctx, cudaMemcpyAsync(h_perm, d_perm, sizeof(int32_t) * (size_t)(S * k), cudaMemcpyDeviceToHost, ctx->stream));
+        BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        prog->launches++;
+        int64_t fact = 1;
+        for (int i = 2; i <= k; i++) fact *= i;
+        prog->evaluated += S * fact;
+        // greedy independent subset of the improving sets
+        int32_t cnt = 0;
+        for (int64_t i = 0; i < S; i++)
+            if (h_best[i] > 0) order[(size_t)cnt++] = (int32_t)i;
+        std::sort(order.begin(), order.begin() + cnt, [&](int32_t x, int32_t y) {
+            if (h_best[x] != h_best[y]) return h_best[x] > h_best[y];
+            return x < y;
+        });
+        mk.reset(ctx->n);
+        ap_sets.clear();
+        ap_perms.clear();
+        int64_t gain = 0;
+        for (int32_t c = 0; c < cnt; c++) {
+            const int32_t i = order[(size_t)c];
+            bool free_ = true;
+            for (int a = 0; a < k; a++) free_ &= !mk.marked(h_sets[i * k + a]);
+            if (!free_) continue;
+            for (int a = 0; a < k; a++) {
+                mk.mark_closed(ctx, h_sets[i * k + a]);
+                ap_sets.push_back(h_sets[i * k + a]);
+                ap_perms.push_back(h_perm[i * k + a]);
+            }
+            gain += h_best[i];
+        }
+        const int32_t na = (int32_t)(ap_sets.size() / (size_t)k);
+        if (na > 0) {
+            BM_CUDA(ctx, cudaMemcpyAsync(d_sets, ap_sets.data(), sizeof(int32_t) * ap_sets.size(), cudaMemcpyHostToDevice, ctx->stream));
+            BM_CUDA(ctx, cudaMemcpyAsync(d_perm, ap_perms.data(), sizeof(int32_t) * ap_perms.size(), cudaMemcpyHostToDevice, ctx->stream));
+            if ((s = bm_launch_apply_sets(ctx, k, d_sets, d_perm, na)) != BM_OK) return s;
+            BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            ctx->score += gain;
+            prog->accepts += na;
+        }
+    }
     prog->seconds += secs_since(t0);
     s = verify_score(ctx);
     prog->score = ctx->score;

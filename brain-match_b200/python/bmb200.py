@@ -130,6 +130,11 @@ def cuda_lib() -> C.CDLL:
             "bm_device_pci_bus_id": (C.c_int, [vp, C.c_char_p, C.c_int32]),
             "bm_rows_max_active_clusters": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
             "bm_set_row_tiling": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "bm_kset_eval": (C.c_int, [vp, C.c_int32, vp, C.c_int64, vp, vp, vp]),
+            "bm_kset_eval_dev": (C.c_int, [vp, C.c_int32, vp, C.c_int64, vp, vp, vp]),
+            "bm_apply_sets": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.c_int32]),
+            "bm_search_ksets": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int64, C.c_double,
+                                          C.POINTER(Progress)]),
             "bm_batch_create": (C.c_int, [vp, C.POINTER(vp)]),
             "bm_batch_destroy": (None, [vp]),
             "bm_batch_add_pair": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, vp, C.c_int64, vp, vp, vp,
@@ -442,6 +447,35 @@ class Engine:
                                       rows_per_batch, max_accepts, max_sweeps, time_budget, target_score,
                                       C.byref(prog))
         self._chk(st, "bm_search_batched", ok=(BM_OK, BM_TIMEOUT))
+        return prog, st
+
+    def kset_eval(self, k: int, sets, all_deltas: bool = False):
+        """Best permutation of each k-set: returns (best_delta, best_perm[, all])."""
+        sets = _i32(sets).reshape(-1)
+        ns = sets.shape[0] // k
+        best = np.zeros(ns, np.int64)
+        perm = np.zeros(ns * k, np.int32)
+        import math
+        alld = np.zeros(ns * math.factorial(k), np.int64) if all_deltas else None
+        self._chk(self.L.bm_kset_eval(self.h, k, _ptr(sets), ns, _ptr(best), _ptr(perm),
+                                      None if alld is None else _ptr(alld)), "bm_kset_eval")
+        perm = perm.reshape(ns, k)
+        if all_deltas:
+            return best, perm, alld.reshape(ns, -1)
+        return best, perm
+
+    def apply_sets(self, k: int, sets, perms, deltas=None) -> None:
+        sets, perms = _i32(sets).reshape(-1), _i32(perms).reshape(-1)
+        d = None if deltas is None else np.ascontiguousarray(np.asarray(deltas, np.int64))
+        self._chk(self.L.bm_apply_sets(self.h, k, _ptr(sets), _ptr(perms), None if d is None else _ptr(d),
+                                       sets.shape[0] // k), "bm_apply_sets")
+
+    def search_ksets(self, k: int, sets_per_launch: int, mode: int = 0, seed: int = 1, max_launches: int = -1,
+                     time_budget: float = 0.0, prog=None):
+        prog = prog or Progress()
+        st = self.L.bm_search_ksets(self.h, k, sets_per_launch, mode, seed, max_launches, time_budget,
+                                    C.byref(prog))
+        self._chk(st, "bm_search_ksets", ok=(BM_OK, BM_TIMEOUT))
         return prog, st
 
     def set_row_tiling(self, ctas_per_row: int = 0, threads: int = 0) -> None:

@@ -178,6 +178,38 @@ bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, int32_t nrows
                             int32_t rows_per_batch, int64_t max_accepts, int32_t max_sweeps,
                             double time_budget_s, int64_t target_score, bm_progress* prog);
 
+/* --------------------------------------------------- k-vertex permutations */
+
+/* Exact deltas of every permutation of small vertex sets (2 <= k <= 8):
+ * sets[i*k + a] is member a of set i.  For each set the best permutation
+ * (largest delta, the first in lexicographic order on ties; the identity,
+ * delta 0, when nothing improves) is returned as best_perm[i*k + a] = the
+ * member whose image member a takes, with its delta in best_delta[i].
+ * all_deltas (optional, nsets * k! entries) receives every permutation's
+ * delta in lexicographic order.  k = 3 gives the 3-vertex moves of
+ * calculateThreeNodeSwapKernel (src/graph-re-alignment-gpu-3-swap.cu:43-305);
+ * k = 4..8 the permutation sets of src/graph-alignment-permset-parallel.c:
+ * 304-363, with exact deltas for edges inside a set.  Host buffers. */
+bm_status bm_kset_eval(bm_ctx* ctx, int32_t k, const int32_t* sets, int64_t nsets, int64_t* best_delta,
+                       int32_t* best_perm, int64_t* all_deltas);
+/* Device-pointer form; *d_status (device int32, zeroed by the caller) gets bit
+ * 0 for a rejected set (bad or repeated id) and bit 1 for a set with more than
+ * 256 A entries between its members (both evaluated as delta 0). */
+bm_status bm_kset_eval_dev(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t nsets,
+                           int64_t* d_best_delta, int32_t* d_best_perm, int32_t* d_status);
+/* Apply permutations of pairwise independent sets (no shared vertex, no A
+ * edge between two sets), as apply_permutation does for triples
+ * (src/graph-re-alignment-gpu-3-swap.cu:925-956).  Host buffers. */
+bm_status bm_apply_sets(bm_ctx* ctx, int32_t k, const int32_t* sets, const int32_t* perms,
+                        const int64_t* deltas, int32_t nsets);
+/* Search by k-vertex permutations: each launch draws sets_per_launch sets
+ * (mode 0: k random distinct vertices; mode 1, k = 3 only: a path u - x - y of
+ * A), evaluates all k! permutations of each, and applies a greedy independent
+ * subset of the improving ones (descending delta).  Sets come from
+ * Philox4x32-10 keyed by seed, so a run is reproducible. */
+bm_status bm_search_ksets(bm_ctx* ctx, int32_t k, int32_t sets_per_launch, int32_t mode, uint64_t seed,
+                          int64_t max_launches, double time_budget_s, bm_progress* prog);
+
 /* ------------------------------------------------- annealing chains */
 
 /* A batch of graph pairs of uneven size, for many independent annealing

@@ -275,3 +275,36 @@ int64_t orc_sa_run(const orc_graph* gm, const orc_graph* gf, int32_t* mapping, u
  * error-bound tests. */
 void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) { bm_philox4x32_10(ctr, key, out); }
 double orc_exp(double x) { return bm_exp(x); }
+
+/* Delta of a permutation of a vertex set: member i takes the image of member
+ * perm[i].  Follows calculate_permutation_delta
+ * (src/graph-alignment-permset-parallel.c:304-339) — every A entry touching
+ * the set, old contribution out, new one in — except that an entry between two
+ * members is counted once (from its source's out-list), where the reference
+ * counts it from both ends.  Exact, including self-loops. */
+int64_t orc_perm_delta(const orc_graph* gm, const orc_graph* gf, const int32_t* mapping, const int32_t* verts,
+                       int32_t k, const int32_t* perm) {
+    int32_t newf[16];
+    for (int32_t i = 0; i < k; i++) newf[i] = mapping[verts[perm[i]]];
+    int64_t delta = 0;
+    for (int32_t i = 0; i < k; i++) {
+        const int32_t v = verts[i];
+        for (int32_t j = gm->optr[v]; j < gm->optr[v + 1]; j++) {
+            const int32_t x = gm->oto[j], w = gm->ow[j];
+            int32_t xm = -1;
+            for (int32_t q = 0; q < k; q++)
+                if (verts[q] == x) xm = q;
+            const int32_t nx = xm >= 0 ? newf[xm] : mapping[x];
+            delta += MIN(w, mat(gf, newf[i], nx)) - MIN(w, mat(gf, mapping[v], mapping[x]));
+        }
+        for (int32_t j = gm->iptr[v]; j < gm->iptr[v + 1]; j++) {
+            const int32_t x = gm->ifrom[j], w = gm->iw[j];
+            int32_t xm = -1;
+            for (int32_t q = 0; q < k; q++)
+                if (verts[q] == x) xm = q;
+            if (xm >= 0) continue; /* counted from x's out-list */
+            delta += MIN(w, mat(gf, mapping[x], newf[i])) - MIN(w, mat(gf, mapping[x], mapping[v]));
+        }
+    }
+    return delta;
+}

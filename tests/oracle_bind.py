@@ -49,6 +49,8 @@ def oracle_lib() -> C.CDLL:
         L.orc_rows_omp.argtypes = [vp, vp, vp, vp, C.c_int32, vp, C.c_int32]
         L.orc_pairs.restype = None
         L.orc_pairs.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
+        L.orc_perm_delta.restype = C.c_int64
+        L.orc_perm_delta.argtypes = [vp, vp, vp, vp, C.c_int32, vp]
         L.orc_sa_run.restype = C.c_int64
         L.orc_sa_run.argtypes = [vp, vp, vp, C.c_uint64, C.c_int64, C.c_double, C.c_double, C.POINTER(C.c_int64)]
         _orc = L
@@ -132,6 +134,10 @@ class Oracle:
         out = np.zeros((rows.shape[0], self.n + 1), np.int64)
         self.L.orc_rows_omp(self.gm, self.gf, _p(pi), _p(rows), rows.shape[0], _p(out), threads)
         return out
+
+    def perm_delta(self, pi, verts, perm) -> int:
+        pi, verts, perm = _i32(pi), _i32(verts), _i32(perm)
+        return int(self.L.orc_perm_delta(self.gm, self.gf, _p(pi), _p(verts), verts.shape[0], _p(perm)))
 
     def sa(self, pi, key, steps, t0=5.0, t_end=0.01):
         """Replay of one annealing chain; returns (pi, score, accepts)."""
