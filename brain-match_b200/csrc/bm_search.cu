@@ -485,3 +485,171 @@ extern "C" bm_status bm_search_ksets(bm_ctx* ctx, int32_t k, int32_t sets_per_la
     if (s != BM_OK) return s;
     return ret;
 }
+
+// ------------------------------------------------------------- perturbation
+
+// k disjoint swaps selected[i] <-> selected[i+k] over 2k distinct vertices, as
+// random_swap_k_vertices (src/graph-re-alignment-gpu.cu:763-810; weighted
+// variant src/graph-re-alignment-gpu-swap.cu:767-887): the first k vertices
+// uniformly (mode 0) or with probability proportional to 7 * out-weight +
+// 3 * in-weight of A (mode 1, the reference's 0.7/0.3 score in integers), the
+// next k uniformly.  Draws come from Philox4x32-10 keyed by seed with
+// `counter` as the stream position, instead of rand() seeded by the clock.
+// Each swap's exact delta is computed and the swap applied in stream order,
+// so the tracked score stays exact.
+extern "C" bm_status bm_perturb(bm_ctx* ctx, int32_t k, int32_t mode, uint64_t seed, uint64_t counter,
+                                int32_t* changed, int64_t* total_delta) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    const int32_t n = ctx->n;
+    if (k < 1 || 2 * (int64_t)k > n) return bm_fail(ctx, BM_INVALID_ARG, "need 1 <= k and 2k <= n");
+    if (mode != 0 && mode != 1) return bm_fail(ctx, BM_INVALID_ARG, "mode must be 0 (uniform) or 1 (weighted)");
+    std::vector<int32_t> sel;
+    std::vector<char> used((size_t)n + 1, 0);
+    uint32_t word[4];
+    int have = 0;
+    uint64_t ctr = counter;
+    auto next = [&]() -> uint32_t {
+        if (have == 0) {
+            const uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), 0x70657274u, 0u};
+            const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+            bm_philox4x32_10(c, key, word);
+            ctr++;
+            have = 4;
+        }
+        return word[--have];
+    };
+    if (mode == 1) {
+        std::vector<int64_t> cum((size_t)n + 1, 0);
+        for (int32_t v = 1; v <= n; v++) {
+            int64_t ow = 0, iw = 0;
+            for (int32_t j = ctx->hA_optr[(size_t)v]; j < ctx->hA_optr[(size_t)v + 1]; j++) ow += bm_ew(ctx->hA_oent[(size_t)j]);
+            for (int32_t j = ctx->hA_iptr[(size_t)v]; j < ctx->hA_iptr[(size_t)v + 1]; j++) iw += bm_ew(ctx->hA_ient[(size_t)j]);
+            cum[(size_t)v] = cum[(size_t)v - 1] + 7 * ow + 3 * iw;
+        }
+        const int64_t total = cum[(size_t)n];
+        while ((int32_t)sel.size() < k) {
+            int32_t v;
+            if (total > 0) {
+                const uint64_t r64 = ((uint64_t)next() << 32) | next();
+                const int64_t r = (int64_t)(r64 % (uint64_t)total);
+                v = (int32_t)(std::upper_bound(cum.begin() + 1, cum.end(), r) - cum.begin());
+            } else {
+                v = 1 + (int32_t)(next() % (uint32_t)n);
+            }
+            if (used[(size_t)v]) {
+                // weights of used vertices stay in the table; step to the next unused one
+                int32_t w = v;
+                do { w = w % n + 1; } while (used[(size_t)w]);
+                v = w;
+            }
+            used[(size_t)v] = 1;
+            sel.push_back(v);
+        }
+    }
+    while ((int32_t)sel.size() < 2 * k) {
+        const int32_t v = 1 + (int32_t)(next() % (uint32_t)n);
+        if (used[(size_t)v]) continue;
+        used[(size_t)v] = 1;
+        sel.push_back(v);
+    }
+    const size_t pb = ((size_t)k * 2 * sizeof(int32_t) + 255) & ~(size_t)255;
+    if ((s = bm_stage(ctx, pb + sizeof(int64_t) * (size_t)k)) != BM_OK) return s;
+    int32_t* d_pairs = (int32_t*)ctx->stage;
+    int64_t* d_delta = (int64_t*)((char*)ctx->stage + pb);
+    std::vector<int32_t> pairs((size_t)2 * k);
+    for (int32_t i = 0; i < k; i++) {
+        pairs[(size_t)2 * i] = sel[(size_t)i];
+        pairs[(size_t)2 * i + 1] = sel[(size_t)i + k];
+    }
+    BM_CUDA(ctx, cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int32_t) * 2 * (size_t)k, cudaMemcpyHostToDevice, ctx->stream));
+    for (int32_t i = 0; i < k; i++) {
+        if ((s = bm_launch_pairs(ctx, d_pairs + 2 * i, 1, d_delta + i)) != BM_OK) return s;
+        if ((s = bm_launch_apply(ctx, d_pairs + 2 * i, 1)) != BM_OK) return s;
+    }
+    std::vector<int64_t> deltas((size_t)k);
+    BM_CUDA(ctx, cudaMemcpyAsync(deltas.data(), d_delta, sizeof(int64_t) * (size_t)k, cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int64_t sum = 0;
+    for (int64_t d : deltas) sum += d;
+    ctx->score += sum;
+    if (changed)
+        for (int32_t i = 0; i < 2 * k; i++) changed[i] = sel[(size_t)i];
+    if (total_delta) *total_delta = sum;
+    return BM_OK;
+}
+
+// Batched search with perturbation restarts, the driver pattern of
+// src/graph-re-alignment-gpu.cu:1004-1028: when a pass finds no improving swap,
+// perturb with k swaps and continue; the best mapping seen is kept and restored
+// at the end.
+extern "C" bm_status bm_search_restarts(bm_ctx* ctx, const int32_t* row_order, int32_t nrows, int32_t rows_per_batch,
+                                        int32_t k_perturb, int32_t mode, uint64_t seed, int32_t max_restarts,
+                                        double time_budget_s, bm_progress* prog, int64_t* best_score) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (!prog) return bm_fail(ctx, BM_INVALID_ARG, "progress struct required");
+    const auto t0 = clk::now();
+    std::vector<int32_t> best_pi((size_t)ctx->n + 1);
+    int64_t best = ctx->score;
+    BM_CUDA(ctx, cudaMemcpy(best_pi.data(), ctx->pi, sizeof(int32_t) * best_pi.size(), cudaMemcpyDeviceToHost));
+    bm_status ret = BM_OK;
+    for (int32_t r = 0;; r++) {
+        const double left = time_budget_s > 0 ? time_budget_s - secs_since(t0) : 0;
+        if (time_budget_s > 0 && left <= 0) { ret = BM_TIMEOUT; break; }
+        bm_progress p = *prog;
+        p.next_row_pos = 0;
+        p.converged = 0;
+        s = bm_search_batched(ctx, row_order, nrows, rows_per_batch, -1, -1, left, 0, &p);
+        const double secs = prog->seconds;
+        *prog = p;
+        prog->seconds = secs;
+        if (s == BM_TIMEOUT) { ret = BM_TIMEOUT; }
+        else if (s != BM_OK) return s;
+        if (ctx->score > best) {
+            best = ctx->score;
+            BM_CUDA(ctx, cudaMemcpy(best_pi.data(), ctx->pi, sizeof(int32_t) * best_pi.size(), cudaMemcpyDeviceToHost));
+        }
+        if (ret == BM_TIMEOUT || r >= max_restarts) break;
+        if ((s = bm_perturb(ctx, k_perturb, mode, seed, (uint64_t)r << 20, nullptr, nullptr)) != BM_OK) return s;
+    }
+    if (ctx->score != best) {
+        // restore the best mapping seen
+        best_pi[0] = 0;
+        if ((s = bm_set_mapping(ctx, best_pi.data())) != BM_OK) return s;
+    }
+    prog->score = ctx->score;
+    prog->seconds += secs_since(t0);
+    if (best_score) *best_score = best;
+    return ret;
+}
+
+// The deterministic selection every rank of a sharded search runs on the same
+// gathered candidate list: descending delta, then ascending position in the
+// list; a candidate is taken when neither endpoint lies in the closed A
+// neighbourhood of an endpoint already taken.
+extern "C" bm_status bm_select_independent(bm_ctx* ctx, const int32_t* pairs, const int64_t* deltas, int32_t count,
+                                           int32_t* chosen, int32_t* nchosen) {
+    if (!ctx || count < 0 || (count > 0 && (!pairs || !deltas || !chosen)) || !nchosen) return BM_INVALID_ARG;
+    if (!ctx->g[0].loaded) return bm_fail(ctx, BM_INVALID_ARG, "graph A not set");
+    const int32_t n = ctx->n;
+    std::vector<int32_t> order;
+    for (int32_t i = 0; i < count; i++) {
+        if (pairs[2 * i] < 1 || pairs[2 * i] > n || pairs[2 * i + 1] < 1 || pairs[2 * i + 1] > n)
+            return bm_fail(ctx, BM_INVALID_ARG, "candidate %d: id outside 1..%d", i, n);
+        if (deltas[i] > 0 && pairs[2 * i] != pairs[2 * i + 1]) order.push_back(i);
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return deltas[a] > deltas[b]; });
+    Marks mk;
+    mk.reset(n);
+    int32_t c = 0;
+    for (int32_t i : order) {
+        const int32_t u = pairs[2 * i], v = pairs[2 * i + 1];
+        if (mk.marked(u) || mk.marked(v)) continue;
+        mk.mark_closed(ctx, u);
+        mk.mark_closed(ctx, v);
+        chosen[c++] = i;
+    }
+    *nchosen = c;
+    return BM_OK;
+}

@@ -183,3 +183,53 @@ int64_t bm_host_score(const bm_edges* A, const bm_edges* B, const int32_t* pi) {
     free(val);
     return s;
 }
+
+/* ------------------------------------------- independent-subset selection */
+
+typedef struct { int64_t d; int32_t i; } dsel;
+
+static int cmp_dsel(const void* a, const void* b) {
+    const dsel* x = (const dsel*)a;
+    const dsel* y = (const dsel*)b;
+    if (x->d != y->d) return x->d > y->d ? -1 : 1;
+    return x->i < y->i ? -1 : (x->i > y->i);
+}
+
+int bm_select_independent_host(const bm_edges* A, const int32_t* pairs, const int64_t* deltas, int32_t count,
+                               int32_t* chosen, int32_t* nchosen) {
+    const int32_t n = A->n;
+    /* undirected closed neighbourhoods as a CSR over both edge directions */
+    int32_t* deg = (int32_t*)calloc((size_t)n + 2, sizeof(int32_t));
+    int32_t* adj = (int32_t*)malloc(sizeof(int32_t) * (size_t)(2 * A->m + 1));
+    dsel* ord = (dsel*)malloc(sizeof(dsel) * (size_t)(count > 0 ? count : 1));
+    uint8_t* mark = (uint8_t*)calloc((size_t)n + 1, 1);
+    if (!deg || !adj || !ord || !mark) { free(deg); free(adj); free(ord); free(mark); return -1; }
+    for (int64_t e = 0; e < A->m; e++) { deg[A->src[e] + 1]++; deg[A->dst[e] + 1]++; }
+    for (int32_t v = 1; v <= n + 1; v++) deg[v] += deg[v - 1];
+    int32_t* fill = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n + 1));
+    memcpy(fill, deg, sizeof(int32_t) * ((size_t)n + 1));
+    for (int64_t e = 0; e < A->m; e++) {
+        if (A->w[e] == 0) continue;
+        adj[fill[A->src[e]]++] = A->dst[e];
+        adj[fill[A->dst[e]]++] = A->src[e];
+    }
+    int32_t k = 0;
+    for (int32_t i = 0; i < count; i++)
+        if (deltas[i] > 0 && pairs[2 * i] != pairs[2 * i + 1]) { ord[k].d = deltas[i]; ord[k].i = i; k++; }
+    qsort(ord, (size_t)k, sizeof(dsel), cmp_dsel);
+    int32_t c = 0;
+    for (int32_t t = 0; t < k; t++) {
+        const int32_t i = ord[t].i, u = pairs[2 * i], v = pairs[2 * i + 1];
+        if (mark[u] || mark[v]) continue;
+        const int32_t ends[2] = {u, v};
+        for (int q = 0; q < 2; q++) {
+            const int32_t x = ends[q];
+            mark[x] = 1;
+            for (int32_t j = deg[x]; j < fill[x]; j++) mark[adj[j]] = 1;
+        }
+        chosen[c++] = i;
+    }
+    *nchosen = c;
+    free(deg); free(adj); free(ord); free(mark); free(fill);
+    return 0;
+}

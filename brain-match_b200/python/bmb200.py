@@ -135,6 +135,9 @@ def cuda_lib() -> C.CDLL:
             "bm_apply_sets": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.c_int32]),
             "bm_search_ksets": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int64, C.c_double,
                                           C.POINTER(Progress)]),
+            "bm_perturb": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, vp, C.POINTER(C.c_int64)]),
+            "bm_search_restarts": (C.c_int, [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
+                                             C.c_int32, C.c_double, C.POINTER(Progress), C.POINTER(C.c_int64)]),
             "bm_batch_create": (C.c_int, [vp, C.POINTER(vp)]),
             "bm_batch_destroy": (None, [vp]),
             "bm_batch_add_pair": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, vp, C.c_int64, vp, vp, vp,
@@ -477,6 +480,24 @@ class Engine:
                                     C.byref(prog))
         self._chk(st, "bm_search_ksets", ok=(BM_OK, BM_TIMEOUT))
         return prog, st
+
+    def perturb(self, k: int, mode: int = 0, seed: int = 1, counter: int = 0):
+        """k disjoint random swaps; returns (changed vertices (2k), total delta)."""
+        ch = np.zeros(2 * k, np.int32)
+        d = C.c_int64()
+        self._chk(self.L.bm_perturb(self.h, k, mode, seed, counter, _ptr(ch), C.byref(d)), "bm_perturb")
+        return ch, d.value
+
+    def search_restarts(self, rows=None, rows_per_batch=0, k_perturb=5, mode=0, seed=1, max_restarts=3,
+                        time_budget=0.0, prog=None):
+        prog = prog or Progress()
+        best = C.c_int64()
+        r = None if rows is None else _i32(rows)
+        st = self.L.bm_search_restarts(self.h, None if r is None else _ptr(r), 0 if r is None else r.shape[0],
+                                       rows_per_batch, k_perturb, mode, seed, max_restarts, time_budget,
+                                       C.byref(prog), C.byref(best))
+        self._chk(st, "bm_search_restarts", ok=(BM_OK, BM_TIMEOUT))
+        return prog, best.value, st
 
     def set_row_tiling(self, ctas_per_row: int = 0, threads: int = 0) -> None:
         self._chk(self.L.bm_set_row_tiling(self.h, ctas_per_row, threads), "bm_set_row_tiling")

@@ -178,6 +178,35 @@ bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, int32_t nrows
                             int32_t rows_per_batch, int64_t max_accepts, int32_t max_sweeps,
                             double time_budget_s, int64_t target_score, bm_progress* prog);
 
+/* Deterministic independent-subset selection of candidate swaps (pairs[2i],
+ * pairs[2i+1]) with deltas[i]: among delta > 0, in descending delta then
+ * ascending index, a swap is taken when neither endpoint lies in the closed A
+ * neighbourhood of an endpoint already taken (the independence rule of
+ * src/independent-hungarian/hungarianSubset.c:657-740).  Every rank of a
+ * sharded search runs it on the same gathered list, so the ranks apply the
+ * same swaps and keep identical mappings.  chosen gets candidate indices. */
+bm_status bm_select_independent(bm_ctx* ctx, const int32_t* pairs, const int64_t* deltas, int32_t count,
+                                int32_t* chosen, int32_t* nchosen);
+
+/* Perturbation: k disjoint swaps selected[i] <-> selected[i+k] over 2k
+ * distinct vertices (random_swap_k_vertices, src/graph-re-alignment-gpu.cu:
+ * 763-810); mode 0 draws all 2k uniformly, mode 1 draws the first k with
+ * probability proportional to 7*out-weight + 3*in-weight of A (the weighted
+ * variant of src/graph-re-alignment-gpu-swap.cu:767-887), the next k
+ * uniformly.  Draws come from Philox4x32-10 keyed by seed, starting at stream
+ * position `counter`.  The exact deltas are applied in order; changed (2k
+ * ints, optional) receives the vertices, total_delta their sum. */
+bm_status bm_perturb(bm_ctx* ctx, int32_t k, int32_t mode, uint64_t seed, uint64_t counter,
+                     int32_t* changed, int64_t* total_delta);
+/* Batched search with perturbation restarts (the pattern of
+ * src/graph-re-alignment-gpu.cu:1004-1028): converge with bm_search_batched,
+ * perturb with k_perturb swaps, repeat up to max_restarts times or until the
+ * budget ends; the best mapping seen is restored at the end and its score
+ * returned in best_score. */
+bm_status bm_search_restarts(bm_ctx* ctx, const int32_t* row_order, int32_t nrows, int32_t rows_per_batch,
+                             int32_t k_perturb, int32_t mode, uint64_t seed, int32_t max_restarts,
+                             double time_budget_s, bm_progress* prog, int64_t* best_score);
+
 /* --------------------------------------------------- k-vertex permutations */
 
 /* Exact deltas of every permutation of small vertex sets (2 <= k <= 8):

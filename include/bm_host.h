@@ -102,6 +102,14 @@ int64_t bm_host_score(const bm_edges* A, const bm_edges* B, const int32_t* pi);
 /* Bijection check of pi on 1..n: 0 if valid, else the first bad id (> 0). */
 int32_t bm_check_bijection(int32_t n, const int32_t* pi);
 
+/* The deterministic selection of a sharded search (the same rule as
+ * bm_select_independent in bm_cuda.h, on the host): among candidates with
+ * delta > 0, in descending delta then ascending index, take a swap when
+ * neither endpoint lies in the closed A neighbourhood of an endpoint already
+ * taken.  chosen receives candidate indices, *nchosen their count. */
+int bm_select_independent_host(const bm_edges* A, const int32_t* pairs, const int64_t* deltas, int32_t count,
+                               int32_t* chosen, int32_t* nchosen);
+
 /* SplitMix64 step and a uniform double in [0,1) — the generator's RNG. */
 uint64_t bm_splitmix64(uint64_t* state);
 
