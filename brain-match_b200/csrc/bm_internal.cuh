@@ -18,6 +18,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -115,6 +116,26 @@ bm_status bm_cuda_fail(bm_ctx* ctx, cudaError_t e, const char* what);
 bm_status bm_stage(bm_ctx* ctx, size_t bytes);
 bm_status bm_hstage(bm_ctx* ctx, size_t bytes);
 bm_status bm_require_mapped(bm_ctx* ctx);
+
+// Stamps of closed A neighbourhoods (host copy of A's lists): the test that
+// keeps a batch of swaps independent (no shared vertex, no A edge between
+// their endpoint sets), so that their deltas add up exactly.
+struct BmMarks {
+    std::vector<uint32_t> stamp;
+    uint32_t cur = 0;
+    void reset(int32_t n) {
+        if (stamp.size() != (size_t)n + 1) { stamp.assign((size_t)n + 1, 0); cur = 0; }
+        if (++cur == 0) { std::fill(stamp.begin(), stamp.end(), 0); cur = 1; }
+    }
+    bool marked(int32_t v) const { return stamp[(size_t)v] == cur; }
+    void mark_closed(const bm_ctx* ctx, int32_t v) {
+        stamp[(size_t)v] = cur;
+        for (int32_t j = ctx->hA_optr[(size_t)v]; j < ctx->hA_optr[(size_t)v + 1]; j++)
+            stamp[(size_t)bm_eid(ctx->hA_oent[(size_t)j])] = cur;
+        for (int32_t j = ctx->hA_iptr[(size_t)v]; j < ctx->hA_iptr[(size_t)v + 1]; j++)
+            stamp[(size_t)bm_eid(ctx->hA_ient[(size_t)j])] = cur;
+    }
+};
 
 inline GView gview(const DevGraph& g) { return GView{g.out_ptr, g.in_ptr, g.out_ent, g.in_ent, g.self_w}; }
 inline HashView hview(const DevGraph& g) { return HashView{g.hash, g.hash_log2, g.n + 1}; }

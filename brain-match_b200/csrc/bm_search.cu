@@ -105,24 +105,6 @@ bm_status load_order(bm_ctx* ctx, const int32_t* row_order, int32_t nrows, std::
     return BM_OK;
 }
 
-// Marks of closed A neighbourhoods, for the independence test.
-struct Marks {
-    std::vector<uint32_t> stamp;
-    uint32_t cur = 0;
-    void reset(int32_t n) {
-        if (stamp.size() != (size_t)n + 1) { stamp.assign((size_t)n + 1, 0); cur = 0; }
-        if (++cur == 0) { std::fill(stamp.begin(), stamp.end(), 0); cur = 1; }
-    }
-    bool marked(int32_t v) const { return stamp[(size_t)v] == cur; }
-    void mark_closed(const bm_ctx* ctx, int32_t v) {
-        stamp[(size_t)v] = cur;
-        for (int32_t j = ctx->hA_optr[(size_t)v]; j < ctx->hA_optr[(size_t)v + 1]; j++)
-            stamp[(size_t)bm_eid(ctx->hA_oent[(size_t)j])] = cur;
-        for (int32_t j = ctx->hA_iptr[(size_t)v]; j < ctx->hA_iptr[(size_t)v + 1]; j++)
-            stamp[(size_t)bm_eid(ctx->hA_ient[(size_t)j])] = cur;
-    }
-};
-
 }  // namespace
 
 extern "C" bm_status bm_apply_swaps(bm_ctx* ctx, const int32_t* pairs, const int64_t* deltas, int32_t k) {
@@ -131,7 +113,7 @@ extern "C" bm_status bm_apply_swaps(bm_ctx* ctx, const int32_t* pairs, const int
     if (k < 0 || (k > 0 && !pairs)) return bm_fail(ctx, BM_INVALID_ARG, "bad swap buffers");
     if (k == 0) return BM_OK;
     const int32_t n = ctx->n;
-    Marks mk;
+    BmMarks mk;
     mk.reset(n);
     for (int32_t i = 0; i < k; i++) {
         const int32_t a = pairs[2 * i], b = pairs[2 * i + 1];
@@ -246,7 +228,7 @@ extern "C" bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, in
     SchedBufs b;
     if ((s = sched_bufs(ctx, R, &b)) != BM_OK) return s;
     std::vector<int32_t> cand;
-    Marks mk;
+    BmMarks mk;
     const auto t0 = clk::now();
     int32_t pos = prog->next_row_pos;
     if (pos < 0 || pos >= nr) pos = 0;
@@ -320,7 +302,7 @@ extern "C" bm_status bm_apply_sets(bm_ctx* ctx, int32_t k, const int32_t* sets, 
     if (nsets < 0 || (nsets > 0 && (!sets || !perms))) return bm_fail(ctx, BM_INVALID_ARG, "bad set buffers");
     if (nsets == 0) return BM_OK;
     const int32_t n = ctx->n;
-    Marks mk;
+    BmMarks mk;
     mk.reset(n);
     for (int32_t i = 0; i < nsets; i++) {
         int used = 0;
@@ -428,7 +410,7 @@ extern "C" bm_status bm_search_ksets(bm_ctx* ctx, int32_t k, int32_t sets_per_la
     int32_t* h_perm = (int32_t*)(h + b_sets);
     long long* h_best = (long long*)(h + 2 * b_sets);
     std::vector<int32_t> order((size_t)S), ap_sets, ap_perms;
-    Marks mk;
+    BmMarks mk;
     const auto t0 = clk::now();
     bm_status ret = BM_OK;
     for (int64_t l = 0; max_launches < 0 || l < max_launches; l++) {
@@ -640,7 +622,7 @@ extern "C" bm_status bm_select_independent(bm_ctx* ctx, const int32_t* pairs, co
         if (deltas[i] > 0 && pairs[2 * i] != pairs[2 * i + 1]) order.push_back(i);
     }
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return deltas[a] > deltas[b]; });
-    Marks mk;
+    BmMarks mk;
     mk.reset(n);
     int32_t c = 0;
     for (int32_t i : order) {

@@ -65,6 +65,23 @@ class SaStats(C.Structure):
     _fields_ = [("candidates", C.c_int32), ("launches", C.c_int64), ("seconds", C.c_double)]
 
 
+class LearnedParams(C.Structure):
+    _fields_ = [("topk", C.c_int32), ("rows_per_batch", C.c_int32), ("refresh_batches", C.c_int32),
+                ("uniform", C.c_int32), ("exact_fallback", C.c_int32), ("train_every", C.c_int32),
+                ("train_batch", C.c_int32), ("lr", C.c_float), ("weight_decay", C.c_float), ("seed", C.c_uint64),
+                ("max_accepts", C.c_int64), ("max_sweeps", C.c_int32), ("time_budget_s", C.c_double),
+                ("target_score", C.c_int64)]
+
+
+class LearnedStats(C.Structure):
+    _fields_ = [("proposals", C.c_int64), ("hits", C.c_int64), ("exact_passes", C.c_int64),
+                ("train_steps", C.c_int64), ("t_propose", C.c_double), ("t_exact", C.c_double),
+                ("t_train", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GenParams(C.Structure):
     _fields_ = [("n", C.c_int32), ("m_target", C.c_int64), ("degree_model", C.c_int32), ("alpha", C.c_double),
                 ("max_degree", C.c_int32), ("weight_model", C.c_int32), ("geo_p", C.c_double),
@@ -145,6 +162,28 @@ def cuda_lib() -> C.CDLL:
             "bm_sa_run": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.POINTER(SaParams), vp, vp, vp, C.POINTER(SaStats)]),
             "bm_sa_layout_size": (C.c_int64, [vp, C.c_int32, vp]),
             "bm_get_row_tiling": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "bm_mlp_create": (C.c_int, [vp, C.c_uint64, C.POINTER(vp)]),
+            "bm_mlp_destroy": (None, [vp]),
+            "bm_mlp_num_params": (C.c_int32, []),
+            "bm_mlp_get_params": (C.c_int, [vp, vp]),
+            "bm_mlp_set_params": (C.c_int, [vp, vp]),
+            "bm_mlp_set_backend": (C.c_int, [vp, C.c_int32]),
+            "bm_mlp_refresh_features": (C.c_int, [vp]),
+            "bm_mlp_get_features": (C.c_int, [vp, vp]),
+            "bm_mlp_pair_features": (C.c_int, [vp, vp, C.c_int64, vp]),
+            "bm_mlp_score_pairs": (C.c_int, [vp, vp, C.c_int64, vp]),
+            "bm_mlp_score_features": (C.c_int, [vp, vp, C.c_int64, vp]),
+            "bm_mlp_score_rows": (C.c_int, [vp, vp, C.c_int32, vp]),
+            "bm_mlp_rows_topk": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp]),
+            "bm_mlp_gradients": (C.c_int, [vp, vp, vp, C.c_int64, vp, C.POINTER(C.c_float)]),
+            "bm_mlp_adamw_step": (C.c_int, [vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.POINTER(C.c_float)]),
+            "bm_mlp_reserve_records": (C.c_int, [vp, C.c_int64]),
+            "bm_mlp_collect_rows": (C.c_int, [vp, vp, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_int64)]),
+            "bm_mlp_clear_records": (C.c_int, [vp]),
+            "bm_mlp_fit": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64,
+                                     C.POINTER(C.c_float)]),
+            "bm_search_learned": (C.c_int, [vp, vp, vp, C.c_int32, C.POINTER(LearnedParams), C.POINTER(Progress),
+                                            C.POINTER(LearnedStats)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -605,6 +644,141 @@ class Batch:
     def close(self):
         if self.h:
             self.L.bm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+MLP_IN = 24
+MLP_FEATURES = 12
+
+
+class Mlp:
+    """Learned partner proposals (bm_mlp) bound to an Engine's graphs."""
+
+    def __init__(self, eng: Engine, seed: int = 1):
+        self.eng = eng
+        self.L = eng.L
+        h = C.c_void_p()
+        eng._chk(self.L.bm_mlp_create(eng.h, seed, C.byref(h)), "bm_mlp_create")
+        self.h = h
+        self.n = eng.n
+        self.nparams = int(self.L.bm_mlp_num_params())
+        import weakref
+        eng._children.append(weakref.ref(self))
+
+    def _chk(self, st, what, ok=(BM_OK,)):
+        return self.eng._chk(st, what, ok)
+
+    def params(self) -> np.ndarray:
+        w = np.zeros(self.nparams, np.float32)
+        self._chk(self.L.bm_mlp_get_params(self.h, _ptr(w)), "bm_mlp_get_params")
+        return w
+
+    def set_params(self, w) -> None:
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.float32))
+        assert w.shape == (self.nparams,)
+        self._chk(self.L.bm_mlp_set_params(self.h, _ptr(w)), "bm_mlp_set_params")
+
+    def set_backend(self, backend: int) -> None:
+        self._chk(self.L.bm_mlp_set_backend(self.h, backend), "bm_mlp_set_backend")
+
+    def refresh_features(self) -> None:
+        self._chk(self.L.bm_mlp_refresh_features(self.h), "bm_mlp_refresh_features")
+
+    def features(self) -> np.ndarray:
+        t = np.zeros((self.n + 1, MLP_FEATURES), np.float32)
+        self._chk(self.L.bm_mlp_get_features(self.h, _ptr(t)), "bm_mlp_get_features")
+        return t
+
+    def pair_features(self, pairs) -> np.ndarray:
+        p = _i32(pairs).reshape(-1, 2)
+        out = np.zeros((p.shape[0], MLP_IN), np.float32)
+        self._chk(self.L.bm_mlp_pair_features(self.h, _ptr(p), p.shape[0], _ptr(out)), "bm_mlp_pair_features")
+        return out
+
+    def score_pairs(self, pairs) -> np.ndarray:
+        p = _i32(pairs).reshape(-1, 2)
+        out = np.zeros(p.shape[0], np.float32)
+        self._chk(self.L.bm_mlp_score_pairs(self.h, _ptr(p), p.shape[0], _ptr(out)), "bm_mlp_score_pairs")
+        return out
+
+    def score_features(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float32).reshape(-1, MLP_IN))
+        out = np.zeros(x.shape[0], np.float32)
+        self._chk(self.L.bm_mlp_score_features(self.h, _ptr(x), x.shape[0], _ptr(out)), "bm_mlp_score_features")
+        return out
+
+    def score_rows(self, rows) -> np.ndarray:
+        r = _i32(rows)
+        out = np.zeros((r.shape[0], self.n), np.float32)
+        self._chk(self.L.bm_mlp_score_rows(self.h, _ptr(r), r.shape[0], _ptr(out)), "bm_mlp_score_rows")
+        return out
+
+    def rows_topk(self, rows, K: int = 64):
+        r = _i32(rows)
+        v = np.zeros((r.shape[0], K), np.int32)
+        sc = np.zeros((r.shape[0], K), np.float32)
+        self._chk(self.L.bm_mlp_rows_topk(self.h, _ptr(r), r.shape[0], K, _ptr(v), _ptr(sc)), "bm_mlp_rows_topk")
+        return v, sc
+
+    def gradients(self, x, y):
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float32).reshape(-1, MLP_IN))
+        y = np.ascontiguousarray(np.asarray(y, dtype=np.float32))
+        g = np.zeros(self.nparams, np.float32)
+        loss = C.c_float()
+        self._chk(self.L.bm_mlp_gradients(self.h, _ptr(x), _ptr(y), x.shape[0], _ptr(g), C.byref(loss)),
+                  "bm_mlp_gradients")
+        return g, loss.value
+
+    def adamw_step(self, x, y, lr=1e-3, weight_decay=0.0) -> float:
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float32).reshape(-1, MLP_IN))
+        y = np.ascontiguousarray(np.asarray(y, dtype=np.float32))
+        loss = C.c_float()
+        self._chk(self.L.bm_mlp_adamw_step(self.h, _ptr(x), _ptr(y), x.shape[0], lr, weight_decay, C.byref(loss)),
+                  "bm_mlp_adamw_step")
+        return loss.value
+
+    def reserve_records(self, capacity: int) -> None:
+        self._chk(self.L.bm_mlp_reserve_records(self.h, capacity), "bm_mlp_reserve_records")
+
+    def collect_rows(self, rows, per_row: int = 64, seed: int = 1) -> int:
+        r = _i32(rows)
+        nrec = C.c_int64()
+        self._chk(self.L.bm_mlp_collect_rows(self.h, _ptr(r), r.shape[0], per_row, seed, C.byref(nrec)),
+                  "bm_mlp_collect_rows")
+        return nrec.value
+
+    def clear_records(self) -> None:
+        self._chk(self.L.bm_mlp_clear_records(self.h), "bm_mlp_clear_records")
+
+    def fit(self, steps: int, batch: int = 4096, lr: float = 1e-3, weight_decay: float = 0.0, seed: int = 1) -> float:
+        loss = C.c_float()
+        self._chk(self.L.bm_mlp_fit(self.h, steps, batch, lr, weight_decay, seed, C.byref(loss)), "bm_mlp_fit")
+        return loss.value
+
+    def search(self, rows=None, topk=64, rows_per_batch=0, refresh_batches=1, uniform=False, exact_fallback=True,
+               train_every=0, train_batch=4096, lr=1e-3, weight_decay=0.0, seed=1, max_accepts=-1, max_sweeps=-1,
+               time_budget=0.0, target_score=0, prog=None, stats=None):
+        """bm_search_learned; returns (status, Progress, LearnedStats)."""
+        prm = LearnedParams(topk, rows_per_batch, refresh_batches, int(bool(uniform)), int(bool(exact_fallback)),
+                            train_every, train_batch, lr, weight_decay, seed, max_accepts, max_sweeps, time_budget,
+                            target_score)
+        prog = prog or Progress()
+        stats = stats or LearnedStats()
+        r = None if rows is None else _i32(rows)
+        st = self.L.bm_search_learned(self.eng.h, self.h, None if r is None else _ptr(r),
+                                      0 if r is None else r.shape[0], C.byref(prm), C.byref(prog), C.byref(stats))
+        self._chk(st, "bm_search_learned", ok=(BM_OK, BM_TIMEOUT))
+        return st, prog, stats
+
+    def close(self):
+        if self.h:
+            self.L.bm_mlp_destroy(self.h)
             self.h = None
 
     def __del__(self):

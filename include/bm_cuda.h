@@ -299,6 +299,98 @@ bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32_t* chain_p
                             const int32_t* init_pi, const bm_sa_params* params, int32_t* final_pi,
                             int64_t* final_score, int64_t* accepts);
 
+/* ------------------------------------------------------ learned proposals */
+
+/* A 24 -> 128 -> 128 -> 1 MLP that scores swap partners v of a vertex u from
+ * structural features, trained on (candidate, exact delta) records.  No
+ * counterpart in the reference: its only guided proposal is the
+ * degree-weighted random swap of src/graph-re-alignment-gpu-swap.cu:767-887.
+ * It only proposes; every accepted swap is gated by the exact int64 delta.
+ * BF16 inputs, weights and activations, FP32 accumulation and FP32 master
+ * weights.  Parameters are packed as W1[24][128] b1[128] W2[128][128] b2[128]
+ * w3[128] b3 (W[i][j]: input i, output j), bm_mlp_num_params() floats.
+ * A model is bound to the context (and the graphs) it was created on. */
+typedef struct bm_mlp bm_mlp;
+
+bm_status bm_mlp_create(bm_ctx* ctx, uint64_t seed, bm_mlp** out);
+void bm_mlp_destroy(bm_mlp* m);
+int32_t bm_mlp_num_params(void);
+bm_status bm_mlp_get_params(bm_mlp* m, float* params);
+bm_status bm_mlp_set_params(bm_mlp* m, const float* params);
+/* Row scoring back end: 0 = tcgen05 tensor-core kernel (default), 1 = SIMT. */
+bm_status bm_mlp_set_backend(bm_mlp* m, int32_t backend);
+
+/* Recompute the per-vertex table (12 floats per vertex, row 0 zero) for the
+ * current mapping; read it back ((n+1)*12 floats). */
+bm_status bm_mlp_refresh_features(bm_mlp* m);
+bm_status bm_mlp_get_features(bm_mlp* m, float* table);
+/* The 24 features (BF16 values) of k pairs, from the current table. */
+bm_status bm_mlp_pair_features(bm_mlp* m, const int32_t* pairs, int64_t k, float* feats);
+
+/* Model scores: of k pairs (SIMT); of k explicit feature rows (k x 24, SIMT);
+ * of whole rows (nrows x n floats, partner v at r*n + v-1, -inf at v == u,
+ * by the selected back end). */
+bm_status bm_mlp_score_pairs(bm_mlp* m, const int32_t* pairs, int64_t k, float* scores);
+bm_status bm_mlp_score_features(bm_mlp* m, const float* x, int64_t k, float* scores);
+bm_status bm_mlp_score_rows(bm_mlp* m, const int32_t* rows, int32_t nrows, float* scores);
+/* The K (1..64) best-scored partners of each row, best first, ties by lower
+ * id; partners[r*K + j], scores optional. */
+bm_status bm_mlp_rows_topk(bm_mlp* m, const int32_t* rows, int32_t nrows, int32_t K, int32_t* partners,
+                           float* scores);
+
+/* Loss mean((out - y)^2) over k feature rows and its gradient
+ * (bm_mlp_num_params() floats), without updating the model. */
+bm_status bm_mlp_gradients(bm_mlp* m, const float* x, const float* y, int64_t k, float* grads, float* loss);
+/* One AdamW step (beta 0.9 / 0.999, eps 1e-8, decoupled weight decay) on
+ * explicit features and targets. */
+bm_status bm_mlp_adamw_step(bm_mlp* m, const float* x, const float* y, int64_t k, float lr, float weight_decay,
+                            float* loss);
+
+/* Training records (features under the mapping of the moment, target
+ * sign(d) * log1p(|d|) / 8 of the exact delta d) kept on the device in a ring.
+ * collect_rows evaluates whole rows with the exact row kernel and keeps per
+ * row up to per_row/2 improving partners plus uniform random partners;
+ * *nrecords = records held. */
+bm_status bm_mlp_reserve_records(bm_mlp* m, int64_t capacity);
+bm_status bm_mlp_collect_rows(bm_mlp* m, const int32_t* rows, int32_t nrows, int32_t per_row, uint64_t seed,
+                              int64_t* nrecords);
+bm_status bm_mlp_clear_records(bm_mlp* m);
+/* AdamW steps on random minibatches of the held records; *loss = loss of the
+ * last minibatch. */
+bm_status bm_mlp_fit(bm_mlp* m, int32_t steps, int32_t batch, float lr, float weight_decay, uint64_t seed,
+                     float* loss);
+
+typedef struct bm_learned_params {
+    int32_t topk;             /* partners proposed per row, 1..64 (0: 64) */
+    int32_t rows_per_batch;   /* rows per launch (0: 2 x SMs) */
+    int32_t refresh_batches;  /* feature table refreshed every this many batches (0: 1) */
+    int32_t uniform;          /* 1: uniform random partners instead of the model (the judge) */
+    int32_t exact_fallback;   /* 1: after a pass without accepts, an exact row pass decides convergence */
+    int32_t train_every;      /* online AdamW step every this many batches (0: no online training) */
+    int32_t train_batch;      /* records per online step (0: 4096) */
+    float lr, weight_decay;
+    uint64_t seed;
+    int64_t max_accepts;      /* < 0: unlimited */
+    int32_t max_sweeps;       /* < 0: unlimited */
+    double time_budget_s;     /* <= 0: none */
+    int64_t target_score;     /* > 0: stop once the score reaches it */
+} bm_learned_params;
+
+typedef struct bm_learned_stats {
+    int64_t proposals;        /* (u, v) proposals checked by the exact delta */
+    int64_t hits;             /* of which improving (delta > 0) */
+    int64_t exact_passes;
+    int64_t train_steps;
+    double t_propose, t_exact, t_train;  /* seconds in features + scoring + top-K, exact checks + applies, training */
+} bm_learned_stats;
+
+/* Search that proposes the top-K partners of each row (model or uniform),
+ * checks them with the exact delta, and applies the best improving proposal
+ * of each row when it is independent of those already taken (descending
+ * delta).  Stats accumulate into *stats. */
+bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* m, const int32_t* row_order, int32_t nrows,
+                            const bm_learned_params* params, bm_progress* prog, bm_learned_stats* stats);
+
 /* ------------------------------------------------------- device utilities */
 
 /* Device memory, copies and events on the context stream, for callers that

@@ -16,6 +16,8 @@
  *                   (bounded: the reference loops forever)
  *   orc_rows_omp    the OpenMP m2 sweep        src/graph-alignment-optimized-parallel.c:544
  *                   (deltas only, no applies)
+ *   orc_mlp         FP64 replica of the engine's learned-proposal MLP (no
+ *                   reference counterpart), the checker of its gradients
  * Parity is pinned by tests/golden/ fixtures produced by the reference's own
  * functions compiled from its sources (oracle/ref_harness.c).
  */
@@ -307,4 +309,95 @@ int64_t orc_perm_delta(const orc_graph* gm, const orc_graph* gf, const int32_t* 
         }
     }
     return delta;
+}
+
+/* ------------------------------------------------ learned-proposal model */
+
+/* FP64 replica of the engine's 24 -> 128 -> 128 -> 1 ReLU MLP (no reference
+ * counterpart).  With rounding != 0 it applies the engine's roundings: inputs,
+ * W1, W2 and w3 rounded to BF16 (nearest even); each hidden pre-activation
+ * (sum + bias) rounded to FP32, then ReLU, then BF16; sums in FP64.  With
+ * rounding == 0 everything stays FP64 (a smooth function, for checking the
+ * backward formulas by finite differences).  Parameters packed as W1[24][128]
+ * b1 W2[128][128] b2 w3 b3.  Writes out[k] when out != NULL and, when grads
+ * != NULL, the gradient of mean((out - y)^2) and *loss. */
+#define ORC_IN 24
+#define ORC_H 128
+static double orc_bf16(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) != 0x7F800000u) {
+        u += 0x7FFFu + ((u >> 16) & 1u);
+        u &= 0xFFFF0000u;
+    }
+    float r;
+    memcpy(&r, &u, 4);
+    return (double)r;
+}
+
+int orc_mlp(const float* w, const float* x, const float* y, int64_t k, int rounding, double* out, double* grads,
+            double* loss) {
+    const int o_b1 = ORC_IN * ORC_H, o_w2 = o_b1 + ORC_H, o_b2 = o_w2 + ORC_H * ORC_H, o_w3 = o_b2 + ORC_H,
+              o_b3 = o_w3 + ORC_H, np = o_b3 + 1;
+    double* wr = (double*)malloc(sizeof(double) * (size_t)np);
+    if (!wr) return -1;
+    for (int i = 0; i < np; i++) wr[i] = (double)w[i];
+    if (rounding) {
+        for (int i = 0; i < ORC_IN * ORC_H; i++) wr[i] = orc_bf16(w[i]);
+        for (int i = 0; i < ORC_H * ORC_H; i++) wr[o_w2 + i] = orc_bf16(w[o_w2 + i]);
+        for (int i = 0; i < ORC_H; i++) wr[o_w3 + i] = orc_bf16(w[o_w3 + i]);
+    }
+    if (grads) memset(grads, 0, sizeof(double) * (size_t)np);
+    double lsum = 0.0;
+    for (int64_t p = 0; p < k; p++) {
+        double xb[ORC_IN], h1[ORC_H], h2[ORC_H], dh2[ORC_H];
+        for (int i = 0; i < ORC_IN; i++) xb[i] = rounding ? orc_bf16(x[p * ORC_IN + i]) : (double)x[p * ORC_IN + i];
+        for (int j = 0; j < ORC_H; j++) {
+            double a = 0.0;
+            for (int i = 0; i < ORC_IN; i++) a += xb[i] * wr[i * ORC_H + j];
+            const double pre = a + wr[o_b1 + j];
+            if (rounding) {
+                const float pf = (float)pre;
+                h1[j] = orc_bf16(pf > 0.f ? pf : 0.f);
+            } else {
+                h1[j] = pre > 0.0 ? pre : 0.0;
+            }
+        }
+        for (int j = 0; j < ORC_H; j++) {
+            double a = 0.0;
+            for (int i = 0; i < ORC_H; i++) a += h1[i] * wr[o_w2 + i * ORC_H + j];
+            const double pre = a + wr[o_b2 + j];
+            if (rounding) {
+                const float pf = (float)pre;
+                h2[j] = orc_bf16(pf > 0.f ? pf : 0.f);
+            } else {
+                h2[j] = pre > 0.0 ? pre : 0.0;
+            }
+        }
+        double o = wr[o_b3];
+        for (int j = 0; j < ORC_H; j++) o += h2[j] * wr[o_w3 + j];
+        if (out) out[p] = o;
+        if (!grads) continue;
+        const double r = o - (double)y[p];
+        lsum += r * r;
+        const double d = 2.0 * r / (double)k;
+        grads[o_b3] += d;
+        for (int j = 0; j < ORC_H; j++) {
+            grads[o_w3 + j] += d * h2[j];
+            dh2[j] = h2[j] > 0.0 ? d * wr[o_w3 + j] : 0.0;
+            grads[o_b2 + j] += dh2[j];
+        }
+        for (int i = 0; i < ORC_H; i++) {
+            for (int j = 0; j < ORC_H; j++) grads[o_w2 + i * ORC_H + j] += h1[i] * dh2[j];
+            if (h1[i] > 0.0) {
+                double a = 0.0;
+                for (int j = 0; j < ORC_H; j++) a += wr[o_w2 + i * ORC_H + j] * dh2[j];
+                grads[o_b1 + i] += a;
+                for (int q = 0; q < ORC_IN; q++) grads[q * ORC_H + i] += xb[q] * a;
+            }
+        }
+    }
+    if (loss) *loss = lsum / (double)(k > 0 ? k : 1);
+    free(wr);
+    return 0;
 }

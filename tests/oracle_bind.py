@@ -209,3 +209,28 @@ class Reference:
         k = min(acc, log_cap)
         log = np.stack([l1[:k].astype(np.int64), l2[:k].astype(np.int64), ld[:k].astype(np.int64)], axis=1)
         return pi, int(score.value), log, int(sw.value), int(cv.value)
+
+
+MLP_IN = 24
+
+
+def mlp_oracle(w, x, y=None, rounding=True):
+    """FP64 replica of the learned-proposal MLP: (out[k], grads or None, loss).
+    w: packed float32 parameters; x: k x 24 float32 features; y: targets."""
+    L = oracle_lib()
+    L.orc_mlp.restype = C.c_int
+    L.orc_mlp.argtypes = [vp, vp, vp, C.c_int64, C.c_int, vp, vp, C.POINTER(C.c_double)]
+    w = np.ascontiguousarray(np.asarray(w, dtype=np.float32))
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float32).reshape(-1, MLP_IN))
+    k = x.shape[0]
+    out = np.zeros(k, np.float64)
+    grads = None
+    yy = None
+    if y is not None:
+        yy = np.ascontiguousarray(np.asarray(y, dtype=np.float32))
+        grads = np.zeros(w.shape[0], np.float64)
+    loss = C.c_double()
+    st = L.orc_mlp(_p(w), _p(x), _p(yy), k, int(bool(rounding)), _p(out), _p(grads), C.byref(loss))
+    if st != 0:
+        raise MemoryError("orc_mlp failed")
+    return out, grads, loss.value
