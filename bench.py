@@ -323,7 +323,8 @@ def run_ours(args, ws, rank, local, dist):
                       "candidates_per_step": deltas_step, "l2": "flushed before every step",
                       "parallelism": f"row batches sharded over {ws} rank(s), no data-path collective"},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                        "frac": achieved / peak,
+                        "traffic": profiled_traffic(args.steps, args.warmup, R), "peak_source": peak_kind,
                         "kernel": "rows_kernel (whole-row 2-hop scatter, fused row reduction)",
                         "bytes_per_step": total_bytes / args.steps},
            "e2e": {"value": e2e_val, "unit": "deltas/s", "h2d_bytes_per_step": 4 * R,
@@ -335,9 +336,124 @@ def run_ours(args, ws, rank, local, dist):
         out["cpu_baseline"] = cpu_baseline(A, B, init, rows, starts[args.warmup:], budget_s=args.ref_seconds)
     if rank == 0 and ws == 1 and args.search_seconds > 0:
         out["search"] = plain_search(eng, rows, args.search_seconds)
+    eng.close()
+    if rank == 0 and ws == 1 and args.learned_seconds > 0 and out.get("search", {}).get("converged"):
+        out["learned_vs_plain"] = learned_compare(local, A, B, init, rows, out["search"], args.learned_seconds)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    eng.close()
+
+
+def profiled_traffic(steps: int, warmup: int, rows_per_step: int):
+    """DRAM bytes per rows_kernel launch (read + write) from the committed ncu
+    summary of this bench's timed launches, when the summary's configuration
+    is this run's; else None."""
+    path = os.path.join(REPO, "profiles", "rows_kernel_cfg2.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("bench-traffic:"):
+                    rec = json.loads(line.split(":", 1)[1])
+                    if (rec["steps"], rec["warmup"], rec["rows_per_step"]) == (steps, warmup, rows_per_step):
+                        return float(rec["bytes_per_launch"])
+    except (OSError, ValueError, KeyError):
+        pass
+    return None
+
+
+MLP_FLOP_PER_PAIR = 2 * (24 * 128 + 128 * 128 + 128)
+
+
+def bf16_peak():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def learned_compare(device, A, B, init, rows, plain, seconds):
+    """Learned vs plain proposals from the same initial matching: time to the
+    plain search's converged score (record harvest, training and inference
+    included), hit rates of one proposal pass, and the tensor-core scorer's
+    throughput against the measured BF16 peak."""
+    n = A.n
+
+    def engine():
+        e = bm.Engine(device)
+        e.set_graphs(A, B)
+        e.set_mapping(init)
+        return e
+
+    out = {"plain_seconds": plain["seconds"], "plain_score": plain["score"]}
+    # scorer throughput, inputs resident: 8 rows per SM-pair of CTAs
+    e = engine()
+    m = bm.Mlp(e, seed=1)
+    R = min(n, 1184)
+    d_rows = e.dev_alloc(4 * R)
+    e.h2d(d_rows, np.ascontiguousarray(rows[:R]))
+    d_sc = e.dev_alloc(4 * R * n)
+    a, b = e.event(), e.event()
+    for backend, reps, name in ((0, 5, "tcgen05"), (1, 1, "simt")):
+        m.set_backend(backend)
+        m.score_rows_dev(d_rows, R, d_sc)
+        e.sync()
+        e.record(a)
+        for _ in range(reps):
+            m.score_rows_dev(d_rows, R, d_sc)
+        e.record(b)
+        e.sync()
+        m.status()
+        ms = e.elapsed_ms(a, b) / reps
+        pairs = R * (n - 1)
+        out[f"scorer_{name}"] = {"pairs_per_s": pairs / (ms / 1e3),
+                                 "tflops": pairs * MLP_FLOP_PER_PAIR / (ms / 1e3) / 1e12, "ms_per_launch": ms,
+                                 "rows_per_launch": R}
+    peak, kind = bf16_peak()
+    tc = out["scorer_tcgen05"]["tflops"]
+    out["roofline_scorer"] = {"bound": "tensor", "achieved": tc, "peak": peak, "unit": "TFLOP/s", "frac": tc / peak,
+                              "peak_source": kind, "kernel": "mlp_rows_tc_kernel",
+                              "flop_per_pair": MLP_FLOP_PER_PAIR}
+    e.dev_free(d_rows)
+    e.dev_free(d_sc)
+    e.close()
+
+    def one_pass(mm, uniform):
+        _, p, s = mm.search(rows, topk=64, max_sweeps=1, exact_fallback=False, uniform=uniform, seed=7)
+        return {"hit_rate": s.hits / max(1, s.proposals), "proposals": int(s.proposals), "accepts": int(p.accepts),
+                "score": int(p.score)}
+
+    e = engine()
+    out["pass_uniform"] = one_pass(bm.Mlp(e, seed=1), True)
+    e.close()
+    # learned: harvest + training + search, all inside the clock
+    e = engine()
+    t0 = time.perf_counter()
+    m = bm.Mlp(e, seed=1)
+    m.reserve_records(5_000_000)
+    nrec = m.collect_rows(rows, per_row=256, seed=3)
+    l0 = m.fit(1, batch=8192, lr=2e-3)
+    l1 = m.fit(1500, batch=8192, lr=2e-3)
+    e.sync()
+    t_train = time.perf_counter() - t0
+    w = m.params()
+    st, p, s = m.search(rows, topk=64, exact_fallback=True, train_every=4, train_batch=4096, lr=5e-4,
+                        target_score=plain["score"], time_budget=seconds)
+    t_total = time.perf_counter() - t0
+    out["learned"] = {"seconds_to_plain_score": t_total if p.score >= plain["score"] else None,
+                      "seconds": t_total, "score": int(p.score), "records": int(nrec), "harvest_train_s": t_train,
+                      "loss_first": l0, "loss_last": l1, "t_propose": s.t_propose, "t_exact": s.t_exact,
+                      "t_train_online": s.t_train, "hit_rate": s.hits / max(1, s.proposals),
+                      "exact_passes": int(s.exact_passes), "timed_out": st == bm.BM_TIMEOUT}
+    e.close()
+    e = engine()
+    m = bm.Mlp(e, seed=1)
+    m.set_params(w)
+    out["pass_trained"] = one_pass(m, False)
+    e.close()
+    e = engine()
+    out["pass_untrained"] = one_pass(bm.Mlp(e, seed=1), False)
+    e.close()
+    return out
 
 
 def plain_search(eng, rows, seconds):
@@ -352,7 +468,8 @@ def plain_search(eng, rows, seconds):
         if prog.converged:
             break
     return {"seconds": round(time.perf_counter() - t0, 3), "accepts": int(prog.accepts),
-            "evaluated": int(prog.evaluated), "trajectory": traj, "converged": int(prog.converged)}
+            "evaluated": int(prog.evaluated), "trajectory": traj, "converged": int(prog.converged),
+            "score": int(prog.score)}
 
 
 def main():
@@ -365,6 +482,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--search-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learned-seconds", type=float, default=90.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

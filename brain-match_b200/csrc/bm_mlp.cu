@@ -50,12 +50,14 @@ constexpr int kOffW3 = kOffB2 + BM_MLP_H;
 constexpr int kOffB3 = kOffW3 + BM_MLP_H;
 constexpr int kNParams = kOffB3 + 1;
 
-// Weight image of the tensor-core kernel: W1 and W2 as BF16 in the K-major,
-// no-swizzle operand layout, then the FP32 epilogue vectors b1, b2, w3, b3.
+// Weight image of the tensor-core kernel: W1, W2 and the output row w3 as
+// BF16 in the K-major, no-swizzle operand layout, then the FP32 epilogue
+// vectors b1, b2, (unused), b3.
 constexpr int kImgW1 = 128 * 32 * 2;   // N=128 hidden x K=32 (24 inputs + 8 zero)
 constexpr int kImgW2 = 128 * 128 * 2;  // N=128 out x K=128 in
+constexpr int kImgW3 = 16 * 128 * 2;   // N=16 x K=128: w3 in row 0, zeros elsewhere
 constexpr int kImgEp = (3 * BM_MLP_H + 4) * 4;
-constexpr int kImgBytes = kImgW1 + kImgW2 + kImgEp;
+constexpr int kImgBytes = kImgW1 + kImgW2 + kImgW3 + kImgEp;
 
 }  // namespace
 
@@ -104,11 +106,6 @@ __host__ __device__ __forceinline__ float bf16r(float x) {
     float r;
     memcpy(&r, &u, 4);
     return r;
-}
-
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
-    // both inputs already hold BF16 values: keep their upper halves
-    return (__float_as_uint(lo) >> 16) | (__float_as_uint(hi) & 0xFFFF0000u);
 }
 
 __device__ __forceinline__ float bf16_to_float(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
@@ -181,8 +178,8 @@ __global__ void vertex_table_kernel(GView A, HashView hb, const int32_t* __restr
 }
 
 // The 24 features of swap (u, v) from the two table rows and the two B
-// adjacency bits, rounded to BF16.
-__device__ __forceinline__ void pair_features(const float* a, const float* b, bool b_uv, bool b_vu, float* x) {
+// adjacency bits, before rounding.
+__device__ __forceinline__ void pair_features_raw(const float* a, const float* b, bool b_uv, bool b_vu, float* x) {
 #pragma unroll
     for (int i = 0; i < 7; i++) {
         x[i] = a[i];
@@ -198,6 +195,11 @@ __device__ __forceinline__ void pair_features(const float* a, const float* b, bo
     x[21] = b_vu ? 1.f : 0.f;
     x[22] = fabsf(a[4] - b[4]);
     x[23] = a[5] + b[5];
+}
+
+// Same, rounded to BF16 (nearest even).
+__device__ __forceinline__ void pair_features(const float* a, const float* b, bool b_uv, bool b_vu, float* x) {
+    pair_features_raw(a, b, b_uv, b_vu, x);
 #pragma unroll
     for (int i = 0; i < BM_MLP_IN; i++) x[i] = bf16r(x[i]);
 }
@@ -543,28 +545,34 @@ __global__ void gather_batch_kernel(const uint16_t* __restrict__ rx, const float
 // --------------------------------------------- tensor-core row scoring kernel
 //
 // One CTA (128 threads) scores whole rows: for row u, candidates v = 1..n in
-// tiles of 128.  Per tile: every thread builds the 24 features of its
-// candidate into the A operand (BF16, K padded to 32); one thread issues
-// layer 1 (two K=16 MMAs, M=N=128) into TMEM columns 0..127; the threads read
-// their accumulator row back (tcgen05.ld 32x32b), add the bias, apply ReLU,
-// round to BF16 and store the A operand of layer 2; eight K=16 MMAs
-// accumulate layer 2 into TMEM columns 128..255; the epilogue adds the bias,
-// applies ReLU, rounds, and dots with w3 in registers (thread i holds row i,
-// so no reduction across threads).
+// tiles of 128, one candidate per thread.  Per tile:
+//   1. every thread builds its candidate's 24 features as the BF16 A operand
+//      (K padded to 32);
+//   2. one thread issues layer 1 (two K=16 MMAs, M=N=128) into TMEM columns
+//      0..127; the threads read their accumulator row back (tcgen05.ld
+//      32x32b), add the bias and convert with ReLU to BF16 (cvt.rn.relu.bf16x2)
+//      into the A operand of layer 2;
+//   3. eight K=16 MMAs accumulate layer 2 into TMEM columns 128..255; the same
+//      epilogue produces the BF16 activations h2 in the same buffer;
+//   4. the output layer h2 . w3 runs as eight K=16 MMAs with N=16 (w3 in row 0
+//      of the B operand, zeros elsewhere) into columns 0..15, and each thread
+//      reads its column 0 and adds b3.
+// The operand buffer holds the features, then h1, then h2: each is consumed
+// by an MMA whose completion is awaited before the buffer is rewritten.
 
 constexpr int kTcThreads = 128;
 constexpr uint32_t kSmW1 = 0;
-constexpr uint32_t kSmW2 = kSmW1 + kImgW1;         // 8192
-constexpr uint32_t kSmX = kSmW2 + kImgW2;          // 40960
-constexpr uint32_t kSmH1 = kSmX + 128 * 32 * 2;    // 49152
-constexpr uint32_t kSmEp = kSmH1 + 128 * 128 * 2;  // 81920
-constexpr uint32_t kSmBits = kSmEp + kImgEp;       // 83472
-constexpr uint32_t kTcMinSmem = 100 * 1024;        // at most 2 CTAs (2 x 256 TMEM columns) per SM
-static_assert(kImgW1 == (int)kSmW2 && kSmBits % 16 == 0, "image layout");
+constexpr uint32_t kSmW2 = kSmW1 + kImgW1;          // 8192
+constexpr uint32_t kSmW3 = kSmW2 + kImgW2;          // 40960
+constexpr uint32_t kSmH = kSmW3 + kImgW3;           // 45056: features / h1 / h2 operand (32 KB)
+constexpr uint32_t kSmEp = kSmH + 128 * 128 * 2;    // 77824: b1, b2, (unused), b3
+constexpr uint32_t kSmBits = kSmEp + kImgEp;        // 79376
+constexpr uint32_t kTcMinSmem = 100 * 1024;         // at most 2 CTAs (2 x 256 TMEM columns) per SM
+static_assert(kSmBits % 16 == 0 && kSmH % 1024 == 0, "operand layout");
 
 __host__ __device__ constexpr uint32_t bits_words(int32_t n) { return (uint32_t)(n + 32) / 32u; }
 __host__ __device__ constexpr uint32_t tc_tail(int32_t n) { return kSmBits + ((2u * bits_words(n) * 4u + 15u) & ~15u); }
-// two candidate bitmaps, then two mbarriers and the TMEM base slot
+// two candidate bitmaps, then three mbarriers and the TMEM base slot
 __host__ __device__ constexpr uint32_t tc_smem_bytes(int32_t n) { return tc_tail(n) + 32u; }
 
 // Byte offset of element (row r, k) in a K-major no-swizzle operand with
@@ -586,17 +594,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
 // Instruction descriptor of kind::f16: FP32 accumulator (bit 4), A and B BF16
 // (bits 7 and 10), both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at
 // bit 24.  A and B have the same type, as kind::f16 requires.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+constexpr uint32_t kIdesc128 = idesc_bf16(128, 128);
+constexpr uint32_t kIdesc16 = idesc_bf16(128, 16);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
         :
-        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 
@@ -607,6 +620,19 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Two FP32 values to packed BF16 (round to nearest even), lo in the low half.
+__device__ __forceinline__ uint32_t cvt_bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+// Same with ReLU applied (negative results become +0).
+__device__ __forceinline__ uint32_t cvt_relu_bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
 
 // 32 consecutive FP32 columns of this thread's TMEM lane.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
@@ -622,6 +648,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// One FP32 column of this thread's TMEM lane.
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    return __uint_as_float(r);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
@@ -650,22 +684,28 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
 __global__ void prep_image_kernel(const float* __restrict__ w, unsigned char* __restrict__ img) {
     unsigned short* w1 = reinterpret_cast<unsigned short*>(img + kSmW1);
     unsigned short* w2 = reinterpret_cast<unsigned short*>(img + kSmW2);
-    float* ep = reinterpret_cast<float*>(img + kImgW1 + kImgW2);
-    const int total = 128 * 32 + 128 * 128 + 3 * 128 + 4;
+    unsigned short* w3 = reinterpret_cast<unsigned short*>(img + kSmW3);
+    float* ep = reinterpret_cast<float*>(img + kImgW1 + kImgW2 + kImgW3);
+    const int n1 = 128 * 32, n2 = 128 * 128, n3 = 16 * 128;
+    const int total = n1 + n2 + n3 + 3 * 128 + 4;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        if (t < 128 * 32) {
+        if (t < n1) {
             const int j = t / 32, i = t % 32;  // hidden j (N), input i (K)
             const float v = i < BM_MLP_IN ? bf16r(w[i * BM_MLP_H + j]) : 0.f;
             w1[kmajor_off(j, i, 32) / 2] = (unsigned short)(__float_as_uint(v) >> 16);
-        } else if (t < 128 * 32 + 128 * 128) {
-            const int q = t - 128 * 32, j = q / 128, i = q % 128;  // out j (N), in i (K)
+        } else if (t < n1 + n2) {
+            const int q = t - n1, j = q / 128, i = q % 128;  // out j (N), in i (K)
             const float v = bf16r(w[kOffW2 + i * BM_MLP_H + j]);
             w2[kmajor_off(j, i, 128) / 2] = (unsigned short)(__float_as_uint(v) >> 16);
+        } else if (t < n1 + n2 + n3) {
+            const int q = t - n1 - n2, j = q / 128, i = q % 128;  // row j (N = 16), in i (K)
+            const float v = j == 0 ? bf16r(w[kOffW3 + i]) : 0.f;
+            w3[kmajor_off(j, i, 128) / 2] = (unsigned short)(__float_as_uint(v) >> 16);
         } else {
-            const int q = t - 128 * 32 - 128 * 128;
+            const int q = t - n1 - n2 - n3;
             if (q < 128) ep[q] = w[kOffB1 + q];
             else if (q < 256) ep[q] = w[kOffB2 + q - 128];
-            else if (q < 384) ep[q] = bf16r(w[kOffW3 + q - 256]);
+            else if (q < 384) ep[q] = 0.f;
             else ep[q] = (q == 384) ? w[kOffB3] : 0.f;
         }
     }
@@ -686,6 +726,27 @@ struct TcArgs {
     int32_t* flag;
 };
 
+// Hidden-layer epilogue: this thread's accumulator row (128 FP32 columns at
+// taddr) plus bias, ReLU, BF16, stored as its row of the next A operand.
+__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* __restrict__ bias, unsigned char* sm,
+                                                int tid) {
+#pragma unroll 1
+    for (int c = 0; c < 4; c++) {
+        float d[32];
+        tmem_ld32(taddr + 32u * c, d);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float* bq = bias + 32 * c + 8 * q;
+            uint4 o;
+            o.x = cvt_relu_bf16x2(d[8 * q + 0] + bq[0], d[8 * q + 1] + bq[1]);
+            o.y = cvt_relu_bf16x2(d[8 * q + 2] + bq[2], d[8 * q + 3] + bq[3]);
+            o.z = cvt_relu_bf16x2(d[8 * q + 4] + bq[4], d[8 * q + 5] + bq[5]);
+            o.w = cvt_relu_bf16x2(d[8 * q + 6] + bq[6], d[8 * q + 7] + bq[7]);
+            *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 32 * c + 8 * q, 128)) = o;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x;
@@ -695,18 +756,19 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     uint32_t* bits_in = bits_out + nw;
     const uint32_t tail = tc_tail(a.n);
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + tail);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + tail + 16);
-    const uint32_t bar1 = smem_u32(&bars[0]), bar2 = smem_u32(&bars[1]);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + tail + 24);
+    const uint32_t bar1 = smem_u32(&bars[0]), bar2 = smem_u32(&bars[1]), bar3 = smem_u32(&bars[2]);
 
-    {  // weights and epilogue vectors into shared memory
+    {  // weights into shared memory; epilogue vectors after the operand buffer
         const uint4* src = reinterpret_cast<const uint4*>(a.img);
-        for (int i = tid; i < (kImgW1 + kImgW2) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
+        for (int i = tid; i < (kImgW1 + kImgW2 + kImgW3) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
         for (int i = tid; i < kImgEp / 16; i += kTcThreads)
-            reinterpret_cast<uint4*>(sm + kSmEp)[i] = src[(kImgW1 + kImgW2) / 16 + i];
+            reinterpret_cast<uint4*>(sm + kSmEp)[i] = src[(kImgW1 + kImgW2 + kImgW3) / 16 + i];
     }
     if (tid == 0) {
         mbar_init(bar1, 1);
         mbar_init(bar2, 1);
+        mbar_init(bar3, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -720,11 +782,12 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t tm_d1 = tmem, tm_d2 = tmem + 128u;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const uint32_t tm_a = tmem + lane_base;         // layer 1, then the output layer (columns 0..)
+    const uint32_t tm_b = tmem + 128u + lane_base;  // layer 2 (columns 128..255)
     const float* ep = reinterpret_cast<const float*>(sm + kSmEp);
-    const uint32_t sW1 = smem_u32(sm + kSmW1), sW2 = smem_u32(sm + kSmW2);
-    const uint32_t sX = smem_u32(sm + kSmX), sH1 = smem_u32(sm + kSmH1);
+    const uint32_t sW1 = smem_u32(sm + kSmW1), sW2 = smem_u32(sm + kSmW2), sW3 = smem_u32(sm + kSmW3);
+    const uint32_t sH = smem_u32(sm + kSmH);
     uint32_t phase = 0;
     uint32_t pending = 0;  // the barrier whose wait ran out, if any
     bool ok = true;
@@ -751,7 +814,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
         for (int32_t v0 = 1; v0 <= a.n; v0 += 128) {
             const int32_t v = v0 + tid;
             const bool valid = v <= a.n && v != u;
-            {  // A operand of layer 1: this thread's row
+            {  // 1. features of this thread's candidate: the A operand of layer 1
                 float x[BM_MLP_IN];
                 if (valid) {
                     float tb[BM_FT];
@@ -762,7 +825,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
                     tb[8] = q2.x; tb[9] = q2.y; tb[10] = q2.z; tb[11] = q2.w;
                     const bool buv = (bits_out[v >> 5] >> (v & 31)) & 1u;
                     const bool bvu = (bits_in[v >> 5] >> (v & 31)) & 1u;
-                    pair_features(ta, tb, buv, bvu, x);
+                    pair_features_raw(ta, tb, buv, bvu, x);
                 } else {
 #pragma unroll
                     for (int i = 0; i < BM_MLP_IN; i++) x[i] = 0.f;
@@ -771,74 +834,58 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
                 for (int c = 0; c < 4; c++) {
                     uint4 q = make_uint4(0u, 0u, 0u, 0u);
                     if (c < 3) {
-                        q.x = pack_bf16x2(x[8 * c + 0], x[8 * c + 1]);
-                        q.y = pack_bf16x2(x[8 * c + 2], x[8 * c + 3]);
-                        q.z = pack_bf16x2(x[8 * c + 4], x[8 * c + 5]);
-                        q.w = pack_bf16x2(x[8 * c + 6], x[8 * c + 7]);
+                        q.x = cvt_bf16x2(x[8 * c + 0], x[8 * c + 1]);
+                        q.y = cvt_bf16x2(x[8 * c + 2], x[8 * c + 3]);
+                        q.z = cvt_bf16x2(x[8 * c + 4], x[8 * c + 5]);
+                        q.w = cvt_bf16x2(x[8 * c + 6], x[8 * c + 7]);
                     }
-                    *reinterpret_cast<uint4*>(sm + kSmX + kmajor_off(tid, 8 * c, 32)) = q;
+                    *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 8 * c, 32)) = q;
                 }
             }
             proxy_fence();
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
-            if (tid == 0) {
+            if (tid == 0) {  // 2. layer 1
 #pragma unroll
                 for (int s = 0; s < 2; s++)
-                    mma_bf16(tm_d1, smem_desc(sX + 256u * s, 128u, 512u), smem_desc(sW1 + 256u * s, 128u, 512u),
-                             s > 0);
+                    mma_bf16(tmem, smem_desc(sH + 256u * s, 128u, 512u), smem_desc(sW1 + 256u * s, 128u, 512u),
+                             kIdesc128, s > 0);
                 mma_commit(bar1);
             }
-            // the completion test is made block-uniform before any tcgen05.ld
+            // completion tests are made block-uniform before any tcgen05.ld
             if (!__syncthreads_and(mbar_wait(bar1, phase))) { ok = false; pending = bar1; break; }
             tc_fence_after();
-            {  // layer 1 epilogue: bias, ReLU, BF16 -> A operand of layer 2
-#pragma unroll 1
-                for (int c = 0; c < 4; c++) {
-                    float d[32];
-                    tmem_ld32(tm_d1 + lane_base + 32u * c, d);
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        float h[8];
-#pragma unroll
-                        for (int e = 0; e < 8; e++) h[e] = bf16r(fmaxf(d[8 * q + e] + ep[32 * c + 8 * q + e], 0.f));
-                        uint4 o;
-                        o.x = pack_bf16x2(h[0], h[1]);
-                        o.y = pack_bf16x2(h[2], h[3]);
-                        o.z = pack_bf16x2(h[4], h[5]);
-                        o.w = pack_bf16x2(h[6], h[7]);
-                        *reinterpret_cast<uint4*>(sm + kSmH1 + kmajor_off(tid, 32 * c + 8 * q, 128)) = o;
-                    }
-                }
-            }
+            hidden_epilogue(tm_a, ep, sm, tid);
             proxy_fence();
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
-            if (tid == 0) {
+            if (tid == 0) {  // 3. layer 2
 #pragma unroll
                 for (int s = 0; s < 8; s++)
-                    mma_bf16(tm_d2, smem_desc(sH1 + 256u * s, 128u, 2048u), smem_desc(sW2 + 256u * s, 128u, 2048u),
-                             s > 0);
+                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, 2048u),
+                             smem_desc(sW2 + 256u * s, 128u, 2048u), kIdesc128, s > 0);
                 mma_commit(bar2);
             }
             if (!__syncthreads_and(mbar_wait(bar2, phase))) { ok = false; pending = bar2; break; }
             tc_fence_after();
-            float acc = 0.f;
-            {  // layer 2 epilogue and output layer
-#pragma unroll 1
-                for (int c = 0; c < 4; c++) {
-                    float d[32];
-                    tmem_ld32(tm_d2 + lane_base + 32u * c, d);
+            hidden_epilogue(tm_b, ep + 128, sm, tid);
+            proxy_fence();
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0) {  // 4. output layer, N = 16 (row 0 of B holds w3)
 #pragma unroll
-                    for (int e = 0; e < 32; e++) {
-                        const float h = bf16r(fmaxf(d[e] + ep[128 + 32 * c + e], 0.f));
-                        acc = fmaf(h, ep[256 + 32 * c + e], acc);
-                    }
-                }
+                for (int s = 0; s < 8; s++)
+                    mma_bf16(tmem, smem_desc(sH + 256u * s, 128u, 2048u), smem_desc(sW3 + 256u * s, 128u, 2048u),
+                             kIdesc16, s > 0);
+                mma_commit(bar3);
             }
-            if (v <= a.n) out_row[v - 1] = valid ? acc + ep[384] : -INFINITY;
+            if (!__syncthreads_and(mbar_wait(bar3, phase))) { ok = false; pending = bar3; break; }
+            tc_fence_after();
+            const float o = tmem_ld1(tm_a);
+            if (v <= a.n) out_row[v - 1] = valid ? o + ep[384] : -INFINITY;
             phase ^= 1u;
             tc_fence_before();
             __syncthreads();
@@ -1219,8 +1266,9 @@ bm_status fit_steps(bm_mlp* M, int32_t steps, int32_t batch, float lr, float wd,
 
 extern "C" void bm_mlp_destroy(bm_mlp* M) {
     if (!M) return;
+    // the context may already be gone: synchronise the device, not its stream
     cudaSetDevice(M->device);
-    if (M->ctx && M->ctx->stream) cudaStreamSynchronize(M->ctx->stream);
+    cudaDeviceSynchronize();
     cudaFree(M->d_w); cudaFree(M->d_m); cudaFree(M->d_v); cudaFree(M->d_g); cudaFree(M->d_loss);
     cudaFree(M->d_tab); cudaFree(M->d_bdeg); cudaFree(M->d_img); cudaFree(M->d_sc); cudaFree(M->d_flag);
     cudaFree(M->d_rx); cudaFree(M->d_ry); cudaFree(M->d_bx); cudaFree(M->d_by); cudaFree(M->d_scr);
@@ -1402,6 +1450,23 @@ extern "C" bm_status bm_mlp_score_rows(bm_mlp* M, const int32_t* rows, int32_t n
     if ((s = launch_row_scores(M, d_r, nrows)) != BM_OK) return s;
     BM_CUDA(ctx, cudaMemcpyAsync(scores, M->d_sc, sizeof(float) * (size_t)nrows * M->n, cudaMemcpyDeviceToHost,
                                  ctx->stream));
+    return check_flag(M);
+}
+
+extern "C" bm_status bm_mlp_score_rows_dev(bm_mlp* M, const int32_t* d_rows, int32_t nrows, float* d_scores) {
+    bm_status s = mlp_check(M);
+    if (s != BM_OK) return s;
+    bm_ctx* ctx = M->ctx;
+    if (nrows < 0 || (nrows > 0 && (!d_rows || !d_scores))) return bm_fail(ctx, BM_INVALID_ARG, "bad buffers");
+    if (nrows == 0) return BM_OK;
+    if ((s = launch_row_scores(M, d_rows, nrows)) != BM_OK) return s;
+    BM_CUDA(ctx, cudaMemcpyAsync(d_scores, M->d_sc, sizeof(float) * (size_t)nrows * M->n, cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_mlp_status(bm_mlp* M) {
+    if (!M || !M->ctx) return BM_INVALID_ARG;
     return check_flag(M);
 }
 

@@ -6,8 +6,10 @@ if libbmcuda.so is missing or no GPU is present, the calls fail loudly.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
+import weakref
 import subprocess
 
 import numpy as np
@@ -175,6 +177,8 @@ def cuda_lib() -> C.CDLL:
             "bm_mlp_score_features": (C.c_int, [vp, vp, C.c_int64, vp]),
             "bm_mlp_score_rows": (C.c_int, [vp, vp, C.c_int32, vp]),
             "bm_mlp_rows_topk": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp]),
+            "bm_mlp_score_rows_dev": (C.c_int, [vp, vp, C.c_int32, vp]),
+            "bm_mlp_status": (C.c_int, [vp]),
             "bm_mlp_gradients": (C.c_int, [vp, vp, vp, C.c_int64, vp, C.POINTER(C.c_float)]),
             "bm_mlp_adamw_step": (C.c_int, [vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.POINTER(C.c_float)]),
             "bm_mlp_reserve_records": (C.c_int, [vp, C.c_int64]),
@@ -366,6 +370,20 @@ class BMError(RuntimeError):
         super().__init__(f"{name}: {msg}")
 
 
+_live_engines = weakref.WeakSet()
+
+
+@atexit.register
+def _close_live_engines() -> None:
+    """Close every engine still open when the interpreter exits, each with its
+    batches and models first, before the CUDA runtime is torn down."""
+    for eng in list(_live_engines):
+        try:
+            eng.close()
+        except Exception:
+            pass
+
+
 class Engine:
     """One device context: graphs, mapping and the search state."""
 
@@ -377,7 +395,8 @@ class Engine:
             raise BMError(st, f"bm_ctx_create({device})")
         self.h = h
         self.n = 0
-        self._children = []  # weak references to batches, closed before the context
+        self._children = []  # weak references to batches and models, closed before the context
+        _live_engines.add(self)
 
     def _chk(self, st: int, what: str, ok=(BM_OK,)) -> int:
         if st not in ok:
@@ -609,7 +628,6 @@ class Batch:
         eng._chk(self.L.bm_batch_create(eng.h, C.byref(h)), "bm_batch_create")
         self.h = h
         self.ns = []
-        import weakref
         eng._children.append(weakref.ref(self))
 
     def add_pair(self, A: Graph, B: Graph) -> int:
@@ -668,7 +686,6 @@ class Mlp:
         self.h = h
         self.n = eng.n
         self.nparams = int(self.L.bm_mlp_num_params())
-        import weakref
         eng._children.append(weakref.ref(self))
 
     def _chk(self, st, what, ok=(BM_OK,)):
@@ -718,6 +735,12 @@ class Mlp:
         out = np.zeros((r.shape[0], self.n), np.float32)
         self._chk(self.L.bm_mlp_score_rows(self.h, _ptr(r), r.shape[0], _ptr(out)), "bm_mlp_score_rows")
         return out
+
+    def score_rows_dev(self, d_rows: int, nrows: int, d_scores: int) -> None:
+        self._chk(self.L.bm_mlp_score_rows_dev(self.h, d_rows, nrows, d_scores), "bm_mlp_score_rows_dev")
+
+    def status(self) -> None:
+        self._chk(self.L.bm_mlp_status(self.h), "bm_mlp_status")
 
     def rows_topk(self, rows, K: int = 64):
         r = _i32(rows)

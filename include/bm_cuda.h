@@ -333,6 +333,13 @@ bm_status bm_mlp_pair_features(bm_mlp* m, const int32_t* pairs, int64_t k, float
 bm_status bm_mlp_score_pairs(bm_mlp* m, const int32_t* pairs, int64_t k, float* scores);
 bm_status bm_mlp_score_features(bm_mlp* m, const float* x, int64_t k, float* scores);
 bm_status bm_mlp_score_rows(bm_mlp* m, const int32_t* rows, int32_t nrows, float* scores);
+/* Same on device buffers, asynchronous on the context stream (the scores are
+ * produced in the model's own buffer and copied to d_scores).  A tensor-core
+ * wait that ran out is reported by the next bm_mlp_status or host-side call. */
+bm_status bm_mlp_score_rows_dev(bm_mlp* m, const int32_t* d_rows, int32_t nrows, float* d_scores);
+/* Synchronise and report (then clear) the tensor-core kernel's error flag:
+ * BM_TIMEOUT if an MMA completion wait ran out, else BM_OK. */
+bm_status bm_mlp_status(bm_mlp* m);
 /* The K (1..64) best-scored partners of each row, best first, ties by lower
  * id; partners[r*K + j], scores optional. */
 bm_status bm_mlp_rows_topk(bm_mlp* m, const int32_t* rows, int32_t nrows, int32_t K, int32_t* partners,
