@@ -339,6 +339,9 @@ def run_ours(args, ws, rank, local, dist):
     eng.close()
     if rank == 0 and ws == 1 and args.learned_seconds > 0 and out.get("search", {}).get("converged"):
         out["learned_vs_plain"] = learned_compare(local, A, B, init, rows, out["search"], args.learned_seconds)
+    if rank == 0 and ws == 1 and not args.no_extras:
+        out["higher_order"] = higher_order(local, A, B, init)
+        out["sa_chains"] = sa_chains(local, args.sa_steps)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -436,8 +439,8 @@ def learned_compare(device, A, B, init, rows, plain, seconds):
     e.sync()
     t_train = time.perf_counter() - t0
     w = m.params()
-    st, p, s = m.search(rows, topk=64, exact_fallback=True, train_every=4, train_batch=4096, lr=5e-4,
-                        target_score=plain["score"], time_budget=seconds)
+    st, p, s = m.search(rows, topk=64, exact_fallback=True, fallback_accepts=n // 100, train_every=4,
+                        train_batch=4096, lr=5e-4, target_score=plain["score"], time_budget=seconds)
     t_total = time.perf_counter() - t0
     out["learned"] = {"seconds_to_plain_score": t_total if p.score >= plain["score"] else None,
                       "seconds": t_total, "score": int(p.score), "records": int(nrec), "harvest_train_s": t_train,
@@ -452,6 +455,71 @@ def learned_compare(device, A, B, init, rows, plain, seconds):
     e.close()
     e = engine()
     out["pass_untrained"] = one_pass(bm.Mlp(e, seed=1), False)
+    e.close()
+    return out
+
+
+def higher_order(device, A, B, init):
+    """Exact k-set permutation deltas on the full-scale pair: 4,096 random
+    8-subsets (8! = 40,320 permutations each) and 65,536 3-vertex sets along
+    2-paths u -> x -> y (all 6 permutations), best permutation per set."""
+    n = A.n
+    e = bm.Engine(device)
+    e.set_graphs(A, B)
+    e.set_mapping(init)
+    rng = np.random.default_rng(4)
+    sets8 = np.stack([rng.choice(n, 8, replace=False) + 1 for _ in range(4096)]).astype(np.int32)
+    order = np.argsort(A.src, kind="stable")
+    src, dst = A.src[order], A.dst[order]
+    ptr = np.searchsorted(src, np.arange(0, n + 2))  # out-list of v: [ptr[v], ptr[v+1])
+    e_idx = rng.integers(0, len(src), 4 * 65536)
+    u, x = src[e_idx], dst[e_idx]
+    deg = ptr[x + 1] - ptr[x]
+    ok = deg > 0
+    pick = ptr[x] + (rng.random(len(x)) * np.maximum(deg, 1)).astype(np.int64)
+    y = np.where(ok, dst[np.minimum(pick, len(dst) - 1)], 0)
+    good = ok & (y != u) & (y != x) & (u != x)
+    sets3 = np.stack([u[good], x[good], y[good]], 1)[:65536].astype(np.int32)
+    out = {}
+    for k, sets, nperm in ((8, sets8, 40320), (3, sets3, 6)):
+        e.kset_eval(k, sets[:64])
+        t0 = time.perf_counter()
+        best, _ = e.kset_eval(k, sets)
+        dt = time.perf_counter() - t0
+        out[f"k{k}"] = {"sets": int(len(sets)), "sets_per_s": len(sets) / dt,
+                        "permutation_deltas_per_s": len(sets) * nperm / dt, "improving_sets": int((best > 0).sum()),
+                        "seconds": dt, "timing": "host call, transfers included"}
+    e.close()
+    return out
+
+
+def sa_chains(device, steps):
+    """Batched annealing chains: 16 pairs with n uniform in 2,000..20,000 and
+    80 n edges, 4 chains per pair, T 5 -> 0.01 geometric."""
+    rng = np.random.default_rng(3)
+    e = bm.Engine(device)
+    batch = bm.Batch(e)
+    inits, ns = [], []
+    t_gen = time.perf_counter()
+    for i in range(16):
+        n = int(rng.integers(2000, 20001))
+        A, B, truth, init = bm.gen_pair(3, n=n, m_target=80 * n, seed=300 + i)
+        batch.add_pair(A, B)
+        inits.append(init)
+        ns.append(n)
+    t_gen = time.perf_counter() - t_gen
+    chain_pair = np.repeat(np.arange(16), 4).astype(np.int32)
+    keys = 1000 + np.arange(64)
+    init_pis = [inits[p] for p in chain_pair]
+    batch.sa_run(chain_pair, keys, init_pis, 2000)  # autotune and warm-up
+    t0 = time.perf_counter()
+    pis, scores, acc, st = batch.sa_run(chain_pair, keys, init_pis, steps, t0=5.0, t_end=0.01)
+    dt = time.perf_counter() - t0
+    out = {"chains": 64, "pairs": 16, "n_range": [min(ns), max(ns)], "steps_per_chain": steps,
+           "proposals_per_s": 64 * steps / dt, "seconds": dt, "candidates_per_iteration": int(st.candidates),
+           "launches": int(st.launches), "accepts_mean": float(np.mean(acc)), "generation_s": t_gen,
+           "timing": "host call: graph replay, transfers and final scores included"}
+    batch.close()
     e.close()
     return out
 
@@ -483,6 +551,8 @@ def main():
     ap.add_argument("--search-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned-seconds", type=float, default=90.0)
+    ap.add_argument("--no-extras", action="store_true", help="skip the k-set and annealing-chain sections")
+    ap.add_argument("--sa-steps", type=int, default=1_000_000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

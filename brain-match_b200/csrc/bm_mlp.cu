@@ -545,30 +545,33 @@ __global__ void gather_batch_kernel(const uint16_t* __restrict__ rx, const float
 // --------------------------------------------- tensor-core row scoring kernel
 //
 // One CTA (128 threads) scores whole rows: for row u, candidates v = 1..n in
-// tiles of 128, one candidate per thread.  Per tile:
+// tiles of 128, one candidate per thread.  Per tile t:
 //   1. every thread builds its candidate's 24 features as the BF16 A operand
-//      (K padded to 32);
+//      (K padded to 32) in the feature buffer X;
 //   2. one thread issues layer 1 (two K=16 MMAs, M=N=128) into TMEM columns
 //      0..127; the threads read their accumulator row back (tcgen05.ld
 //      32x32b), add the bias and convert with ReLU to BF16 (cvt.rn.relu.bf16x2)
-//      into the A operand of layer 2;
+//      into the activation buffer H;
 //   3. eight K=16 MMAs accumulate layer 2 into TMEM columns 128..255; the same
-//      epilogue produces the BF16 activations h2 in the same buffer;
+//      epilogue writes h2 over h1 in H;
 //   4. the output layer h2 . w3 runs as eight K=16 MMAs with N=16 (w3 in row 0
-//      of the B operand, zeros elsewhere) into columns 0..15, and each thread
-//      reads its column 0 and adds b3.
-// The operand buffer holds the features, then h1, then h2: each is consumed
-// by an MMA whose completion is awaited before the buffer is rewritten.
+//      of the B operand, zeros elsewhere) into columns 128..143, and each
+//      thread reads its column 128 and adds b3.
+// Tiles overlap: while layer 2 of tile t runs on the tensor cores, the threads
+// build the features of tile t+1 into X and issue its layer 1 into columns
+// 0..127, which step 2 of tile t has already read back.  Every buffer is
+// rewritten only after the MMA that reads it has signalled completion.
 
 constexpr int kTcThreads = 128;
 constexpr uint32_t kSmW1 = 0;
 constexpr uint32_t kSmW2 = kSmW1 + kImgW1;          // 8192
 constexpr uint32_t kSmW3 = kSmW2 + kImgW2;          // 40960
-constexpr uint32_t kSmH = kSmW3 + kImgW3;           // 45056: features / h1 / h2 operand (32 KB)
-constexpr uint32_t kSmEp = kSmH + 128 * 128 * 2;    // 77824: b1, b2, (unused), b3
-constexpr uint32_t kSmBits = kSmEp + kImgEp;        // 79376
+constexpr uint32_t kSmH = kSmW3 + kImgW3;           // 45056: h1 / h2 operand (32 KB)
+constexpr uint32_t kSmX = kSmH + 128 * 128 * 2;     // 77824: features operand (8 KB)
+constexpr uint32_t kSmEp = kSmX + 128 * 32 * 2;     // 86016: b1, b2, (unused), b3
+constexpr uint32_t kSmBits = kSmEp + kImgEp;        // 87568
 constexpr uint32_t kTcMinSmem = 100 * 1024;         // at most 2 CTAs (2 x 256 TMEM columns) per SM
-static_assert(kSmBits % 16 == 0 && kSmH % 1024 == 0, "operand layout");
+static_assert(kSmBits % 16 == 0 && kSmH % 1024 == 0 && kSmX % 1024 == 0, "operand layout");
 
 __host__ __device__ constexpr uint32_t bits_words(int32_t n) { return (uint32_t)(n + 32) / 32u; }
 __host__ __device__ constexpr uint32_t tc_tail(int32_t n) { return kSmBits + ((2u * bits_words(n) * 4u + 15u) & ~15u); }
@@ -662,22 +665,22 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 
-// Bounded wait for phase `parity` of an mbarrier: about two seconds of SM
-// clock at most, then false.
+// Bounded wait for phase `parity` of an mbarrier: try_wait suspends the thread
+// until the phase completes or a hardware time slice passes; the loop gives up
+// after about two seconds of SM clock and returns false.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     const long long t0 = clock64();
     for (;;) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
             : "r"(mbar), "r"(parity)
             : "memory");
         if (done) return true;
         if (clock64() - t0 > 4000000000ll) return false;
-        __nanosleep(32);
     }
 }
 
@@ -747,6 +750,47 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* __r
     }
 }
 
+// Features of this thread's candidate v of row u into its row of the X operand.
+__device__ __forceinline__ void build_features(const TcArgs& a, const float* ta, const uint32_t* bits_out,
+                                               const uint32_t* bits_in, int32_t u, int32_t v, unsigned char* sm,
+                                               int tid) {
+    float x[BM_MLP_IN];
+    if (v <= a.n && v != u) {
+        float tb[BM_FT];
+        const float4* t4 = reinterpret_cast<const float4*>(a.tab + (size_t)v * BM_FT);
+        const float4 q0 = t4[0], q1 = t4[1], q2 = t4[2];
+        tb[0] = q0.x; tb[1] = q0.y; tb[2] = q0.z; tb[3] = q0.w;
+        tb[4] = q1.x; tb[5] = q1.y; tb[6] = q1.z; tb[7] = q1.w;
+        tb[8] = q2.x; tb[9] = q2.y; tb[10] = q2.z; tb[11] = q2.w;
+        const bool buv = (bits_out[v >> 5] >> (v & 31)) & 1u;
+        const bool bvu = (bits_in[v >> 5] >> (v & 31)) & 1u;
+        pair_features_raw(ta, tb, buv, bvu, x);
+    } else {
+#pragma unroll
+        for (int i = 0; i < BM_MLP_IN; i++) x[i] = 0.f;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        uint4 q = make_uint4(0u, 0u, 0u, 0u);
+        if (c < 3) {
+            q.x = cvt_bf16x2(x[8 * c + 0], x[8 * c + 1]);
+            q.y = cvt_bf16x2(x[8 * c + 2], x[8 * c + 3]);
+            q.z = cvt_bf16x2(x[8 * c + 4], x[8 * c + 5]);
+            q.w = cvt_bf16x2(x[8 * c + 6], x[8 * c + 7]);
+        }
+        *reinterpret_cast<uint4*>(sm + kSmX + kmajor_off(tid, 8 * c, 32)) = q;
+    }
+}
+
+// Make this thread's generic shared-memory writes visible to the tensor cores
+// and order its earlier tcgen05 accesses before the barrier.
+__device__ __forceinline__ void tc_handoff() {
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+
 __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x;
@@ -759,7 +803,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + tail + 24);
     const uint32_t bar1 = smem_u32(&bars[0]), bar2 = smem_u32(&bars[1]), bar3 = smem_u32(&bars[2]);
 
-    {  // weights into shared memory; epilogue vectors after the operand buffer
+    {  // weights into shared memory; epilogue vectors after the operand buffers
         const uint4* src = reinterpret_cast<const uint4*>(a.img);
         for (int i = tid; i < (kImgW1 + kImgW2 + kImgW3) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
         for (int i = tid; i < kImgEp / 16; i += kTcThreads)
@@ -777,20 +821,31 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    proxy_fence();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
+    tc_handoff();
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    const uint32_t tm_a = tmem + lane_base;         // layer 1, then the output layer (columns 0..)
-    const uint32_t tm_b = tmem + 128u + lane_base;  // layer 2 (columns 128..255)
+    const uint32_t tm_1 = tmem + lane_base;         // layer 1 (columns 0..127)
+    const uint32_t tm_2 = tmem + 128u + lane_base;  // layer 2, then the output layer (columns 128..)
     const float* ep = reinterpret_cast<const float*>(sm + kSmEp);
     const uint32_t sW1 = smem_u32(sm + kSmW1), sW2 = smem_u32(sm + kSmW2), sW3 = smem_u32(sm + kSmW3);
-    const uint32_t sH = smem_u32(sm + kSmH);
-    uint32_t phase = 0;
-    uint32_t pending = 0;  // the barrier whose wait ran out, if any
+    const uint32_t sH = smem_u32(sm + kSmH), sX = smem_u32(sm + kSmX);
+    uint32_t phase = 0;  // parity of the current tile's completions (each barrier completes once per tile)
+    // the last commit and the parity it completes: it covers every earlier MMA
+    // of the issuing thread, so the error path waits on it alone
+    uint32_t last_bar = 0, last_par = 0;
     bool ok = true;
+
+    auto issue_layer1 = [&](uint32_t par) {
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < 2; s++)
+                mma_bf16(tmem, smem_desc(sX + 256u * s, 128u, 512u), smem_desc(sW1 + 256u * s, 128u, 512u),
+                         kIdesc128, s > 0);
+            mma_commit(bar1);
+        }
+        last_bar = bar1;
+        last_par = par;
+    };
 
     for (int32_t r = blockIdx.x; r < a.nrows && ok; r += gridDim.x) {
         const int32_t u = a.rows[r];
@@ -811,81 +866,52 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
         for (int i = 0; i < BM_FT; i++) ta[i] = a.tab[(size_t)u * BM_FT + i];
         __syncthreads();
         float* out_row = a.scores + (size_t)r * a.n;
+        // prologue: features and layer 1 of the row's first tile
+        build_features(a, ta, bits_out, bits_in, u, 1 + tid, sm, tid);
+        tc_handoff();
+        issue_layer1(phase);
         for (int32_t v0 = 1; v0 <= a.n; v0 += 128) {
             const int32_t v = v0 + tid;
-            const bool valid = v <= a.n && v != u;
-            {  // 1. features of this thread's candidate: the A operand of layer 1
-                float x[BM_MLP_IN];
-                if (valid) {
-                    float tb[BM_FT];
-                    const float4* t4 = reinterpret_cast<const float4*>(a.tab + (size_t)v * BM_FT);
-                    const float4 q0 = t4[0], q1 = t4[1], q2 = t4[2];
-                    tb[0] = q0.x; tb[1] = q0.y; tb[2] = q0.z; tb[3] = q0.w;
-                    tb[4] = q1.x; tb[5] = q1.y; tb[6] = q1.z; tb[7] = q1.w;
-                    tb[8] = q2.x; tb[9] = q2.y; tb[10] = q2.z; tb[11] = q2.w;
-                    const bool buv = (bits_out[v >> 5] >> (v & 31)) & 1u;
-                    const bool bvu = (bits_in[v >> 5] >> (v & 31)) & 1u;
-                    pair_features_raw(ta, tb, buv, bvu, x);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < BM_MLP_IN; i++) x[i] = 0.f;
-                }
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    uint4 q = make_uint4(0u, 0u, 0u, 0u);
-                    if (c < 3) {
-                        q.x = cvt_bf16x2(x[8 * c + 0], x[8 * c + 1]);
-                        q.y = cvt_bf16x2(x[8 * c + 2], x[8 * c + 3]);
-                        q.z = cvt_bf16x2(x[8 * c + 4], x[8 * c + 5]);
-                        q.w = cvt_bf16x2(x[8 * c + 6], x[8 * c + 7]);
-                    }
-                    *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 8 * c, 32)) = q;
-                }
-            }
-            proxy_fence();
-            tc_fence_before();
-            __syncthreads();
+            // layer 1 done: its epilogue fills H with h1
+            if (!__syncthreads_and(mbar_wait(bar1, phase))) { ok = false; break; }
             tc_fence_after();
-            if (tid == 0) {  // 2. layer 1
-#pragma unroll
-                for (int s = 0; s < 2; s++)
-                    mma_bf16(tmem, smem_desc(sH + 256u * s, 128u, 512u), smem_desc(sW1 + 256u * s, 128u, 512u),
-                             kIdesc128, s > 0);
-                mma_commit(bar1);
-            }
-            // completion tests are made block-uniform before any tcgen05.ld
-            if (!__syncthreads_and(mbar_wait(bar1, phase))) { ok = false; pending = bar1; break; }
-            tc_fence_after();
-            hidden_epilogue(tm_a, ep, sm, tid);
-            proxy_fence();
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
-            if (tid == 0) {  // 3. layer 2
+            hidden_epilogue(tm_1, ep, sm, tid);
+            tc_handoff();
+            if (tid == 0) {  // layer 2
 #pragma unroll
                 for (int s = 0; s < 8; s++)
                     mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, 2048u),
                              smem_desc(sW2 + 256u * s, 128u, 2048u), kIdesc128, s > 0);
                 mma_commit(bar2);
             }
-            if (!__syncthreads_and(mbar_wait(bar2, phase))) { ok = false; pending = bar2; break; }
+            last_bar = bar2;
+            last_par = phase;
+            // next tile's features and layer 1 while layer 2 runs (X and columns
+            // 0..127 are free: layer 1 of this tile completed and was read back)
+            const bool more = v0 + 128 <= a.n;
+            if (more) {
+                build_features(a, ta, bits_out, bits_in, u, v + 128, sm, tid);
+                tc_handoff();
+                issue_layer1(phase ^ 1u);
+            }
+            // layer 2 done: its epilogue writes h2 over h1
+            if (!__syncthreads_and(mbar_wait(bar2, phase))) { ok = false; break; }
             tc_fence_after();
-            hidden_epilogue(tm_b, ep + 128, sm, tid);
-            proxy_fence();
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
-            if (tid == 0) {  // 4. output layer, N = 16 (row 0 of B holds w3)
+            hidden_epilogue(tm_2, ep + 128, sm, tid);
+            tc_handoff();
+            if (tid == 0) {  // output layer, N = 16 (row 0 of B holds w3), into columns 128..143
 #pragma unroll
                 for (int s = 0; s < 8; s++)
-                    mma_bf16(tmem, smem_desc(sH + 256u * s, 128u, 2048u), smem_desc(sW3 + 256u * s, 128u, 2048u),
-                             kIdesc16, s > 0);
+                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, 2048u),
+                             smem_desc(sW3 + 256u * s, 128u, 2048u), kIdesc16, s > 0);
                 mma_commit(bar3);
             }
-            if (!__syncthreads_and(mbar_wait(bar3, phase))) { ok = false; pending = bar3; break; }
+            last_bar = bar3;
+            last_par = phase;
+            if (!__syncthreads_and(mbar_wait(bar3, phase))) { ok = false; break; }
             tc_fence_after();
-            const float o = tmem_ld1(tm_a);
-            if (v <= a.n) out_row[v - 1] = valid ? o + ep[384] : -INFINITY;
+            const float o = tmem_ld1(tm_2);
+            if (v <= a.n) out_row[v - 1] = (v != u) ? o + ep[384] : -INFINITY;
             phase ^= 1u;
             tc_fence_before();
             __syncthreads();
@@ -896,7 +922,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
-        if (!ok) mbar_wait(pending, phase);  // let the late MMA finish before its columns are freed
+        if (!ok) mbar_wait(last_bar, last_par);  // let the MMAs in flight finish before the columns are freed
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
     }
@@ -1741,8 +1767,8 @@ extern "C" bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* M, const int32_t* ro
         if (pos >= nr) {
             pos = 0;
             prog->sweeps++;
-            if (pass_accepts == 0) {
-                // the proposals found nothing in a whole pass: an exact pass judges
+            if (pass_accepts <= (int64_t)std::max(0, p->fallback_accepts)) {
+                // the proposals found (almost) nothing in a whole pass: an exact pass judges
                 if (p->exact_fallback) {
                     ta = clk::now();
                     bm_progress ex;
@@ -1757,7 +1783,7 @@ extern "C" bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* M, const int32_t* ro
                     if (s != BM_OK && s != BM_TIMEOUT) return s;
                     if (s == BM_TIMEOUT) { ret = BM_TIMEOUT; break; }
                     if (ex.accepts == 0 || ex.converged) { prog->converged = 1; break; }
-                } else {
+                } else if (pass_accepts == 0) {
                     prog->converged = 1;
                     break;
                 }

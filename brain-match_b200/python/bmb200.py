@@ -69,7 +69,8 @@ class SaStats(C.Structure):
 
 class LearnedParams(C.Structure):
     _fields_ = [("topk", C.c_int32), ("rows_per_batch", C.c_int32), ("refresh_batches", C.c_int32),
-                ("uniform", C.c_int32), ("exact_fallback", C.c_int32), ("train_every", C.c_int32),
+                ("uniform", C.c_int32), ("exact_fallback", C.c_int32), ("fallback_accepts", C.c_int32),
+                ("train_every", C.c_int32),
                 ("train_batch", C.c_int32), ("lr", C.c_float), ("weight_decay", C.c_float), ("seed", C.c_uint64),
                 ("max_accepts", C.c_int64), ("max_sweeps", C.c_int32), ("time_budget_s", C.c_double),
                 ("target_score", C.c_int64)]
@@ -785,12 +786,12 @@ class Mlp:
         return loss.value
 
     def search(self, rows=None, topk=64, rows_per_batch=0, refresh_batches=1, uniform=False, exact_fallback=True,
-               train_every=0, train_batch=4096, lr=1e-3, weight_decay=0.0, seed=1, max_accepts=-1, max_sweeps=-1,
-               time_budget=0.0, target_score=0, prog=None, stats=None):
+               fallback_accepts=0, train_every=0, train_batch=4096, lr=1e-3, weight_decay=0.0, seed=1,
+               max_accepts=-1, max_sweeps=-1, time_budget=0.0, target_score=0, prog=None, stats=None):
         """bm_search_learned; returns (status, Progress, LearnedStats)."""
         prm = LearnedParams(topk, rows_per_batch, refresh_batches, int(bool(uniform)), int(bool(exact_fallback)),
-                            train_every, train_batch, lr, weight_decay, seed, max_accepts, max_sweeps, time_budget,
-                            target_score)
+                            fallback_accepts, train_every, train_batch, lr, weight_decay, seed, max_accepts,
+                            max_sweeps, time_budget, target_score)
         prog = prog or Progress()
         stats = stats or LearnedStats()
         r = None if rows is None else _i32(rows)

@@ -372,7 +372,9 @@ typedef struct bm_learned_params {
     int32_t rows_per_batch;   /* rows per launch (0: 2 x SMs) */
     int32_t refresh_batches;  /* feature table refreshed every this many batches (0: 1) */
     int32_t uniform;          /* 1: uniform random partners instead of the model (the judge) */
-    int32_t exact_fallback;   /* 1: after a pass without accepts, an exact row pass decides convergence */
+    int32_t exact_fallback;   /* 1: after a pass with at most fallback_accepts accepts, an exact row pass
+                                 runs; a pass of it without accepts ends the search (converged) */
+    int32_t fallback_accepts; /* threshold of the above (0: only passes without accepts) */
     int32_t train_every;      /* online AdamW step every this many batches (0: no online training) */
     int32_t train_batch;      /* records per online step (0: 4096) */
     float lr, weight_decay;
