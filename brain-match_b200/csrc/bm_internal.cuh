@@ -145,7 +145,7 @@ inline HashView hview(const DevGraph& g) { return HashView{g.hash, g.hash_log2, 
 // Weight of B edge g->h (B ids), 0 if absent.  Linear probing read two slots
 // (16 bytes) at a time from the even slot at or below the home slot; in the
 // first pair a slot before the home slot is not part of the probe sequence.
-// The table is at most 3/4 full, so an empty slot ends every sequence; the
+// The table is at most half full, so an empty slot ends every sequence; the
 // loop is also bounded by the table size.
 __device__ __forceinline__ int32_t bm_hash_get(const HashView& hv, int32_t g, int32_t h) {
     const unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;

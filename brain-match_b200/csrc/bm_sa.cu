@@ -10,13 +10,16 @@
 // bit on the CPU; every chain ends on its final mapping and score, like the
 // reference's return value (:407).
 //
-// One CTA runs one chain.  Its K warps evaluate the K proposals of steps
-// s..s+K-1 under the current mapping; the first accepted one in step order is
-// applied and the rest are discarded, so the chain is exactly the one-at-a-
-// time chain for every K (the step counter moves past the accepted proposal,
-// or by K when none is accepted).  K and the block size are the tuning knobs.
-// A launch advances every chain by at most `chunk` proposals; the launch is
-// captured once in a CUDA graph and replayed until all chains finish.
+// One CTA runs one chain.  Each iteration evaluates the K proposals of steps
+// s..s+K-1 under the current mapping with the whole CTA (their list entries
+// are spread over all warps, so a proposal touching a hub does not stall the
+// others); the first accepted one in step order is applied and the rest are
+// discarded, so the chain is exactly the one-at-a-time chain for every K (the
+// step counter moves past the accepted proposal, or by K when none is
+// accepted).  K is the tuning knob; the chain's mapping lives in shared memory
+// when it fits.  A launch advances every chain by at most `chunk` proposals;
+// the launch is captured once in a CUDA graph and replayed until all chains
+// finish.
 #include <algorithm>
 #include <chrono>
 #include <mutex>
@@ -59,59 +62,41 @@ struct SaArgs {
     const PairDev* pairs;
     ChainDev* chains;
     int32_t nchains;
+    int32_t K;        // proposals evaluated per iteration (1..16)
+    int32_t pi_smem;  // 1: the chain's mapping is kept in shared memory
     uint64_t steps;
     uint64_t chunk;
     double t0;
     double log_ratio;
 };
 
-// Exact delta of swapping pi(u), pi(v) for one chain, computed by one warp
-// (the per-pair identity of bm_pairs.cu).
-// pi and ov are written by the same kernel (chain_apply_block), so they are
-// read with plain coherent loads, never through the read-only path.
-__device__ long long chain_delta_warp(const PairDev& P, const int32_t* pi, const int32_t* ov, int32_t u, int32_t v,
-                                      int lane) {
-    const int32_t fu = pi[u], fv = pi[v];
-    long long s = 0;
-    int32_t corr = 0;
-    for (int side = 0; side < 2; side++) {
-        const int32_t me = side ? v : u, other = side ? u : v;
-        const int32_t fnew = side ? fu : fv;
-        {
-            const int32_t b = __ldg(P.Aout_ptr + me), e = __ldg(P.Aout_ptr + me + 1);
-            for (int32_t j = b + lane; j < e; j += 32) {
-                const uint32_t ent = __ldg(P.Aout_ent + j);
-                if (ent == 0) continue;
-                const int32_t x = bm_eid(ent), w = bm_ew(ent);
-                s += imin(w, bm_hash_get(P.hb, fnew, pi[x]));
-                if (side == 0 && x == other) corr += imin(w, bm_hash_get(P.hb, fu, fv)) + imin(w, bm_hash_get(P.hb, fv, fu));
-            }
-        }
-        {
-            const int32_t b = __ldg(P.Ain_ptr + me), e = __ldg(P.Ain_ptr + me + 1);
-            for (int32_t j = b + lane; j < e; j += 32) {
-                const uint32_t ent = __ldg(P.Ain_ent + j);
-                if (ent == 0) continue;
-                const int32_t x = bm_eid(ent), w = bm_ew(ent);
-                s += imin(w, bm_hash_get(P.hb, pi[x], fnew));
-                if (side == 0 && x == other) corr += imin(w, bm_hash_get(P.hb, fu, fv)) + imin(w, bm_hash_get(P.hb, fv, fu));
-            }
-        }
+constexpr int kSaThreads = 256;
+constexpr int kSaMaxK = 16;
+constexpr int kSaUnit = 32;    // list entries per work unit (one per lane)
+constexpr int kSaBatch = 4;    // units a warp takes at once
+
+// First probe of the B hash for (g, h): the two 8-byte slots at or below the
+// home slot, as bm_hash_get reads them first.  Returns true when that settles
+// the lookup (key found or an empty slot met) and sets *w; false means the
+// probe sequence continues and the caller falls back to bm_hash_get.
+__device__ __forceinline__ bool hash_probe_first(const HashView& hv, int32_t g, int32_t h, int32_t* w) {
+    const unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;
+    const unsigned long long s0 = bm_hash_slot0(key, hv.log2);
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(hv.tab + (s0 & ~1ull)));
+    if (!(s0 & 1ull)) {
+        if (v.x == BM_HASH_EMPTY) { *w = 0; return true; }
+        if ((v.x >> 16) == key) { *w = (int32_t)(v.x & 0xFFFFull); return true; }
     }
-    s += corr;
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    s -= (long long)ov[u] + (long long)ov[v];
-    if (P.has_self) {
-        const int32_t su = __ldg(P.selfA + u), sv = __ldg(P.selfA + v);
-        const int32_t bu = __ldg(P.selfB + fu), bv = __ldg(P.selfB + fv);
-        s += imin(su, bv) - imin(su, bu) + imin(sv, bu) - imin(sv, bv);
-    }
-    return s;
+    if (v.y == BM_HASH_EMPTY) { *w = 0; return true; }
+    if ((v.y >> 16) == key) { *w = (int32_t)(v.y & 0xFFFFull); return true; }
+    return false;
 }
 
 // Apply the swap pi(a) <-> pi(b) of one chain with the whole CTA: S updates of
 // every A entry incident to a or b (as apply_kernel in bm_apply.cu), then pi.
-__device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* ov, int32_t sa, int32_t sb) {
+// `pi` is the working copy (shared or global memory), `gpi` the chain's
+// mapping in global memory, updated too.
+__device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, int32_t* ov, int32_t sa, int32_t sb) {
     const int32_t fa = pi[sa], fb = pi[sb];
     for (int side = 0; side < 2; side++) {
         const int32_t me = side ? sb : sa, other = side ? sa : sb;
@@ -149,49 +134,204 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* ov, in
     if (threadIdx.x == 0) {
         pi[sa] = fb;
         pi[sb] = fa;
+        if (gpi != pi) {
+            gpi[sa] = fb;
+            gpi[sb] = fa;
+        }
     }
     __syncthreads();
 }
 
-__global__ void sa_chain_kernel(SaArgs a) {
+// One CTA runs one chain.  Each iteration draws the proposals of steps
+// s..s+K-1 and evaluates all of them at once under the current mapping: the
+// four A lists of each proposal (out(u), in(u), out(v), in(v)) are cut into
+// units of 32 entries that the warps take, four at a time, from a shared
+// counter, so a proposal touching a hub is spread over the whole CTA instead
+// of one warp.  Each entry contributes (the per-pair identity of bm_pairs.cu)
+//   out(u): min(w, B(pi v, pi x))   in(u): min(w, B(pi x, pi v))
+//   out(v): min(w, B(pi u, pi x))   in(v): min(w, B(pi x, pi u))
+// plus, for an entry of u whose other end is v, the direct-edge repair
+// min(w, B(pi u, pi v)) + min(w, B(pi v, pi u)); the unit sums meet in a
+// per-proposal shared counter, then
+//   delta = sum - S(u) - S(v) + self-loop terms.
+// The first accepted proposal in step order is applied and the rest are
+// discarded, so the chain is the one-at-a-time chain for every K.
+__global__ void __launch_bounds__(kSaThreads) sa_chain_kernel(SaArgs a) {
+    extern __shared__ int32_t s_pi_dyn[];
     const int c = blockIdx.x;
     if (c >= a.nchains) return;
-    __shared__ long long s_delta[32];
-    __shared__ int s_acc[32];
-    __shared__ int s_u[32], s_v[32];
+    __shared__ bm_proposal s_prop[kSaMaxK];
+    __shared__ int32_t s_valid[kSaMaxK];
+    __shared__ int32_t s_sum[kSaMaxK];
+    __shared__ int32_t s_seglen[4 * kSaMaxK];      // entries per list
+    __shared__ int32_t s_segbase[4 * kSaMaxK];     // offset of each list in its CSR
+    __shared__ int32_t s_acc[kSaMaxK];
+    __shared__ long long s_d[kSaMaxK];
+    __shared__ int32_t s_upre[4 * kSaMaxK + 1];    // unit prefix over the lists
+    __shared__ int32_t s_ctr;
+    __shared__ int32_t s_first;
+    __shared__ long long s_fdelta;
     ChainDev& ch = a.chains[c];
     const PairDev P = a.pairs[ch.pair];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, K = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int K = a.K;
+    const int nseg = 4 * K;
+    int32_t* gpi = ch.pi;
+    int32_t* pi = gpi;
+    if (a.pi_smem) {
+        for (int32_t i = tid; i <= P.n; i += blockDim.x) s_pi_dyn[i] = gpi[i];
+        pi = s_pi_dyn;
+        __syncthreads();
+    }
+    int32_t* ov = ch.ov;
     uint64_t step = ch.step;
     const uint64_t end = min(a.steps, step + a.chunk);
     long long score = ch.score, accepts = ch.accepts;
-    int32_t* pi = ch.pi;
-    int32_t* ov = ch.ov;
     while (step < end) {
-        const uint64_t s = step + (uint64_t)warp;
-        int acc = 0;
-        long long d = 0;
-        int32_t pu = 0, pv = 0;
-        if (s < end) {
-            const bm_proposal pr = bm_sa_proposal(ch.key, s, P.n);
-            pu = pr.u;
-            pv = pr.v;
-            d = chain_delta_warp(P, pi, ov, pu, pv, lane);
-            acc = bm_sa_accept(d, pr.uni, bm_sa_temperature(a.t0, a.log_ratio, s, a.steps)) ? 1 : 0;
+        // ---- proposals and their list lengths
+        if (tid < K) {
+            const uint64_t s = step + (uint64_t)tid;
+            s_valid[tid] = s < end;
+            if (s < end) s_prop[tid] = bm_sa_proposal(ch.key, s, P.n);
+            s_sum[tid] = 0;
         }
-        if (lane == 0) {
-            s_delta[warp] = d;
-            s_acc[warp] = acc;
-            s_u[warp] = pu;
-            s_v[warp] = pv;
+        if (tid == 0) s_ctr = 0;
+        __syncthreads();
+        if (tid < nseg) {
+            const int w = tid >> 2, kind = tid & 3;
+            int32_t len = 0, base = 0;
+            if (s_valid[w]) {
+                const int32_t me = kind < 2 ? s_prop[w].u : s_prop[w].v;
+                const int32_t* ptr = (kind & 1) ? P.Ain_ptr : P.Aout_ptr;
+                base = __ldg(ptr + me);
+                len = __ldg(ptr + me + 1) - base;
+            }
+            s_seglen[tid] = len;
+            s_segbase[tid] = base;
         }
         __syncthreads();
-        int first = -1;
-        for (int w = 0; w < K; w++)
-            if (s_acc[w]) { first = w; break; }
+        if (tid < 32) {  // unit prefix over at most 64 lists: two per lane
+            const int i0 = 2 * lane, i1 = 2 * lane + 1;
+            const int32_t n0 = i0 < nseg ? (s_seglen[i0] + kSaUnit - 1) / kSaUnit : 0;
+            const int32_t n1 = i1 < nseg ? (s_seglen[i1] + kSaUnit - 1) / kSaUnit : 0;
+            int32_t incl = n0 + n1;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int32_t excl = incl - n0 - n1;
+            if (i0 <= nseg) s_upre[i0] = excl;
+            if (i1 <= nseg) s_upre[i1] = excl + n0;
+            if (lane == 31) s_upre[nseg] = incl;  // the total (index 64 when K = 16)
+        }
+        __syncthreads();
+        const int32_t U = s_upre[nseg];
+        // ---- evaluate: warps take kSaBatch units at a time
+        for (;;) {
+            int32_t ub = 0;
+            if (lane == 0) ub = atomicAdd(&s_ctr, kSaBatch);
+            ub = __shfl_sync(0xffffffffu, ub, 0);
+            if (ub >= U) break;
+            int32_t val[kSaBatch], wid[kSaBatch];
+            uint32_t ent[kSaBatch];
+            int32_t gx[kSaBatch], fnew[kSaBatch], kindv[kSaBatch];
+#pragma unroll
+            for (int q = 0; q < kSaBatch; q++) {
+                const int32_t unit = ub + q;
+                ent[q] = 0;
+                wid[q] = -1;
+                kindv[q] = 0;
+                fnew[q] = 0;
+                if (unit < U) {
+                    int32_t lo = 0, hi = nseg;  // last list with s_upre[list] <= unit
+                    while (hi - lo > 1) {
+                        const int32_t mid = (lo + hi) >> 1;
+                        if (s_upre[mid] <= unit) lo = mid; else hi = mid;
+                    }
+                    const int w = lo >> 2, kind = lo & 3;
+                    wid[q] = w;
+                    kindv[q] = kind;
+                    const int32_t off = (unit - s_upre[lo]) * kSaUnit + lane;
+                    if (off < s_seglen[lo]) {
+                        const bool out = !(kind & 1);
+                        ent[q] = __ldg((out ? P.Aout_ent : P.Ain_ent) + s_segbase[lo] + off);
+                    }
+                    fnew[q] = kind < 2 ? pi[s_prop[w].v] : pi[s_prop[w].u];
+                }
+            }
+            // first hash probes of the batch issued together
+            bool done[kSaBatch];
+            int32_t bw[kSaBatch];
+#pragma unroll
+            for (int q = 0; q < kSaBatch; q++) {
+                done[q] = true;
+                bw[q] = 0;
+                gx[q] = 0;
+                if (ent[q] != 0) {
+                    gx[q] = pi[bm_eid(ent[q])];
+                    const bool out = !(kindv[q] & 1);
+                    done[q] = out ? hash_probe_first(P.hb, fnew[q], gx[q], &bw[q])
+                                  : hash_probe_first(P.hb, gx[q], fnew[q], &bw[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kSaBatch; q++) {
+                val[q] = 0;
+                if (ent[q] != 0) {
+                    const bool out = !(kindv[q] & 1);
+                    if (!done[q]) bw[q] = out ? bm_hash_get(P.hb, fnew[q], gx[q]) : bm_hash_get(P.hb, gx[q], fnew[q]);
+                    const int32_t w = bm_ew(ent[q]);
+                    val[q] = imin(w, bw[q]);
+                    if (kindv[q] < 2 && bm_eid(ent[q]) == s_prop[wid[q]].v) {
+                        const int32_t fu = pi[s_prop[wid[q]].u], fv = pi[s_prop[wid[q]].v];
+                        val[q] += imin(w, bm_hash_get(P.hb, fu, fv)) + imin(w, bm_hash_get(P.hb, fv, fu));
+                    }
+                }
+            }
+            // a unit lies in one list, hence one proposal: warp sum, one atomic
+#pragma unroll
+            for (int q = 0; q < kSaBatch; q++) {
+                if (wid[q] < 0) continue;  // uniform over the warp
+                int32_t v = val[q];
+#pragma unroll
+                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && v) atomicAdd(&s_sum[wid[q]], v);
+            }
+        }
+        __syncthreads();
+        // ---- deltas and acceptance, one thread per proposal; the first
+        // accepted one in step order wins
+        if (tid < K) {
+            int acc = 0;
+            long long d = 0;
+            if (s_valid[tid]) {
+                const bm_proposal pr = s_prop[tid];
+                d = (long long)s_sum[tid] - (long long)ov[pr.u] - (long long)ov[pr.v];
+                if (P.has_self) {
+                    const int32_t fu = pi[pr.u], fv = pi[pr.v];
+                    const int32_t su = __ldg(P.selfA + pr.u), sv = __ldg(P.selfA + pr.v);
+                    const int32_t bu = __ldg(P.selfB + fu), bv = __ldg(P.selfB + fv);
+                    d += imin(su, bv) - imin(su, bu) + imin(sv, bu) - imin(sv, bv);
+                }
+                acc = bm_sa_accept(d, pr.uni, bm_sa_temperature(a.t0, a.log_ratio, step + (uint64_t)tid, a.steps));
+            }
+            s_acc[tid] = acc;
+            s_d[tid] = d;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int first = -1;
+            for (int w = 0; w < K; w++)
+                if (s_acc[w]) { first = w; break; }
+            s_first = first;
+            s_fdelta = first >= 0 ? s_d[first] : 0;
+        }
+        __syncthreads();
+        const int first = s_first;
         if (first >= 0) {
-            chain_apply_block(P, pi, ov, s_u[first], s_v[first]);
-            score += s_delta[first];
+            chain_apply_block(P, pi, gpi, ov, s_prop[first].u, s_prop[first].v);
+            score += s_fdelta;
             accepts++;
             step += (uint64_t)first + 1;
         } else {
@@ -358,6 +498,25 @@ void tune_store(const std::string& key, int32_t cand) {
 
 }  // namespace
 
+namespace {
+
+// Shared memory for a chain's mapping when it fits (the largest n + 1 ints of
+// the launch), else the mapping stays in global memory.  Sets the kernel's
+// dynamic shared-memory limit; called before any stream capture.
+bm_status chain_smem(bm_ctx* ctx, SaArgs& args, int32_t n_max, size_t* smem) {
+    const size_t need = sizeof(int32_t) * ((size_t)n_max + 1);
+    *smem = 0;
+    args.pi_smem = 0;
+    if (need + 8192 <= ctx->smem_optin) {
+        args.pi_smem = 1;
+        *smem = need;
+        BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    }
+    return BM_OK;
+}
+
+}  // namespace
+
 extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chain_pair, const uint64_t* chain_key,
                                const int32_t* init_pi, const bm_sa_params* prm, int32_t* final_pi,
                                int64_t* final_score, int64_t* accepts, bm_sa_stats* stats) {
@@ -432,11 +591,16 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
     args.t0 = prm->t0;
     args.log_ratio = log(prm->t_end / prm->t0);
     args.chunk = prm->chunk > 0 ? (uint64_t)prm->chunk : (uint64_t)65536;
-    cudaFuncAttributes fa;
-    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel));
-    const int32_t kmax = std::max(1, std::min(16, fa.maxThreadsPerBlock / 32));
+    const int32_t kmax = kSaMaxK;
     int32_t K = prm->candidates;
     if (K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates %d above this build's limit %d", K, kmax);
+    int32_t n_max = 0;
+    for (int32_t c = 0; c < nchains; c++) n_max = std::max(n_max, b->pairs[(size_t)chain_pair[c]].n);
+    size_t smem = 0;
+    {
+        bm_status st = chain_smem(ctx, args, n_max, &smem);
+        if (st != BM_OK) return st;
+    }
     if (K == 0) {
         int64_t ntot = 0;
         for (int32_t c = 0; c < nchains; c++) ntot += b->pairs[(size_t)chain_pair[c]].n;
@@ -458,6 +622,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
                 sa_init_kernel<<<dim3(64, (unsigned)nchains), 256, 0, ctx->stream>>>(b->d_pairs, d_ch, nchains);
                 BM_LAUNCH_CHECK(ctx, "sa_init_kernel");
                 SaArgs t = args;
+                t.K = cand;
                 t.chunk = std::min<uint64_t>(4096, args.steps > 0 ? args.steps : 1);
                 struct Events {
                     cudaEvent_t a = nullptr, b = nullptr;
@@ -466,7 +631,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
                 BM_CUDA(ctx, cudaEventCreate(&ev.a));
                 BM_CUDA(ctx, cudaEventCreate(&ev.b));
                 BM_CUDA(ctx, cudaEventRecord(ev.a, ctx->stream));
-                sa_chain_kernel<<<nchains, 32 * cand, 0, ctx->stream>>>(t);
+                sa_chain_kernel<<<nchains, kSaThreads, smem, ctx->stream>>>(t);
                 BM_LAUNCH_CHECK(ctx, "sa_chain_kernel(tune)");
                 BM_CUDA(ctx, cudaEventRecord(ev.b, ctx->stream));
                 BM_CUDA(ctx, cudaEventSynchronize(ev.b));
@@ -490,8 +655,9 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
     if (launches > 0) {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
+        args.K = K;
         BM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        sa_chain_kernel<<<nchains, 32 * K, 0, ctx->stream>>>(args);
+        sa_chain_kernel<<<nchains, kSaThreads, smem, ctx->stream>>>(args);
         cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
         if (ce != cudaSuccess) return bm_cuda_fail(ctx, ce, "cudaStreamEndCapture");
         ce = cudaGraphInstantiate(&exec, graph, 0);
@@ -626,11 +792,11 @@ extern "C" bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32
         }
     }
     BM_CUDA(ctx, cudaSetDevice(ctx->device));
-    cudaFuncAttributes fa;
-    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel));
-    const int32_t kmax = std::max(1, std::min(16, fa.maxThreadsPerBlock / 32));
+    const int32_t kmax = kSaMaxK;
     int32_t K = prm->candidates == 0 ? std::min(8, kmax) : prm->candidates;
     if (K < 1 || K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates must be 0 or 1..%d", kmax);
+    int32_t n_max = 0;
+    for (int32_t c = 0; c < nchains; c++) n_max = std::max(n_max, b->pairs[(size_t)chain_pair[c]].n);
     unsigned char* base = nullptr;
     bm_status st = noalloc_scratch(ctx, &base);
     if (st != BM_OK) return st;
@@ -676,9 +842,12 @@ extern "C" bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32
     args.t0 = prm->t0;
     args.log_ratio = log(prm->t_end / prm->t0);
     args.chunk = prm->chunk > 0 ? (uint64_t)prm->chunk : (uint64_t)65536;
+    args.K = K;
+    size_t smem = 0;
+    if ((st = chain_smem(ctx, args, n_max, &smem)) != BM_OK) return st;
     const uint64_t launches = args.steps == 0 ? 0 : (args.steps + args.chunk - 1) / args.chunk;
     for (uint64_t l = 0; l < launches; l++) {
-        sa_chain_kernel<<<nchains, 32 * K, 0, ctx->stream>>>(args);
+        sa_chain_kernel<<<nchains, kSaThreads, smem, ctx->stream>>>(args);
         BM_LAUNCH_CHECK(ctx, "sa_chain_kernel");
     }
     if (final_pi)
