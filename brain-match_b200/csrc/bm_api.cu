@@ -383,8 +383,8 @@ extern "C" bm_status bm_event_elapsed_ms(bm_ctx* ctx, void* a, void* b, float* m
 
 extern "C" bm_status bm_set_row_tiling(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads) {
     if (!ctx) return BM_INVALID_ARG;
-    if (ctas_per_row != 0 && ctas_per_row != 1 && ctas_per_row != 2 && ctas_per_row != 4 && ctas_per_row != 8)
-        return bm_fail(ctx, BM_INVALID_ARG, "ctas_per_row must be 1, 2, 4 or 8");
+    if (ctas_per_row < 0 || ctas_per_row > 8)
+        return bm_fail(ctx, BM_INVALID_ARG, "ctas_per_row must be 0 (automatic) or 1..8");
     if (threads != 0 && threads != 256 && threads != 512)
         return bm_fail(ctx, BM_INVALID_ARG, "threads must be 256 or 512");
     if (ctas_per_row) ctx->row_ctas = ctas_per_row;

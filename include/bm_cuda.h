@@ -421,9 +421,9 @@ int64_t bm_launch_count(const bm_ctx* ctx);
 /* PCI bus id of the context's device ("0000:1b:00.0"), for NVML queries. */
 bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len);
 
-/* Tuning knobs of the row kernel: CTAs per row (1, 2, 4 or 8: a thread-block
- * cluster sharing the row through distributed shared memory) and threads per
- * CTA (256 or 512).  0 keeps the current value. */
+/* Tuning knobs of the row kernel: CTAs per row (1..8: a thread-block cluster
+ * sharing the row through distributed shared memory) and threads per CTA
+ * (256 or 512).  0 keeps the current value. */
 bm_status bm_set_row_tiling(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads);
 bm_status bm_get_row_tiling(bm_ctx* ctx, int32_t* ctas_per_row, int32_t* threads);
 /* How many row clusters of the given shape can be resident at once on the

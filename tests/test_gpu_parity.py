@@ -90,7 +90,8 @@ def test_rows_best_matches_full_rows(golden_cfg1, eng_cfg1):
         assert got == exp
 
 
-@pytest.mark.parametrize("ctas,threads", [(1, 256), (1, 512), (2, 512), (4, 256), (8, 512)])
+@pytest.mark.parametrize("ctas,threads", [(1, 256), (1, 512), (2, 512), (3, 512), (4, 256), (5, 256), (7, 512),
+                                          (8, 512)])
 def test_row_tiling_variants_agree(golden_cfg1, eng_cfg1, ctas, threads):
     rows = np.arange(1, 2001, 37, dtype=np.int32)
     exp = Oracle(*golden_graphs(golden_cfg1)).rows(golden_cfg1["pi_init"], rows)
@@ -229,7 +230,7 @@ def test_invalid_arguments(golden_small):
     with pytest.raises(bm.BMError):
         e.delta_rows(np.array([0], np.int32))
     with pytest.raises(bm.BMError):
-        e.set_row_tiling(3, 0)
+        e.set_row_tiling(9, 0)
     assert e.score() == int(golden_small["score_init"])  # context still usable
     e.close()
 
