@@ -340,6 +340,7 @@ def run_ours(args, ws, rank, local, dist):
     if rank == 0 and ws == 1 and args.learned_seconds > 0 and out.get("search", {}).get("converged"):
         out["learned_vs_plain"] = learned_compare(local, A, B, init, rows, out["search"], args.learned_seconds)
     if rank == 0 and ws == 1 and not args.no_extras:
+        out["initial_matching"] = initial_matching(local, A, B, init)
         out["higher_order"] = higher_order(local, A, B, init)
         out["sa_chains"] = sa_chains(local, args.sa_steps)
     if rank == 0:
@@ -522,6 +523,21 @@ def sa_chains(device, steps):
     batch.close()
     e.close()
     return out
+
+
+def initial_matching(device, A, B, init):
+    """Greedy-similarity initial matching of the full-scale pair: the host
+    library (all host cores) and the device version, which must agree."""
+    t = time.perf_counter()
+    host = bm.greedy_match(A, B)
+    th = time.perf_counter() - t
+    with bm.Engine(device) as e:
+        e.greedy_match(A, B)
+        t = time.perf_counter()
+        dev = e.greedy_match(A, B)
+        td = time.perf_counter() - t
+    return {"host_seconds": th, "device_seconds": td, "equal": bool(np.array_equal(host, dev)),
+            "equals_workload_init": bool(np.array_equal(dev, init)), "host_cores": os.cpu_count()}
 
 
 def plain_search(eng, rows, seconds):

@@ -165,6 +165,7 @@ def cuda_lib() -> C.CDLL:
             "bm_sa_run": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.POINTER(SaParams), vp, vp, vp, C.POINTER(SaStats)]),
             "bm_sa_layout_size": (C.c_int64, [vp, C.c_int32, vp]),
             "bm_get_row_tiling": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "bm_greedy_match_dev": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, C.c_int64, vp, vp, vp]),
             "bm_mlp_create": (C.c_int, [vp, C.c_uint64, C.POINTER(vp)]),
             "bm_mlp_destroy": (None, [vp]),
             "bm_mlp_num_params": (C.c_int32, []),
@@ -557,6 +558,14 @@ class Engine:
                                        C.byref(prog), C.byref(best))
         self._chk(st, "bm_search_restarts", ok=(BM_OK, BM_TIMEOUT))
         return prog, best.value, st
+
+    def greedy_match(self, A: Graph, B: Graph) -> np.ndarray:
+        """Greedy-similarity initial matching on the device (n+1 ints)."""
+        n = max(A.n, B.n)
+        pi = np.zeros(n + 1, np.int32)
+        self._chk(self.L.bm_greedy_match_dev(self.h, n, A.m, _ptr(A.src), _ptr(A.dst), B.m, _ptr(B.src),
+                                             _ptr(B.dst), _ptr(pi)), "bm_greedy_match_dev")
+        return pi
 
     def set_row_tiling(self, ctas_per_row: int = 0, threads: int = 0) -> None:
         self._chk(self.L.bm_set_row_tiling(self.h, ctas_per_row, threads), "bm_set_row_tiling")

@@ -299,6 +299,20 @@ bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32_t* chain_p
                             const int32_t* init_pi, const bm_sa_params* params, int32_t* final_pi,
                             int64_t* final_score, int64_t* accepts);
 
+/* ------------------------------------------------------- initial matching */
+
+/* Greedy-similarity initial matching on the device: the algorithm of
+ * src/greedy-match.c (features compute_vertex_features/compute_2hop_metrics
+ * :213-293; vertices sorted by descending feature sum :295-300; each A vertex
+ * in turn takes the unmatched B vertex at the smallest L1 feature distance
+ * :442-530), ties broken by vertex id; the same mapping as bm_greedy_match in
+ * bm_host.h.  Edge lists with ids 1..n; weights are not used and duplicate
+ * edges count, like the reference's adjacency lists.  pi receives n+1 ints
+ * (slot 0 = 0).  The context provides the device and stream only; its graphs
+ * and mapping are not touched. */
+bm_status bm_greedy_match_dev(bm_ctx* ctx, int32_t n, int64_t mA, const int32_t* srcA, const int32_t* dstA,
+                              int64_t mB, const int32_t* srcB, const int32_t* dstB, int32_t* pi);
+
 /* ------------------------------------------------------ learned proposals */
 
 /* A 24 -> 128 -> 128 -> 1 MLP that scores swap partners v of a vertex u from
