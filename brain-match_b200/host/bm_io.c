@@ -215,6 +215,41 @@ int bm_read_mapping(const char* path, int32_t n, int32_t* pi, int64_t* count, in
     return 0;
 }
 
+int bm_read_mapping_pairs(const char* path, int32_t** a, int32_t** b, int64_t* count) {
+    size_t len = 0;
+    char* buf = slurp(path, &len);
+    if (!buf) return -1;
+    const char* end = buf + len;
+    int64_t cap = 1024, cnt = 0;
+    int32_t* xa = (int32_t*)malloc(sizeof(int32_t) * (size_t)cap);
+    int32_t* xb = (int32_t*)malloc(sizeof(int32_t) * (size_t)cap);
+    if (!xa || !xb) { free(xa); free(xb); free(buf); return -1; }
+    const char* p = next_line(buf, end);
+    while (p < end) {
+        const char* le = next_line(p, end);
+        long long x, y;
+        if (parse_mapping_line(p, le, &x, &y)) {
+            if (cnt == cap) {
+                cap *= 2;
+                int32_t* na = (int32_t*)realloc(xa, sizeof(int32_t) * (size_t)cap);
+                if (na) xa = na;
+                int32_t* nb = (int32_t*)realloc(xb, sizeof(int32_t) * (size_t)cap);
+                if (nb) xb = nb;
+                if (!na || !nb) { free(xa); free(xb); free(buf); return -1; }
+            }
+            xa[cnt] = (int32_t)(x > 0x7fffffff ? 0x7fffffff : (x < -0x7fffffff ? -0x7fffffff : x));
+            xb[cnt] = (int32_t)(y > 0x7fffffff ? 0x7fffffff : (y < -0x7fffffff ? -0x7fffffff : y));
+            cnt++;
+        }
+        p = le;
+    }
+    free(buf);
+    *a = xa;
+    *b = xb;
+    *count = cnt;
+    return 0;
+}
+
 int bm_write_mapping(const char* path, int32_t n, const int32_t* pi) {
     size_t plen = strlen(path);
     char* tmp = (char*)malloc(plen + 32);

@@ -47,6 +47,12 @@ int bm_read_mapping(const char* path, int32_t n, int32_t* pi, int64_t* count, in
  * is written under a temporary name and renamed. */
 int bm_write_mapping(const char* path, int32_t n, const int32_t* pi);
 
+/* Every (male, female) id pair of a mapping file in file order (header
+ * skipped, malformed lines skipped), as two malloc'd arrays the caller frees.
+ * For checkers that must see duplicate assignments (verify-mapping,
+ * src/verify-mapping.c:113-232). */
+int bm_read_mapping_pairs(const char* path, int32_t** male, int32_t** female, int64_t* count);
+
 /* Largest id in a mapping file without storing it (to size arrays). */
 int bm_scan_mapping_max_id(const char* path, int32_t* max_id);
 
