@@ -99,6 +99,7 @@ extern "C" void bm_ctx_destroy(bm_ctx* ctx) {
     cudaFree(ctx->d_score);
     cudaFree(ctx->stage);
     cudaFree(ctx->flush_buf);
+    cudaFree(ctx->tscr);
     if (ctx->hstage) cudaFreeHost(ctx->hstage);
     cudaStreamDestroy(ctx->stream);
     delete ctx;

@@ -86,6 +86,8 @@ struct bm_ctx {
     size_t hstage_bytes = 0;
     void* flush_buf = nullptr;
     size_t flush_bytes = 0;
+    void* tscr = nullptr;           // scratch of the delta-table top-K
+    size_t tscr_bytes = 0;
     int64_t launches = 0;
     int32_t row_ctas = 0;           // CTAs per row (cluster size); 0 = auto
     int32_t row_threads = 512;
@@ -175,6 +177,10 @@ bm_status bm_launch_relabel(bm_ctx* ctx);
 bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_out);
 bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
                          int64_t* d_full, bm_row_result* d_res);
+// Same with a delta-table output: entry (u, v) of row u at d_tab[u * tab_ld + v]
+// as int32, and with tab_sym also (v, u).
+bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
+                            int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym);
 bm_status bm_launch_apply(bm_ctx* ctx, const int32_t* d_pairs, int32_t k);
 bm_status bm_rows_smem_check(bm_ctx* ctx);
 bm_status bm_launch_kset(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t nsets, long long* d_best,

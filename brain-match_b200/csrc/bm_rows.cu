@@ -66,6 +66,9 @@ struct RowArgs {
     int32_t nrows;
     int64_t* full;
     bm_row_result* res;
+    int32_t* tab;      // delta table: entry (u, v) at u * tab_ld + v (int32; |delta| < 2^31 checked)
+    int64_t tab_ld;
+    int32_t tab_sym;   // also write entry (v, u)
 };
 
 struct Partial {
@@ -391,6 +394,10 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 }
             }
             if (frow) frow[v] = d;
+            if (a.tab && valid) {
+                a.tab[(size_t)u * (size_t)a.tab_ld + (size_t)v] = (int32_t)d;
+                if (a.tab_sym && v >= 1 && v != u) a.tab[(size_t)v * (size_t)a.tab_ld + (size_t)u] = (int32_t)d;
+            }
         }
     }
     if (a.res) {
@@ -496,6 +503,11 @@ bm_status bm_rows_smem_check(bm_ctx* ctx) {
 
 bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows, int64_t* d_full,
                          bm_row_result* d_res) {
+    return bm_launch_rows_ex(ctx, d_rows, d_col_lo, nrows, d_full, d_res, nullptr, 0, 0);
+}
+
+bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
+                            int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym) {
     if (nrows <= 0) return BM_OK;
     bm_status st = bm_rows_smem_check(ctx);
     if (st != BM_OK) return st;
@@ -522,6 +534,9 @@ bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_co
     args.col_lo = d_col_lo;
     args.full = d_full;
     args.res = d_res;
+    args.tab = d_tab;
+    args.tab_ld = tab_ld;
+    args.tab_sym = tab_sym;
     int cl = ctx->row_ctas;
     if (cl == 0) {
         // two CTAs fit per SM: the largest cluster size with nrows*cl <= 2*SMs

@@ -166,6 +166,12 @@ def cuda_lib() -> C.CDLL:
             "bm_sa_layout_size": (C.c_int64, [vp, C.c_int32, vp]),
             "bm_get_row_tiling": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "bm_greedy_match_dev": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, C.c_int64, vp, vp, vp]),
+            "bm_delta_table_dev": (C.c_int, [vp, vp, C.c_int64]),
+            "bm_table_refresh_dev": (C.c_int, [vp, vp, C.c_int64, vp, C.c_int32]),
+            "bm_table_topk": (C.c_int, [vp, vp, C.c_int64, C.c_int32, vp, vp, C.POINTER(C.c_int32)]),
+            "bm_table_topk_dev": (C.c_int, [vp, vp, C.c_int64, C.c_int32, vp, vp, vp]),
+            "bm_search_table": (C.c_int, [vp, vp, C.c_int64, C.c_int32, C.c_int64, C.c_int32, C.c_double,
+                                          C.POINTER(Progress)]),
             "bm_mlp_create": (C.c_int, [vp, C.c_uint64, C.POINTER(vp)]),
             "bm_mlp_destroy": (None, [vp]),
             "bm_mlp_num_params": (C.c_int32, []),
@@ -558,6 +564,46 @@ class Engine:
                                        C.byref(prog), C.byref(best))
         self._chk(st, "bm_search_restarts", ok=(BM_OK, BM_TIMEOUT))
         return prog, best.value, st
+
+    # delta table (device array owned by the caller; see bm_delta_table_dev)
+    def table_alloc(self):
+        """A device int32 table for this context's n: returns (pointer, ld)."""
+        ld = (self.n + 1 + 3) & ~3
+        return self.dev_alloc(4 * (self.n + 1) * ld), ld
+
+    def delta_table_dev(self, d_tab: int, ld: int) -> None:
+        self._chk(self.L.bm_delta_table_dev(self.h, d_tab, ld), "bm_delta_table_dev")
+
+    def table_refresh_dev(self, d_tab: int, ld: int, rows) -> None:
+        r = _i32(rows)
+        d_r = self.dev_alloc(max(4, r.nbytes))
+        try:
+            self.h2d(d_r, r)
+            self._chk(self.L.bm_table_refresh_dev(self.h, d_tab, ld, d_r, r.shape[0]), "bm_table_refresh_dev")
+            self.sync()
+        finally:
+            self.dev_free(d_r)
+
+    def table_download(self, d_tab: int, ld: int) -> np.ndarray:
+        out = np.zeros((self.n + 1, ld), np.int32)
+        self.sync()
+        self.d2h(out, d_tab)
+        return out
+
+    def table_topk(self, d_tab: int, ld: int, k: int):
+        pairs = np.zeros((k, 2), np.int32)
+        deltas = np.zeros(k, np.int64)
+        cnt = C.c_int32()
+        self._chk(self.L.bm_table_topk(self.h, d_tab, ld, k, _ptr(pairs), _ptr(deltas), C.byref(cnt)),
+                  "bm_table_topk")
+        return pairs[:cnt.value], deltas[:cnt.value]
+
+    def search_table(self, d_tab: int, ld: int, k: int = 1024, max_accepts: int = -1, max_rounds: int = -1,
+                     time_budget: float = 0.0, prog=None):
+        prog = prog or Progress()
+        st = self.L.bm_search_table(self.h, d_tab, ld, k, max_accepts, max_rounds, time_budget, C.byref(prog))
+        self._chk(st, "bm_search_table", ok=(BM_OK, BM_TIMEOUT))
+        return prog, st
 
     def greedy_match(self, A: Graph, B: Graph) -> np.ndarray:
         """Greedy-similarity initial matching on the device (n+1 ints)."""

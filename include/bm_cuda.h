@@ -299,6 +299,40 @@ bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32_t* chain_p
                             const int32_t* init_pi, const bm_sa_params* params, int32_t* final_pi,
                             int64_t* final_score, int64_t* accepts);
 
+/* ------------------------------------------------------------ delta table */
+
+/* The table of every pair's exact delta, the score-lookup engine of
+ * src/best-swap/score-lookup.c (create_score_lookup :246-293), kept exact:
+ * entry (u, v) of a device int32 array at d_table[u * ld + v] for
+ * 1 <= u, v <= n (0 on the diagonal and in row and column 0), ld >= n + 1.
+ * The caller owns the array ((n + 1) * ld * 4 bytes: 1.37 GB at n = 18,524).
+ * Deltas fit int32 (the engine rejects weighted degrees that could overflow);
+ * the reference truncates them to short. */
+bm_status bm_delta_table_dev(bm_ctx* ctx, int32_t* d_table, int64_t ld);
+/* Recompute rows d_rows[0..nrows) and the matching columns.  After a swap of
+ * a and b, the rows of a, b and their A neighbours are all that change (the
+ * reference's update_lookup_and_heap, :129-244, recomputes the pairs of a and b
+ * only and lets the rest go stale). */
+bm_status bm_table_refresh_dev(bm_ctx* ctx, int32_t* d_table, int64_t ld, const int32_t* d_rows, int32_t nrows);
+/* The k (1..4096) best pairs u < v of the table, largest delta first, then
+ * smallest u, then smallest v: the order the reference's max-heap
+ * (heap.c:79-164) extracts swaps in, with its ties made deterministic.
+ * pairs receives 2*count ints, deltas count values; count = min(k, n(n-1)/2).
+ * _dev: device outputs (count may be NULL), asynchronous. */
+bm_status bm_table_topk(bm_ctx* ctx, const int32_t* d_table, int64_t ld, int32_t k, int32_t* pairs,
+                        int64_t* deltas, int32_t* count);
+bm_status bm_table_topk_dev(bm_ctx* ctx, const int32_t* d_table, int64_t ld, int32_t k, int32_t* d_pairs,
+                            int64_t* d_deltas, int32_t* d_count);
+/* Best-swap search on the table (the optimize loop of score-lookup,
+ * :530-…, without its annealing phases): take the k best pairs, apply the
+ * improving ones that are independent of better ones (bm_select_independent's
+ * rule), refresh the changed rows, repeat until the best delta is <= 0 or a
+ * budget ends.  The table must hold the current mapping's deltas
+ * (bm_delta_table_dev) and stays exact; every call ends with a full re-score
+ * (BM_PARITY_FAIL on a mismatch). */
+bm_status bm_search_table(bm_ctx* ctx, int32_t* d_table, int64_t ld, int32_t k, int64_t max_accepts,
+                          int32_t max_rounds, double time_budget_s, bm_progress* prog);
+
 /* ------------------------------------------------------- initial matching */
 
 /* Greedy-similarity initial matching on the device: the algorithm of
