@@ -334,8 +334,11 @@ def run_ours(args, ws, rank, local, dist):
         out["clocks"] = clk
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(A, B, init, rows, starts[args.warmup:], budget_s=args.ref_seconds)
+    converged_pi = None
     if rank == 0 and ws == 1 and args.search_seconds > 0:
         out["search"] = plain_search(eng, rows, args.search_seconds)
+        if out["search"]["converged"]:
+            converged_pi = eng.get_mapping()
     eng.close()
     if rank == 0 and ws == 1 and args.learned_seconds > 0 and out.get("search", {}).get("converged"):
         out["learned_vs_plain"] = learned_compare(local, A, B, init, rows, out["search"], args.learned_seconds)
@@ -343,6 +346,10 @@ def run_ours(args, ws, rank, local, dist):
         out["initial_matching"] = initial_matching(local, A, B, init)
         out["higher_order"] = higher_order(local, A, B, init)
         out["delta_table"] = delta_table(local, A, B, init, out.get("search", {}))
+        out["subset_assignment"] = [subset_assignment(local, A, B, init, "initial matching")]
+        if converged_pi is not None:
+            out["subset_assignment"].append(subset_assignment(local, A, B, converged_pi,
+                                                              "plain search's local optimum"))
         out["sa_chains"] = sa_chains(local, args.sa_steps)
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -569,6 +576,21 @@ def delta_table(device, A, B, init, plain):
                "plain_score": plain.get("score"), "plain_seconds": plain.get("seconds")}
         e.dev_free(d_tab)
     return out
+
+
+def subset_assignment(device, A, B, start_pi, label):
+    """Independent-subset re-assignment (random A-independent subsets of up
+    to 4,096 members, optimal assignment of their images) from a given
+    mapping: time per iteration and the score it adds."""
+    with bm.Engine(device) as e:
+        e.set_graphs(A, B)
+        e.set_mapping(start_pi)
+        s0 = e.score()
+        prog, st = e.search_hungarian(k=4096, seed=5, iterations=10)
+        return {"start": label, "start_score": int(s0), "score": int(prog.score), "gain": int(prog.score - s0),
+                "iterations": int(prog.launches), "members_per_iteration": int(prog.rows_done // max(1, prog.launches)),
+                "moved": int(prog.accepts), "seconds": prog.seconds,
+                "seconds_per_iteration": prog.seconds / max(1, prog.launches)}
 
 
 def plain_search(eng, rows, seconds):

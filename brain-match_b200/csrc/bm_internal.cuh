@@ -181,6 +181,12 @@ bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_co
 // as int32, and with tab_sym also (v, u).
 bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
                             int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym);
+// One-sided mode: for each row u, G_u(pi v) - S(u) + self-loop term at the
+// columns v = d_cols[0..ncols), into d_colout[r * ncols + j] (int32): the gain
+// of u alone taking v's image with every other vertex fixed.
+bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
+                             int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym,
+                             const int32_t* d_cols, int32_t ncols, int32_t* d_colout);
 bm_status bm_launch_apply(bm_ctx* ctx, const int32_t* d_pairs, int32_t k);
 bm_status bm_rows_smem_check(bm_ctx* ctx);
 bm_status bm_launch_kset(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t nsets, long long* d_best,

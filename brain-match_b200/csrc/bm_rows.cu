@@ -69,6 +69,13 @@ struct RowArgs {
     int32_t* tab;      // delta table: entry (u, v) at u * tab_ld + v (int32; |delta| < 2^31 checked)
     int64_t tab_ld;
     int32_t tab_sym;   // also write entry (v, u)
+    // one-sided mode: only T1 + T2 (u's own edges moved to pi v, everything
+    // else fixed), read at the columns cols[0..ncols): colout[r * ncols + j] =
+    // G_u(pi cols[j]) - S(u) + self-loop term
+    int32_t half;
+    const int32_t* cols;
+    int32_t ncols;
+    int32_t* colout;
 };
 
 struct Partial {
@@ -144,7 +151,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
         const int32_t ai = __ldg(a.Ain_ptr + u), d2 = __ldg(a.Ain_ptr + u + 1) - ai;
         const int32_t bo = __ldg(a.Bout_ptr + fu), d3 = __ldg(a.Bout_ptr + fu + 1) - bo;
         const int32_t bi = __ldg(a.Bin_ptr + fu), d4 = __ldg(a.Bin_ptr + fu + 1) - bi;
-        const int32_t F = d1 + d2 + d3 + d4;
+        const int32_t F = a.half ? d1 + d2 : d1 + d2 + d3 + d4;
         const int32_t dA = d1 + d2;
         // ---- direct-edge corrections C, for A entries (x, w) of u:
         //   acc[x] += min(w, B(pi u, pi x)) + min(w, B(pi x, pi u)).
@@ -154,7 +161,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
         // more than kSideCap A entries use hash lookups, spread over the
         // cluster's CTAs.
         const bool side_path = dA <= kSideCap;
-        if (side_path && crank == 0) {
+        if (!a.half && side_path && crank == 0) {
             int32_t* side = reinterpret_cast<int32_t*>(it_base);
             for (int32_t j = tid; j < d3; j += THREADS) {
                 const uint32_t e = __ldg(a.Bout_ent + bo + j);
@@ -221,7 +228,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                             len = __ldg(a.Bout_ptr + g + 1) - o;
                         }
                         cap = w;
-                        if (!side_path && (i % CL) == crank) {
+                        if (!a.half && !side_path && (i % CL) == crank) {
                             const int32_t c = imin(w, bm_hash_get(a.hb, fu, g)) + imin(w, bm_hash_get(a.hb, g, fu));
                             if (c) atomicAdd(acc + x, c);
                         }
@@ -365,7 +372,18 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     if (valid && a.has_self) { sAu = __ldg(a.selfA + u); sBu = __ldg(a.selfB + fu); }
     int64_t* frow = a.full ? a.full + (size_t)r * ((size_t)n + 1) : nullptr;
     const int4* ov4 = reinterpret_cast<const int4*>(a.ov);
-    for (int32_t gi = glo + tid; gi < ghi; gi += THREADS) {
+    if (a.cols && valid) {
+        // one-sided mode: the requested columns, split over the cluster's CTAs
+        for (int32_t j = crank * THREADS + tid; j < a.ncols; j += CL * THREADS) {
+            const int32_t v = __ldg(a.cols + j);
+            int32_t sum = acc[v];
+            for (int q = 1; q < CL; q++) sum += *cluster.map_shared_rank(acc + v, (crank + q) % CL);
+            long long c = (long long)sum - ovu;
+            if (a.has_self) c += imin(sAu, __ldg(a.selfB + __ldg(a.pi + v))) - imin(sAu, sBu);
+            a.colout[(size_t)r * (size_t)a.ncols + j] = (int32_t)c;
+        }
+    }
+    for (int32_t gi = glo + tid; gi < ghi && !a.cols; gi += THREADS) {
         int4 s4 = reinterpret_cast<const int4*>(acc)[gi];
         for (int q = 1; q < CL; q++) {
             const int4 t4 = *reinterpret_cast<const int4*>(cluster.map_shared_rank(acc + 4 * gi, (crank + q) % CL));
@@ -508,6 +526,12 @@ bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_co
 
 bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
                             int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym) {
+    return bm_launch_rows_gen(ctx, d_rows, d_col_lo, nrows, d_full, d_res, d_tab, tab_ld, tab_sym, nullptr, 0, nullptr);
+}
+
+bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
+                             int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym,
+                             const int32_t* d_cols, int32_t ncols, int32_t* d_colout) {
     if (nrows <= 0) return BM_OK;
     bm_status st = bm_rows_smem_check(ctx);
     if (st != BM_OK) return st;
@@ -537,6 +561,10 @@ bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d
     args.tab = d_tab;
     args.tab_ld = tab_ld;
     args.tab_sym = tab_sym;
+    args.half = d_cols ? 1 : 0;
+    args.cols = d_cols;
+    args.ncols = ncols;
+    args.colout = d_colout;
     int cl = ctx->row_ctas;
     if (cl == 0) {
         // two CTAs fit per SM: the largest cluster size with nrows*cl <= 2*SMs
@@ -552,6 +580,7 @@ bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d
         ar.col_lo = d_col_lo ? d_col_lo + r0 : nullptr;
         ar.full = d_full ? d_full + (size_t)r0 * ((size_t)ctx->n + 1) : nullptr;
         ar.res = d_res ? d_res + r0 : nullptr;
+        ar.colout = d_colout ? d_colout + (size_t)r0 * (size_t)ncols : nullptr;
         st = (ctx->row_threads == 256) ? launch_rows_t<256>(ctx, ar, cl, smem) : launch_rows_t<512>(ctx, ar, cl, smem);
         if (st != BM_OK) return st;
     }

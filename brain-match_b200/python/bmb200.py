@@ -167,6 +167,9 @@ def cuda_lib() -> C.CDLL:
             "bm_get_row_tiling": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "bm_greedy_match_dev": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, C.c_int64, vp, vp, vp]),
             "bm_delta_table_dev": (C.c_int, [vp, vp, C.c_int64]),
+            "bm_lap_solve": (C.c_int, [vp, vp, C.c_int32, vp, C.POINTER(C.c_int64)]),
+            "bm_subset_assign": (C.c_int, [vp, vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+            "bm_search_hungarian": (C.c_int, [vp, C.c_int32, C.c_uint64, C.c_int32, C.c_double, C.POINTER(Progress)]),
             "bm_table_refresh_dev": (C.c_int, [vp, vp, C.c_int64, vp, C.c_int32]),
             "bm_table_topk": (C.c_int, [vp, vp, C.c_int64, C.c_int32, vp, vp, C.POINTER(C.c_int32)]),
             "bm_table_topk_dev": (C.c_int, [vp, vp, C.c_int64, C.c_int32, vp, vp, vp]),
@@ -603,6 +606,27 @@ class Engine:
         prog = prog or Progress()
         st = self.L.bm_search_table(self.h, d_tab, ld, k, max_accepts, max_rounds, time_budget, C.byref(prog))
         self._chk(st, "bm_search_table", ok=(BM_OK, BM_TIMEOUT))
+        return prog, st
+
+    def lap_solve(self, benefit):
+        a = np.ascontiguousarray(np.asarray(benefit, dtype=np.int32))
+        k = a.shape[0]
+        assign = np.zeros(k, np.int32)
+        tot = C.c_int64()
+        self._chk(self.L.bm_lap_solve(self.h, _ptr(a), k, _ptr(assign), C.byref(tot)), "bm_lap_solve")
+        return assign, tot.value
+
+    def subset_assign(self, subset):
+        s = _i32(subset)
+        d = C.c_int64()
+        ch = C.c_int32()
+        self._chk(self.L.bm_subset_assign(self.h, _ptr(s), s.shape[0], C.byref(d), C.byref(ch)), "bm_subset_assign")
+        return d.value, ch.value
+
+    def search_hungarian(self, k=1024, seed=1, iterations=10, time_budget=0.0, prog=None):
+        prog = prog or Progress()
+        st = self.L.bm_search_hungarian(self.h, k, seed, iterations, time_budget, C.byref(prog))
+        self._chk(st, "bm_search_hungarian", ok=(BM_OK, BM_TIMEOUT))
         return prog, st
 
     def greedy_match(self, A: Graph, B: Graph) -> np.ndarray:

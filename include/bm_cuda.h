@@ -333,6 +333,28 @@ bm_status bm_table_topk_dev(bm_ctx* ctx, const int32_t* d_table, int64_t ld, int
 bm_status bm_search_table(bm_ctx* ctx, int32_t* d_table, int64_t ld, int32_t k, int64_t max_accepts,
                           int32_t max_rounds, double time_budget_s, bm_progress* prog);
 
+/* ------------------------------------------- independent-subset assignment */
+
+/* Optimal linear assignment of a k x k integer benefit matrix (row-major,
+ * |benefit| <= 2^30, 1 <= k <= 4096): assign[i] = the column of row i in a
+ * permutation maximising the total, *total that total.  Replaces the
+ * reference's Hungarian method (src/independent-hungarian/hungarian.c:144-334)
+ * with the auction algorithm on the device; ties between optimal permutations
+ * may be broken differently. */
+bm_status bm_lap_solve(bm_ctx* ctx, const int32_t* benefit, int32_t k, int32_t* assign, int64_t* total);
+/* Re-assign the images of an A-independent subset (no A edge between two of
+ * its k <= 4096 members) by the best permutation of those images, as
+ * src/independent-hungarian/hungarianSubset.c:657-795 does with the one-sided
+ * gains of one_side_swap_delta (:414-459), self-loops included (the reference
+ * skips them and re-scores).  *delta >= 0 is the exact score change, *changed
+ * the number of members that moved. */
+bm_status bm_subset_assign(bm_ctx* ctx, const int32_t* subset, int32_t k, int64_t* delta, int32_t* changed);
+/* Repeat: draw a random A-independent subset of up to k members (Philox keyed
+ * by seed), re-assign it optimally; `iterations` times (< 0: until the
+ * budget).  Ends with a full re-score (BM_PARITY_FAIL on a mismatch). */
+bm_status bm_search_hungarian(bm_ctx* ctx, int32_t k, uint64_t seed, int32_t iterations, double time_budget_s,
+                              bm_progress* prog);
+
 /* ------------------------------------------------------- initial matching */
 
 /* Greedy-similarity initial matching on the device: the algorithm of
