@@ -100,7 +100,10 @@ extern "C" void bm_ctx_destroy(bm_ctx* ctx) {
     cudaFree(ctx->stage);
     cudaFree(ctx->flush_buf);
     cudaFree(ctx->tscr);
+    cudaFree(ctx->rwork); cudaFree(ctx->spart); cudaFree(ctx->scnt); cudaFree(ctx->rpart); cudaFree(ctx->slots);
     if (ctx->hstage) cudaFreeHost(ctx->hstage);
+    if (ctx->h_slots) cudaFreeHost(ctx->h_slots);
+    if (ctx->slots_ev) cudaEventDestroy(ctx->slots_ev);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -264,6 +267,7 @@ extern "C" bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* pi) {
     BM_TRY(bm_launch_relabel(ctx));
     int64_t s = 0;
     BM_TRY(bm_launch_score(ctx, &s));
+    BM_TRY(bm_rows_prepare(ctx));
     ctx->score = s;
     ctx->mapped = true;
     return BM_OK;
@@ -390,6 +394,19 @@ extern "C" bm_status bm_set_row_tiling(bm_ctx* ctx, int32_t ctas_per_row, int32_
         return bm_fail(ctx, BM_INVALID_ARG, "threads must be 256 or 512");
     if (ctas_per_row) ctx->row_ctas = ctas_per_row;
     if (threads) ctx->row_threads = threads;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_set_row_split(bm_ctx* ctx, int32_t slots) {
+    if (!ctx) return BM_INVALID_ARG;
+    if (slots < -1) return bm_fail(ctx, BM_INVALID_ARG, "slots must be -1 (off), 0 (automatic) or a slot count");
+    ctx->row_split = slots;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_get_row_split(bm_ctx* ctx, int32_t* slots) {
+    if (!ctx || !slots) return BM_INVALID_ARG;
+    *slots = ctx->row_split;
     return BM_OK;
 }
 

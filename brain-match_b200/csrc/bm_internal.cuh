@@ -91,6 +91,21 @@ struct bm_ctx {
     int64_t launches = 0;
     int32_t row_ctas = 0;           // CTAs per row (cluster size); 0 = auto
     int32_t row_threads = 512;
+    // split rows (bm_rows.cu): per-row work estimate, slot partial sums,
+    // self-resetting arrival counters and slice reductions
+    int32_t row_split = 0;          // 0 = automatic slots, -1 = off, k > 0 = k slots
+    int32_t* rwork = nullptr;
+    std::vector<int32_t> h_rwork;   // host copy (the split plan is made on the host)
+    int4* slots = nullptr;          // slot table of a split launch (device)
+    int4* h_slots = nullptr;        // its pinned host copy
+    cudaEvent_t slots_ev = nullptr; // recorded after each upload of h_slots
+    void* spart = nullptr;
+    unsigned* scnt = nullptr;
+    unsigned* rcnt = nullptr;       // inside the scnt allocation
+    void* rpart = nullptr;
+    int32_t split_n = 0;
+    int32_t split_slots_max = 0;
+    int split_active[2 * 9] = {};   // resident clusters per (threads, cluster size); 0 = not queried
     // host copy of A's adjacency (independence tests of batched swaps)
     std::vector<int32_t> hA_optr, hA_iptr;
     std::vector<uint32_t> hA_oent, hA_ient;
@@ -175,18 +190,25 @@ __device__ __forceinline__ int32_t imin(int32_t a, int32_t b) { return a < b ? a
 bm_status bm_launch_score(bm_ctx* ctx, int64_t* score_out);
 bm_status bm_launch_relabel(bm_ctx* ctx);
 bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_out);
+// Allocate the split-row buffers for the current n and refresh the per-row
+// work estimate (after the mapping is set); refresh alone after many swaps.
+bm_status bm_rows_prepare(bm_ctx* ctx);
+bm_status bm_rows_refresh_work(bm_ctx* ctx);
+// h_rows: a host copy of the rows, when the caller has one; it lets the
+// launch spread heavy rows over several clusters (split rows).
 bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
-                         int64_t* d_full, bm_row_result* d_res);
+                         int64_t* d_full, bm_row_result* d_res, const int32_t* h_rows = nullptr);
 // Same with a delta-table output: entry (u, v) of row u at d_tab[u * tab_ld + v]
 // as int32, and with tab_sym also (v, u).
 bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
-                            int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym);
+                            int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym,
+                            const int32_t* h_rows = nullptr);
 // One-sided mode: for each row u, G_u(pi v) - S(u) + self-loop term at the
 // columns v = d_cols[0..ncols), into d_colout[r * ncols + j] (int32): the gain
 // of u alone taking v's image with every other vertex fixed.
 bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
                              int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym,
-                             const int32_t* d_cols, int32_t ncols, int32_t* d_colout);
+                             const int32_t* d_cols, int32_t ncols, int32_t* d_colout, const int32_t* h_rows = nullptr);
 bm_status bm_launch_apply(bm_ctx* ctx, const int32_t* d_pairs, int32_t k);
 bm_status bm_rows_smem_check(bm_ctx* ctx);
 bm_status bm_launch_kset(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t nsets, long long* d_best,

@@ -25,13 +25,26 @@
 // Work per row is the number of 2-hop entries (about 10 per delta at the
 // full-scale workload) and every list is read as a coalesced stream.  Load
 // balance: first-hop items are cut into units of kSeg second-hop entries; the
-// units of a row are dealt round-robin to the CTAs of a thread-block cluster
-// (1..8 CTAs per row) and to their warps.  Each CTA scatters into its own
-// accumulator; after a cluster barrier each CTA sums one slice of v across the
-// cluster's accumulators through distributed shared memory and finalises it.
+// warps of all CTAs of a thread-block cluster (1..8 CTAs per row) take the
+// row's units one at a time from a counter in the cluster's first CTA.  Each
+// CTA scatters into its own accumulator; after a cluster barrier each CTA sums
+// one slice of v across the cluster's accumulators through distributed shared
+// memory and finalises it.
+//
+// Split rows.  A heavy row (a hub: up to 19 chunks of 1,024 first-hop items
+// and 7M 2-hop entries) is bound by its chunk count and its cluster's width.
+// When the caller holds the rows on the host, the launcher plans slots there
+// from a per-row work estimate kept beside the mapping: row r gets c_r
+// consecutive cluster slots, and slot j of c_r takes the first-hop items j,
+// j + c_r, j + 2 c_r, ...  Split rows meet in global memory: each slot
+// cluster writes its slice sums, the last slot to arrive (a self-resetting
+// counter) finalises the slice, and the last slice to arrive writes the row's
+// reduction.  Nothing waits on another cluster.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <climits>
+#include <vector>
 
 #include "bm_internal.cuh"
 
@@ -44,6 +57,16 @@ constexpr int kSeg = 512;         // second-hop entries per work unit
 constexpr int kMaxCluster = 8;
 constexpr int kSideCap = 4096;    // A entries of u whose corrections go through shared memory
 constexpr int kMaxUnits = 4096;   // units per chunk with a unit -> item table (else binary search)
+constexpr int kItemCost = 32;     // work estimate: entries charged per first-hop item
+
+struct Partial {
+    int32_t first_v;
+    int32_t best_v;
+    int32_t npos;
+    int32_t pad;
+    long long first_d;
+    long long best_d;
+};
 
 struct RowArgs {
     const int32_t* Aout_ptr;
@@ -76,15 +99,14 @@ struct RowArgs {
     const int32_t* cols;
     int32_t ncols;
     int32_t* colout;
-};
-
-struct Partial {
-    int32_t first_v;
-    int32_t best_v;
-    int32_t npos;
-    int32_t pad;
-    long long first_d;
-    long long best_d;
+    // split rows: slots[s] = {row, part, parts, 0} of cluster slot s (the
+    // parts of a row are consecutive slots); null = one slot per row
+    int32_t nslots;
+    const int4* slots;
+    int4* spart;        // [nslots][nvec / 4] slice sums of each slot cluster
+    unsigned* scnt;     // [nrows][kMaxCluster] slot arrivals per slice (self-resetting)
+    unsigned* rcnt;     // [nrows] slice arrivals per row (self-resetting)
+    Partial* rpart;     // [nrows][kMaxCluster] slice reductions
 };
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -92,13 +114,14 @@ __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~(siz
 __host__ __device__ inline int32_t nvec_of(int32_t n) { return (n + 1 + 3) & ~3; }
 
 __host__ __device__ inline size_t rows_smem_bytes(int32_t n) {
-    return align16(sizeof(int32_t) * (size_t)nvec_of(n))  // acc
+    return align16(sizeof(int32_t) * ((size_t)nvec_of(n) + 32))  // acc + one sink slot per lane
            + sizeof(void*) * kItemChunk                  // item base
            + sizeof(int32_t) * kItemChunk * 2            // len, cap
            + sizeof(int32_t) * (kItemChunk + 4)          // unit prefix
            + sizeof(int16_t) * kMaxUnits                 // unit -> item
-           + sizeof(int32_t) * 32                        // scan scratch + unit counter
-           + sizeof(Partial) * (kMaxCluster + 32);       // cluster partials + warp partials
+           + sizeof(int32_t) * 32                        // scan scratch + unit counters
+           + sizeof(Partial) * (kMaxCluster + 32)        // cluster partials + warp partials
+           + sizeof(int32_t) * 4;                        // split plan of this slot
 }
 
 __device__ __forceinline__ void better_first(int32_t& v, long long& d, int32_t v2, long long d2) {
@@ -109,6 +132,27 @@ __device__ __forceinline__ void better_best(int32_t& v, long long& d, int32_t v2
     if (d2 > d || (d2 == d && v2 < v)) { v = v2; d = d2; }
 }
 
+__device__ __forceinline__ Partial ld_partial(const Partial* p) {
+    const int4* q = reinterpret_cast<const int4*>(p);
+    const int4 x = __ldcg(q), y = __ldcg(q + 1);
+    Partial t;
+    t.first_v = x.x; t.best_v = x.y; t.npos = x.z; t.pad = x.w;
+    t.first_d = ((long long)(unsigned)y.y << 32) | (unsigned)y.x;
+    t.best_d = ((long long)(unsigned)y.w << 32) | (unsigned)y.z;
+    return t;
+}
+
+__device__ __forceinline__ bm_row_result row_result(int32_t u, const Partial& t) {
+    bm_row_result out;
+    out.row = u;
+    out.first_pos = (t.first_v == INT_MAX) ? 0 : t.first_v;
+    out.first_delta = (t.first_v == INT_MAX) ? 0 : t.first_d;
+    out.best = (t.best_v == INT_MAX) ? 0 : t.best_v;
+    out.best_delta = (t.best_v == INT_MAX) ? 0 : t.best_d;
+    out.npos = t.npos;
+    return out;
+}
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     constexpr int NW = THREADS / 32;
@@ -117,32 +161,47 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     cg::cluster_group cluster = cg::this_cluster();
     const int CL = (int)cluster.num_blocks();
     const int crank = (int)cluster.block_rank();
-    const int r = blockIdx.x / CL;
+    const int slot = blockIdx.x / CL;
     const int32_t n = a.n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     const int32_t nv = nvec_of(n);
     int32_t* acc = (int32_t*)smem;
-    unsigned char* p = smem + align16(sizeof(int32_t) * (size_t)nv);
+    unsigned char* p = smem + align16(sizeof(int32_t) * ((size_t)nv + 32));
     const uint32_t** it_base = (const uint32_t**)p;
     p += sizeof(void*) * kItemChunk;
     int32_t* it_len = (int32_t*)p;
     int32_t* it_cap = it_len + kItemChunk;
     int32_t* it_upre = it_cap + kItemChunk;
     int16_t* unit_item = reinterpret_cast<int16_t*>(it_upre + kItemChunk + 4);
-    int32_t* scan_tmp = reinterpret_cast<int32_t*>(unit_item + kMaxUnits);  // [0..15] warp offsets, [31] unit counter
-    int* unit_ctr = scan_tmp + 31;
+    int32_t* scan_tmp = reinterpret_cast<int32_t*>(unit_item + kMaxUnits);  // [0..15] warp offsets, [29..30] unit counters
     Partial* parts = (Partial*)(scan_tmp + 32);  // [kMaxCluster] cluster partials
     Partial* wparts = parts + kMaxCluster;       // [32] warp partials
+    int32_t* plan = reinterpret_cast<int32_t*>(wparts + 32);  // row, part, parts, last-arrival flag
 
-    const int32_t u = (r < a.nrows) ? __ldg(a.rows + r) : 0;
-    const bool valid = (u >= 1 && u <= n);
-
+    // plan[0..2]: row, part of the row, parts of the row.  Read back from
+    // shared memory where needed (short register live ranges).
+    if (tid == 0) {
+        if (a.slots) {
+            const int4 d = __ldg(a.slots + slot);
+            plan[0] = d.x; plan[1] = d.y; plan[2] = d.z;
+        } else {
+            plan[0] = slot; plan[1] = 0; plan[2] = 1;
+        }
+    }
+    auto P = [&](int k) -> int32_t { return *reinterpret_cast<volatile int32_t*>(plan + k); };
     {
         int4* acc4 = reinterpret_cast<int4*>(acc);
         for (int32_t i = tid; i < (nv >> 2); i += THREADS) acc4[i] = make_int4(0, 0, 0, 0);
     }
-    __syncthreads();
+    // Units are shared out across the whole cluster from counters in CTA 0's
+    // shared memory (one per chunk parity), so a CTA that shares its SM or
+    // also runs the corrections simply takes fewer units.
+    int* cctr = scan_tmp + 29;
+    if (crank == 0 && tid == 0) { cctr[0] = 0; cctr[1] = 0; }
+    cluster.sync();
+    const int32_t u = (P(0) < 0 || P(0) >= a.nrows) ? 0 : __ldg(a.rows + P(0));
+    const bool valid = (u >= 1 && u <= n);
 
     int32_t fu = 0;
     if (valid) {
@@ -161,7 +220,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
         // more than kSideCap A entries use hash lookups, spread over the
         // cluster's CTAs.
         const bool side_path = dA <= kSideCap;
-        if (!a.half && side_path && crank == 0) {
+        if (!a.half && side_path && crank == 0 && P(1) == 0) {
             int32_t* side = reinterpret_cast<int32_t*>(it_base);
             for (int32_t j = tid; j < d3; j += THREADS) {
                 const uint32_t e = __ldg(a.Bout_ent + bo + j);
@@ -201,15 +260,24 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             }
             __syncthreads();
         }
-        for (int32_t c0 = 0; c0 < F; c0 += kItemChunk) {
-            const int32_t cnt = min(kItemChunk, F - c0);
+        // a split row's slot j of c takes the first-hop items j, j + c, ...
+        // (j and c are read back from shared memory where they are used)
+        const int32_t Fs = (F - P(1) + P(2) - 1) / P(2);
+        for (int32_t c0 = 0; c0 < Fs; c0 += kItemChunk) {
+            const int32_t cnt = min(kItemChunk, Fs - c0);
+            const int ci = c0 / kItemChunk;
+            if (crank == 0 && tid == 0) cctr[(ci + 1) & 1] = 0;  // next chunk's counter (unused until the chunk barrier)
+            // 32-bit shared::cluster address of CTA 0's counter for this chunk
+            uint32_t gctr;
+            asm volatile("mapa.shared::cluster.u32 %0, %1, 0;"
+                         : "=r"(gctr) : "r"((uint32_t)__cvta_generic_to_shared(cctr + (ci & 1))));
             // ---- build this thread's IPT consecutive items (null padding
             // entries give empty items)
             int32_t tsum = 0;
 #pragma unroll
             for (int k = 0; k < IPT; k++) {
                 const int32_t li = tid * IPT + k;
-                const int32_t i = c0 + li;
+                const int32_t i = P(1) + P(2) * (c0 + li);
                 if (li >= cnt) break;
                 const uint32_t* base = a.Aout_ent;
                 int32_t len = 0, cap = 0;
@@ -274,7 +342,6 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                     if (lane >= o) wi += t;
                 }
                 if (lane < NW) scan_tmp[lane] = wi - wv;  // exclusive warp offsets
-                if (lane == 0) *unit_ctr = 0;
             }
             __syncthreads();
             {
@@ -293,6 +360,8 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             // binary search), when the chunk's units fit
             const int32_t U = it_upre[cnt];
             const bool table = U <= kMaxUnits;
+            // this slot's share of the chunk's units
+            const int32_t uhi = U;
             if (table) {
 #pragma unroll
                 for (int k = 0; k < IPT; k++) {
@@ -302,16 +371,16 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 }
                 __syncthreads();
             }
-            // ---- scatter: this CTA owns units crank, crank+CL, ...; its warps
-            // take them one at a time from a shared counter.  A unit is at most
+            // ---- scatter: warps of every CTA of the cluster take this slot's
+            // units one at a time from the cluster counter.  A unit is at most
             // kSeg entries of one list, read as 16-byte vectors (lists are
             // padded to multiples of 4 entries and start 16-byte aligned).  The
             // loop is software-pipelined: the next unit's loads are issued
             // before the current unit's shared-memory atomics.
             auto grab = [&]() -> int32_t {
                 int32_t k = 0;
-                if (lane == 0) k = atomicAdd(unit_ctr, 1);
-                return crank + CL * __shfl_sync(0xffffffffu, k, 0);
+                if (lane == 0) asm volatile("atom.shared::cluster.add.u32 %0, [%1], 1;" : "=r"(k) : "r"(gctr));
+                return __shfl_sync(0xffffffffu, k, 0);
             };
             auto load_unit = [&](int32_t unit, uint4 (&q)[kSeg / 128], int32_t& cap) {
                 int32_t it;
@@ -332,29 +401,32 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) {
                     const int qi = lane + 32 * t;
-                    q[t] = (qi < nq) ? __ldg(b4 + qi) : make_uint4(0u, 0u, 0u, 0u);
+                    // lanes past the unit's end add 0 to their own sink slot
+                    // past the accumulator (no branch around the atomics)
+                    const uint32_t sink = (uint32_t)(nv + lane);
+                    q[t] = (qi < nq) ? __ldg(b4 + qi) : make_uint4(sink, sink, sink, sink);
                 }
             };
             uint4 qa[kSeg / 128], qb[kSeg / 128];
             int32_t capa = 0, capb = 0;
             int32_t ua = grab();
-            if (ua < U) load_unit(ua, qa, capa);
-            while (ua < U) {
+            if (ua < uhi) load_unit(ua, qa, capa);
+            while (ua < uhi) {
                 const int32_t ub = grab();
-                if (ub < U) load_unit(ub, qb, capb);
+                if (ub < uhi) load_unit(ub, qb, capb);
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) {
                     const uint32_t e4[4] = {qa[t].x, qa[t].y, qa[t].z, qa[t].w};
 #pragma unroll
                     for (int c = 0; c < 4; c++)
-                        if (e4[c] != 0) atomicAdd(acc + bm_eid(e4[c]), imin(capa, bm_ew(e4[c])));
+                        atomicAdd(acc + bm_eid(e4[c]), imin(capa, bm_ew(e4[c])));
                 }
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) qa[t] = qb[t];
                 capa = capb;
                 ua = ub;
             }
-            __syncthreads();
+            if (c0 + kItemChunk < Fs) cluster.sync(); else __syncthreads();
         }
     }
     cluster.sync();
@@ -364,14 +436,40 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     const int32_t gslice = (groups + CL - 1) / CL;
     const int32_t glo = crank * gslice;
     const int32_t ghi = min(groups, glo + gslice);
+    const int r = P(0), sj = P(1), sc = P(2);
+    const bool idle = r < 0 || r >= a.nrows;
     const int32_t collo = (valid && a.col_lo) ? __ldg(a.col_lo + r) : 1;
     int32_t first_v = INT_MAX, best_v = INT_MAX, npos = 0;
     long long first_d = 0, best_d = LLONG_MIN;
     const long long ovu = valid ? (long long)__ldg(a.ov + u) : 0;
     int32_t sAu = 0, sBu = 0;
     if (valid && a.has_self) { sAu = __ldg(a.selfA + u); sBu = __ldg(a.selfB + fu); }
-    int64_t* frow = a.full ? a.full + (size_t)r * ((size_t)n + 1) : nullptr;
+    int64_t* frow = (a.full && !idle) ? a.full + (size_t)r * ((size_t)n + 1) : nullptr;
     const int4* ov4 = reinterpret_cast<const int4*>(a.ov);
+    auto cluster_sum = [&](int32_t gi) -> int4 {
+        int4 s4 = reinterpret_cast<const int4*>(acc)[gi];
+        for (int q = 1; q < CL; q++) {
+            const int4 t4 = *reinterpret_cast<const int4*>(cluster.map_shared_rank(acc + 4 * gi, (crank + q) % CL));
+            s4.x += t4.x; s4.y += t4.y; s4.z += t4.z; s4.w += t4.w;
+        }
+        return s4;
+    };
+    // split row: publish this slot's slice sums; the last slot to arrive for
+    // the slice finalises it from all the row's slot sums
+    bool fin = !idle;
+    if (sc > 1) {
+        int4* mine = a.spart + (size_t)slot * (size_t)groups;
+        for (int32_t gi = glo + tid; gi < ghi; gi += THREADS) mine[gi] = cluster_sum(gi);
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) {
+            const unsigned old = atomicInc(a.scnt + (size_t)r * kMaxCluster + crank, (unsigned)(sc - 1));
+            plan[3] = (old == (unsigned)(sc - 1)) ? 1 : 0;
+        }
+        __syncthreads();
+        fin = plan[3] != 0;
+        if (fin) __threadfence();
+    }
     if (a.cols && valid) {
         // one-sided mode: the requested columns, split over the cluster's CTAs
         for (int32_t j = crank * THREADS + tid; j < a.ncols; j += CL * THREADS) {
@@ -383,11 +481,17 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             a.colout[(size_t)r * (size_t)a.ncols + j] = (int32_t)c;
         }
     }
-    for (int32_t gi = glo + tid; gi < ghi && !a.cols; gi += THREADS) {
-        int4 s4 = reinterpret_cast<const int4*>(acc)[gi];
-        for (int q = 1; q < CL; q++) {
-            const int4 t4 = *reinterpret_cast<const int4*>(cluster.map_shared_rank(acc + 4 * gi, (crank + q) % CL));
-            s4.x += t4.x; s4.y += t4.y; s4.z += t4.z; s4.w += t4.w;
+    for (int32_t gi = glo + tid; fin && gi < ghi && !a.cols; gi += THREADS) {
+        int4 s4;
+        if (sc > 1) {
+            s4 = make_int4(0, 0, 0, 0);
+            const int4* base = a.spart + (size_t)(slot - sj) * (size_t)groups + gi;
+            for (int q = 0; q < sc; q++) {
+                const int4 t4 = __ldcg(base + (size_t)q * (size_t)groups);
+                s4.x += t4.x; s4.y += t4.y; s4.z += t4.z; s4.w += t4.w;
+            }
+        } else {
+            s4 = cluster_sum(gi);
         }
         const int4 o4 = __ldg(ov4 + gi);
         const int32_t sv[4] = {s4.x, s4.y, s4.z, s4.w};
@@ -418,7 +522,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             }
         }
     }
-    if (a.res) {
+    if (a.res && fin) {
         // warp, then block reduction
 #pragma unroll
         for (int o = 16; o; o >>= 1) {
@@ -439,26 +543,65 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 better_best(t.best_v, t.best_d, wparts[w].best_v, wparts[w].best_d);
                 t.npos += wparts[w].npos;
             }
-            *cluster.map_shared_rank(parts + crank, 0) = t;
+            if (sc > 1) {
+                // split row: the last slice to arrive combines the slices
+                Partial* rp = a.rpart + (size_t)r * kMaxCluster;
+                rp[crank] = t;
+                __threadfence();
+                const unsigned old = atomicInc(a.rcnt + r, (unsigned)(CL - 1));
+                if (old == (unsigned)(CL - 1)) {
+                    __threadfence();
+                    Partial c = ld_partial(rp);
+                    for (int q = 1; q < CL; q++) {
+                        const Partial pq = ld_partial(rp + q);
+                        better_first(c.first_v, c.first_d, pq.first_v, pq.first_d);
+                        better_best(c.best_v, c.best_d, pq.best_v, pq.best_d);
+                        c.npos += pq.npos;
+                    }
+                    a.res[r] = row_result(u, c);
+                }
+            } else {
+                *cluster.map_shared_rank(parts + crank, 0) = t;
+            }
         }
     }
     cluster.sync();
-    if (a.res && crank == 0 && tid == 0) {
+    if (a.res && !idle && sc == 1 && crank == 0 && tid == 0) {
         Partial t = parts[0];
         for (int q = 1; q < CL; q++) {
             better_first(t.first_v, t.first_d, parts[q].first_v, parts[q].first_d);
             better_best(t.best_v, t.best_d, parts[q].best_v, parts[q].best_d);
             t.npos += parts[q].npos;
         }
-        bm_row_result out;
-        out.row = u;
-        out.first_pos = (t.first_v == INT_MAX) ? 0 : t.first_v;
-        out.first_delta = (t.first_v == INT_MAX) ? 0 : t.first_d;
-        out.best = (t.best_v == INT_MAX) ? 0 : t.best_v;
-        out.best_delta = (t.best_v == INT_MAX) ? 0 : t.best_d;
-        out.npos = t.npos;
-        a.res[r] = out;
+        a.res[r] = row_result(u, t);
     }
+}
+
+// Work estimate of every row u (what the split plan weighs): the 2-hop
+// entries T1..T4 of u plus kItemCost per first-hop item.  One warp per row.
+constexpr int kWorkThreads = 256;
+__global__ void __launch_bounds__(kWorkThreads) row_work_kernel(RowArgs a, int32_t* __restrict__ work) {
+    const int32_t u = (int32_t)((blockIdx.x * (size_t)kWorkThreads + threadIdx.x) >> 5) + 1;
+    const int lane = threadIdx.x & 31;
+    if (u > a.n) return;
+    const int32_t fu = __ldg(a.pi + u);
+    long long s = 0;
+    auto walk = [&](const int32_t* ptr, const uint32_t* ent, int32_t i, bool map, const int32_t* ptr2) {
+        const int32_t o = __ldg(ptr + i), e = __ldg(ptr + i + 1);
+        for (int32_t j = o + lane; j < e; j += 32) {
+            const uint32_t x = __ldg(ent + j);
+            if (!x) continue;
+            const int32_t y = map ? __ldg(a.pi + bm_eid(x)) : bm_eid(x);
+            s += kItemCost + (__ldg(ptr2 + y + 1) - __ldg(ptr2 + y));
+        }
+    };
+    walk(a.Aout_ptr, a.Aout_ent, u, true, a.Bin_ptr);   // T1: B-in lists of pi x
+    walk(a.Ain_ptr, a.Ain_ent, u, true, a.Bout_ptr);    // T2: B-out lists of pi x
+    walk(a.Bout_ptr, a.Bout_ent, fu, false, a.Ain_ptr); // T3: A-in lists of y
+    walk(a.Bin_ptr, a.Bin_ent, fu, false, a.Aout_ptr);  // T4: A-out lists of y
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) work[u] = (int32_t)min(s, (long long)INT_MAX);
 }
 
 template <int THREADS>
@@ -470,7 +613,7 @@ bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem) {
         configured[ctx->device & 63] = true;
     }
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(args.nrows * cl), 1, 1);
+    cfg.gridDim = dim3((unsigned)(args.nslots * cl), 1, 1);
     cfg.blockDim = dim3(THREADS, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = ctx->stream;
@@ -507,6 +650,102 @@ bm_status max_clusters_t(bm_ctx* ctx, int cl, size_t smem, int* out) {
 
 }  // namespace
 
+bm_status bm_rows_prepare(bm_ctx* ctx) {
+    // split-row buffers, sized for n and at most split_slots_max slots
+    const int32_t smax = 2 * ctx->num_sms;
+    if (ctx->split_n != ctx->n || ctx->split_slots_max != smax) {
+        BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->rwork); cudaFree(ctx->spart); cudaFree(ctx->scnt); cudaFree(ctx->rpart); cudaFree(ctx->slots);
+        ctx->rwork = nullptr; ctx->spart = nullptr; ctx->scnt = nullptr; ctx->rpart = nullptr; ctx->rcnt = nullptr;
+        ctx->slots = nullptr;
+        ctx->split_n = 0;
+        BM_CUDA(ctx, cudaMalloc(&ctx->rwork, sizeof(int32_t) * (size_t)ctx->nvec));
+        BM_CUDA(ctx, cudaMalloc(&ctx->spart, sizeof(int32_t) * (size_t)ctx->nvec * (size_t)smax));
+        const size_t cnt_bytes = sizeof(unsigned) * (size_t)smax * (kMaxCluster + 1);
+        BM_CUDA(ctx, cudaMalloc(&ctx->scnt, cnt_bytes));
+        ctx->rcnt = ctx->scnt + (size_t)smax * kMaxCluster;
+        BM_CUDA(ctx, cudaMalloc(&ctx->rpart, sizeof(Partial) * (size_t)smax * kMaxCluster));
+        BM_CUDA(ctx, cudaMalloc(&ctx->slots, sizeof(int4) * (size_t)smax));
+        if (!ctx->h_slots) BM_CUDA(ctx, cudaHostAlloc((void**)&ctx->h_slots, sizeof(int4) * (size_t)2 * ctx->num_sms,
+                                                      cudaHostAllocDefault));
+        if (!ctx->slots_ev) BM_CUDA(ctx, cudaEventCreateWithFlags(&ctx->slots_ev, cudaEventDisableTiming));
+        BM_CUDA(ctx, cudaMemsetAsync(ctx->scnt, 0, cnt_bytes, ctx->stream));
+        ctx->split_n = ctx->n;
+        ctx->split_slots_max = smax;
+        for (int& c : ctx->split_active) c = 0;
+    }
+    return bm_rows_refresh_work(ctx);
+}
+
+bm_status bm_rows_refresh_work(bm_ctx* ctx) {
+    if (!ctx->rwork || !ctx->pi || ctx->n <= 0) return BM_OK;
+    const DevGraph& A = ctx->g[0];
+    const DevGraph& B = ctx->g[1];
+    RowArgs args = {};
+    args.Aout_ptr = A.out_ptr;
+    args.Ain_ptr = A.in_ptr;
+    args.Aout_ent = A.out_ent;
+    args.Ain_ent = A.in_ent;
+    args.Bout_ptr = B.out_ptr;
+    args.Bin_ptr = B.in_ptr;
+    args.Bout_ent = B.out_ent;
+    args.Bin_ent = B.in_ent;
+    args.pi = ctx->pi;
+    args.n = ctx->n;
+    const size_t threads = (size_t)ctx->n * 32;
+    const unsigned blocks = (unsigned)((threads + kWorkThreads - 1) / kWorkThreads);
+    row_work_kernel<<<blocks, kWorkThreads, 0, ctx->stream>>>(args, ctx->rwork);
+    BM_LAUNCH_CHECK(ctx, "row_work_kernel");
+    // the plan is made on the host, from rows the host holds
+    ctx->h_rwork.resize((size_t)ctx->n + 1);
+    BM_CUDA(ctx, cudaMemcpyAsync(ctx->h_rwork.data(), ctx->rwork, sizeof(int32_t) * ((size_t)ctx->n + 1),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BM_OK;
+}
+
+namespace {
+
+// Split plan for host-held rows: row i weighs w_i = max(1, rwork[rows[i]]);
+// with L the smallest integer (at least min_work) such that sum_i c_i <= S,
+// c_i = min(kMaxParts, ceil(w_i / L)), row i gets c_i consecutive slots
+// {i, j, c_i}.  Returns the slots used (sum_i c_i).  kMinSlotWork (the
+// automatic setting's min_work) keeps rows whose scatter would take less than
+// the global-memory merge unsplit.
+constexpr int kMaxParts = 16;
+constexpr int64_t kMinSlotWork = 300000;
+
+int32_t host_split_plan(const bm_ctx* ctx, const int32_t* h_rows, int32_t nrows, int32_t S, int64_t min_work,
+                        std::vector<int4>& out) {
+    std::vector<int64_t> w((size_t)nrows);
+    int64_t wmax = 1;
+    for (int32_t i = 0; i < nrows; i++) {
+        const int32_t u = h_rows[i];
+        w[(size_t)i] = (u >= 1 && u <= ctx->n) ? std::max<int64_t>(1, ctx->h_rwork[(size_t)u]) : 1;
+        wmax = std::max(wmax, w[(size_t)i]);
+    }
+    auto parts = [&](int64_t wi, int64_t L) { return (int32_t)std::min<int64_t>(kMaxParts, (wi + L - 1) / L); };
+    auto f = [&](int64_t L) {
+        int64_t s = 0;
+        for (int64_t wi : w) s += parts(wi, L);
+        return s;
+    };
+    int64_t lo = 1, hi = wmax;  // f(wmax) = nrows <= S
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        if (f(mid) <= S) hi = mid; else lo = mid + 1;
+    }
+    lo = std::max(lo, min_work);
+    out.clear();
+    for (int32_t i = 0; i < nrows; i++) {
+        const int32_t c = parts(w[(size_t)i], lo);
+        for (int32_t j = 0; j < c; j++) out.push_back(make_int4(i, j, c, 0));
+    }
+    return (int32_t)out.size();
+}
+
+}  // namespace
+
 bm_status bm_rows_smem_check(bm_ctx* ctx) {
     const size_t smem = rows_smem_bytes(ctx->n);
     if (smem > ctx->smem_optin)
@@ -520,18 +759,20 @@ bm_status bm_rows_smem_check(bm_ctx* ctx) {
 }
 
 bm_status bm_launch_rows(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows, int64_t* d_full,
-                         bm_row_result* d_res) {
-    return bm_launch_rows_ex(ctx, d_rows, d_col_lo, nrows, d_full, d_res, nullptr, 0, 0);
+                         bm_row_result* d_res, const int32_t* h_rows) {
+    return bm_launch_rows_ex(ctx, d_rows, d_col_lo, nrows, d_full, d_res, nullptr, 0, 0, h_rows);
 }
 
 bm_status bm_launch_rows_ex(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
-                            int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym) {
-    return bm_launch_rows_gen(ctx, d_rows, d_col_lo, nrows, d_full, d_res, d_tab, tab_ld, tab_sym, nullptr, 0, nullptr);
+                            int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym,
+                            const int32_t* h_rows) {
+    return bm_launch_rows_gen(ctx, d_rows, d_col_lo, nrows, d_full, d_res, d_tab, tab_ld, tab_sym, nullptr, 0, nullptr,
+                              h_rows);
 }
 
 bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo, int32_t nrows,
                              int64_t* d_full, bm_row_result* d_res, int32_t* d_tab, int64_t tab_ld, int32_t tab_sym,
-                             const int32_t* d_cols, int32_t ncols, int32_t* d_colout) {
+                             const int32_t* d_cols, int32_t ncols, int32_t* d_colout, const int32_t* h_rows) {
     if (nrows <= 0) return BM_OK;
     bm_status st = bm_rows_smem_check(ctx);
     if (st != BM_OK) return st;
@@ -571,11 +812,53 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
         cl = 1;
         while (cl < kMaxCluster && (int64_t)nrows * cl * 2 <= (int64_t)ctx->num_sms * 2) cl *= 2;
     }
+    args.nslots = nrows;
+    args.slots = nullptr;
+    args.spart = (int4*)ctx->spart;
+    args.scnt = ctx->scnt;
+    args.rcnt = ctx->rcnt;
+    args.rpart = (Partial*)ctx->rpart;
+    if (h_rows && ctx->row_split >= 0 && !d_cols && ctx->slots && nrows < ctx->split_slots_max &&
+        ctx->h_rwork.size() == (size_t)ctx->n + 1) {
+        // slots: the resident clusters of this shape when they are at least
+        // four times the rows (automatic: launches of a few rows, where most
+        // of the GPU would wait on the heaviest row), or the set count
+        int32_t S = ctx->row_split;
+        if (S == 0) {
+            int& cached = ctx->split_active[(ctx->row_threads == 256 ? 0 : 1) * (kMaxCluster + 1) + cl];
+            if (cached == 0) {
+                const size_t sm = rows_smem_bytes(ctx->n);
+                st = (ctx->row_threads == 256) ? max_clusters_t<256>(ctx, cl, sm, &cached)
+                                               : max_clusters_t<512>(ctx, cl, sm, &cached);
+                if (st != BM_OK) return st;
+                if (cached <= 0) cached = -1;
+            }
+            S = (cached >= 4 * nrows) ? cached : 0;
+        }
+        S = min(S, ctx->split_slots_max);
+        if (S > nrows) {
+            std::vector<int4> plan;
+            // a set slot count splits whatever it can (min_work 1); the
+            // automatic one only rows worth a global-memory merge
+            const int32_t used = host_split_plan(ctx, h_rows, nrows, S, ctx->row_split ? 1 : kMinSlotWork, plan);
+            if (used > nrows) {
+                // the pinned table is rewritten only after the previous upload ran
+                BM_CUDA(ctx, cudaEventSynchronize(ctx->slots_ev));
+                std::copy(plan.begin(), plan.end(), ctx->h_slots);
+                BM_CUDA(ctx, cudaMemcpyAsync(ctx->slots, ctx->h_slots, sizeof(int4) * (size_t)used,
+                                             cudaMemcpyHostToDevice, ctx->stream));
+                BM_CUDA(ctx, cudaEventRecord(ctx->slots_ev, ctx->stream));
+                args.slots = ctx->slots;
+                args.nslots = used;
+            }
+        }
+    }
     // grid.x is limited to 2^31-1; chunk very long row lists
     const int32_t max_rows_per_launch = 1 << 20;
     for (int32_t r0 = 0; r0 < nrows; r0 += max_rows_per_launch) {
         RowArgs ar = args;
         ar.nrows = min(max_rows_per_launch, nrows - r0);
+        if (!args.slots) ar.nslots = ar.nrows;  // one slot per row (a split launch is never chunked)
         ar.rows = d_rows + r0;
         ar.col_lo = d_col_lo ? d_col_lo + r0 : nullptr;
         ar.full = d_full ? d_full + (size_t)r0 * ((size_t)ctx->n + 1) : nullptr;
@@ -621,7 +904,7 @@ extern "C" bm_status bm_delta_rows(bm_ctx* ctx, const int32_t* rows, int32_t nro
     int32_t* d_rows = (int32_t*)ctx->stage;
     int64_t* d_out = (int64_t*)((char*)ctx->stage + in_al);
     BM_CUDA(ctx, cudaMemcpyAsync(d_rows, rows, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
-    if ((s = bm_launch_rows(ctx, d_rows, nullptr, nrows, d_out, nullptr)) != BM_OK) return s;
+    if ((s = bm_launch_rows(ctx, d_rows, nullptr, nrows, d_out, nullptr, rows)) != BM_OK) return s;
     BM_CUDA(ctx, cudaMemcpyAsync(deltas, d_out, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return BM_OK;
@@ -643,7 +926,7 @@ extern "C" bm_status bm_rows_best(bm_ctx* ctx, const int32_t* rows, const int32_
     BM_CUDA(ctx, cudaMemcpyAsync(d_rows, rows, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
     if (col_lo)
         BM_CUDA(ctx, cudaMemcpyAsync(d_col, col_lo, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
-    if ((s = bm_launch_rows(ctx, d_rows, col_lo ? d_col : nullptr, nrows, nullptr, d_out)) != BM_OK) return s;
+    if ((s = bm_launch_rows(ctx, d_rows, col_lo ? d_col : nullptr, nrows, nullptr, d_out, rows)) != BM_OK) return s;
     BM_CUDA(ctx, cudaMemcpyAsync(out, d_out, ob, cudaMemcpyDeviceToHost, ctx->stream));
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return BM_OK;

@@ -65,7 +65,7 @@ bm_status eval_rows(bm_ctx* ctx, SchedBufs& b, int32_t k, bool with_col) {
     BM_CUDA(ctx, cudaMemcpyAsync(b.d_rows, b.h_rows, sizeof(int32_t) * k, cudaMemcpyHostToDevice, ctx->stream));
     if (with_col)
         BM_CUDA(ctx, cudaMemcpyAsync(b.d_col, b.h_col, sizeof(int32_t) * k, cudaMemcpyHostToDevice, ctx->stream));
-    bm_status s = bm_launch_rows(ctx, b.d_rows, with_col ? b.d_col : nullptr, k, nullptr, b.d_res);
+    bm_status s = bm_launch_rows(ctx, b.d_rows, with_col ? b.d_col : nullptr, k, nullptr, b.d_res, b.h_rows);
     if (s != BM_OK) return s;
     BM_CUDA(ctx, cudaMemcpyAsync(b.h_res, b.d_res, sizeof(bm_row_result) * k, cudaMemcpyDeviceToHost, ctx->stream));
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -149,6 +149,7 @@ extern "C" bm_status bm_sweep_parity(bm_ctx* ctx, const int32_t* row_order, int3
     const int32_t kmax = std::max(1, std::min(nr, ctx->num_sms));
     SchedBufs b;
     if ((s = sched_bufs(ctx, kmax, &b)) != BM_OK) return s;
+    if ((s = bm_rows_refresh_work(ctx)) != BM_OK) return s;
 
     const auto t0 = clk::now();
     int32_t pos = prog->next_row_pos, col = prog->next_col;
@@ -227,6 +228,7 @@ extern "C" bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, in
     R = std::min(R, nr);
     SchedBufs b;
     if ((s = sched_bufs(ctx, R, &b)) != BM_OK) return s;
+    if ((s = bm_rows_refresh_work(ctx)) != BM_OK) return s;
     std::vector<int32_t> cand;
     BmMarks mk;
     const auto t0 = clk::now();

@@ -415,7 +415,8 @@ extern "C" bm_status bm_search_table(bm_ctx* ctx, int32_t* d_table, int64_t ld, 
         }
         BM_CUDA(ctx, cudaMemcpyAsync(d_rows, rows.data(), sizeof(int32_t) * rows.size(), cudaMemcpyHostToDevice,
                                      ctx->stream));
-        if ((s = bm_launch_rows_ex(ctx, d_rows, nullptr, (int32_t)rows.size(), nullptr, nullptr, d_table, ld, 1)) !=
+        if ((s = bm_launch_rows_ex(ctx, d_rows, nullptr, (int32_t)rows.size(), nullptr, nullptr, d_table, ld, 1,
+                                   rows.data())) !=
             BM_OK)
             return s;
         prog->rows_done += (int64_t)rows.size();

@@ -150,6 +150,8 @@ def cuda_lib() -> C.CDLL:
             "bm_device_pci_bus_id": (C.c_int, [vp, C.c_char_p, C.c_int32]),
             "bm_rows_max_active_clusters": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
             "bm_set_row_tiling": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "bm_set_row_split": (C.c_int, [vp, C.c_int32]),
+            "bm_get_row_split": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "bm_kset_eval": (C.c_int, [vp, C.c_int32, vp, C.c_int64, vp, vp, vp]),
             "bm_kset_eval_dev": (C.c_int, [vp, C.c_int32, vp, C.c_int64, vp, vp, vp]),
             "bm_apply_sets": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.c_int32]),
@@ -639,6 +641,15 @@ class Engine:
 
     def set_row_tiling(self, ctas_per_row: int = 0, threads: int = 0) -> None:
         self._chk(self.L.bm_set_row_tiling(self.h, ctas_per_row, threads), "bm_set_row_tiling")
+
+    def set_row_split(self, slots: int = 0) -> None:
+        """Cluster slots of a row launch: 0 automatic, -1 off, k > 0 k slots."""
+        self._chk(self.L.bm_set_row_split(self.h, slots), "bm_set_row_split")
+
+    def row_split(self) -> int:
+        v = C.c_int32()
+        self._chk(self.L.bm_get_row_split(self.h, C.byref(v)), "bm_get_row_split")
+        return v.value
 
     def launch_count(self) -> int:
         return int(self.L.bm_launch_count(self.h))

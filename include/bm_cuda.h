@@ -496,6 +496,19 @@ bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len);
  * (256 or 512).  0 keeps the current value. */
 bm_status bm_set_row_tiling(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads);
 bm_status bm_get_row_tiling(bm_ctx* ctx, int32_t* ctas_per_row, int32_t* threads);
+/* Split rows: in a row launch whose rows the caller passed from the host
+ * (bm_rows_best, bm_delta_rows and the search schedules; not the _dev entry
+ * points), heavy rows (by a per-row work estimate refreshed when the mapping
+ * is set and when a search starts) are spread over several thread-block
+ * clusters, each taking a strided share of the row's first-hop items, whose
+ * partial sums meet in global memory; results are identical either way.
+ * slots: 0 = automatic (default: split rows of at least ~300k 2-hop entries
+ * when the resident clusters of the launch's shape are at least 4x the rows),
+ * -1 = off (one cluster per row), k > 0 = up to k slots (capped at 2 x SMs),
+ * splitting every row it can.  No reference counterpart: the reference
+ * evaluates one pair per thread. */
+bm_status bm_set_row_split(bm_ctx* ctx, int32_t slots);
+bm_status bm_get_row_split(bm_ctx* ctx, int32_t* slots);
 /* How many row clusters of the given shape can be resident at once on the
  * device for the current n (cudaOccupancyMaxActiveClusters). */
 bm_status bm_rows_max_active_clusters(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads, int32_t* out);
