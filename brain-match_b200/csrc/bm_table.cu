@@ -16,8 +16,10 @@
 // Top-K: three radix passes (11, 11 and 10 bits of an order-preserving key)
 // build histograms of the upper triangle in shared memory, a one-block kernel
 // picks each digit, then one pass gathers every entry above the threshold and
-// a second gathers the first ties in (u, v) order (each block owns a
-// contiguous range of rows), and one block sorts the K entries by rank.
+// counts the ties per row, and a second gathers the first ties in (u, v)
+// order (each block owns a contiguous range of rows and starts at the row
+// prefix of the tie counts), and one block sorts the K entries by rank.  The
+// order-free passes give each block row pairs (u, n - u), equal in entries.
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -43,15 +45,88 @@ struct TopState {
 
 __device__ __forceinline__ uint32_t okey(int32_t d) { return (uint32_t)d ^ 0x80000000u; }
 
-__device__ __forceinline__ void block_rows(int32_t n, int32_t* lo, int32_t* hi) {
-    // rows 1..n-1 (row u holds the entries v > u), split into contiguous ranges
-    const int64_t rows = n > 1 ? n - 1 : 0;
-    const int64_t per = (rows + gridDim.x - 1) / gridDim.x;
-    const int64_t a = per * (int64_t)blockIdx.x, b = per * ((int64_t)blockIdx.x + 1);
-    *lo = 1 + (int32_t)(a < rows ? a : rows);
-    *hi = 1 + (int32_t)(b < rows ? b : rows);
+// Entries of the upper triangle in rows 1..u-1 (row i holds v = i+1..n).
+__device__ __forceinline__ int64_t tri_before(int64_t u, int64_t n) { return (u - 1) * n - (u - 1) * u / 2; }
+
+// First row u in [1, n] with tri_before(u) >= e.
+__device__ __forceinline__ int32_t tri_row(int64_t e, int32_t n) {
+    int32_t lo = 1, hi = n;
+    while (lo < hi) {
+        const int32_t mid = lo + ((hi - lo) >> 1);
+        if (tri_before(mid, n) >= e) hi = mid; else lo = mid + 1;
+    }
+    return lo;
 }
 
+__device__ __forceinline__ void block_rows(int32_t n, int32_t* lo, int32_t* hi) {
+    // rows 1..n-1 split into contiguous ranges of about equal entry counts
+    // (row u holds n - u entries), in block order
+    if (n < 2) { *lo = *hi = 1; return; }
+    const int64_t total = tri_before(n, n);
+    const int64_t b = blockIdx.x, g = gridDim.x;
+    *lo = tri_row(total * b / g, n);
+    *hi = b + 1 == g ? n : tri_row(total * (b + 1) / g, n);
+}
+
+// Rows of this block for the order-free scans: pairs (u, n - u), whose
+// lengths n - u and u add up to n, for u in an equal share of 1..(n-1)/2; the
+// middle row of an even n goes to the last block.  Returns the pair count;
+// row j of the block is pair_row(j).
+struct PairRows {
+    int32_t p0, np, n, mid;
+    __device__ __forceinline__ int32_t rows() const { return 2 * np + mid; }
+    __device__ __forceinline__ int32_t row(int32_t j) const {
+        if (j == 2 * np) return n / 2;  // the middle row
+        const int32_t u = p0 + (j >> 1);
+        return (j & 1) ? n - u : u;
+    }
+};
+
+__device__ __forceinline__ PairRows block_pairs(int32_t n) {
+    PairRows r;
+    r.n = n;
+    const int64_t P = n > 1 ? (n - 1) / 2 : 0;
+    const int64_t b = blockIdx.x, g = gridDim.x;
+    const int64_t a = P * b / g, e = P * (b + 1) / g;
+    r.p0 = 1 + (int32_t)a;
+    r.np = (int32_t)(e - a);
+    r.mid = (n > 1 && (n - 1) % 2 == 1 && b + 1 == g) ? 1 : 0;
+    return r;
+}
+
+// Visit the upper triangle of this block's rows with 16-byte streaming loads
+// (rows start 16-byte aligned: ld is a multiple of 4).  The group loop is
+// uniform over the block; f(u, v, d, ok) sees every lane, ok marks v in (u, n].
+// Any order: used by the passes that do not depend on it.
+template <class F>
+__device__ __forceinline__ void scan_upper(const int32_t* __restrict__ tab, int64_t ld, int32_t n, F&& f) {
+    const PairRows pr = block_pairs(n);
+    for (int32_t j = 0; j < pr.rows(); j++) {
+        const int32_t u = pr.row(j);
+        const int4* r4 = reinterpret_cast<const int4*>(tab + (size_t)u * (size_t)ld);
+        const int32_t g0 = (u + 1) >> 2, g1 = n >> 2;
+        for (int32_t gb = g0; gb <= g1; gb += 2 * kTabThreads) {
+            const int32_t ga = gb + (int32_t)threadIdx.x, gc = ga + kTabThreads;
+            const int4 qa = ga <= g1 ? __ldcs(r4 + ga) : make_int4(0, 0, 0, 0);
+            const int4 qc = gc <= g1 ? __ldcs(r4 + gc) : make_int4(0, 0, 0, 0);
+            const int32_t da[4] = {qa.x, qa.y, qa.z, qa.w}, dc[4] = {qc.x, qc.y, qc.z, qc.w};
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int32_t v = 4 * ga + c;
+                f(u, v, da[c], ga <= g1 && v > u && v <= n);
+            }
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int32_t v = 4 * gc + c;
+                f(u, v, dc[c], gc <= g1 && v > u && v <= n);
+            }
+        }
+    }
+}
+
+// Histogram of one digit over the entries whose fixed digits match.  Deltas
+// crowd into a few bins, so each thread merges runs of equal bins in a
+// register and adds a run with one shared-memory atomic.
 __global__ void __launch_bounds__(kTabThreads) hist_kernel(const int32_t* __restrict__ tab, int64_t ld, int32_t n,
                                                            const TopState* st, int shift, int bits,
                                                            uint32_t* __restrict__ ghist) {
@@ -59,35 +134,68 @@ __global__ void __launch_bounds__(kTabThreads) hist_kernel(const int32_t* __rest
     for (int i = threadIdx.x; i < kBins; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const uint32_t prefix = st->prefix, mask = st->mask, dm = (1u << bits) - 1u;
-    int32_t lo, hi;
-    block_rows(n, &lo, &hi);
-    for (int32_t u = lo; u < hi; u++) {
-        const int32_t* row = tab + (size_t)u * (size_t)ld;
-        for (int32_t v = u + 1 + threadIdx.x; v <= n; v += blockDim.x) {
-            const uint32_t key = okey(row[v]);
-            if ((key & mask) == prefix) atomicAdd(&h[(key >> shift) & dm], 1u);
+    uint32_t run_bin = 0, run_cnt = 0;
+    scan_upper(tab, ld, n, [&](int32_t, int32_t, int32_t d, bool ok) {
+        const uint32_t key = okey(d);
+        if (ok && (key & mask) == prefix) {
+            const uint32_t b = (key >> shift) & dm;
+            if (b != run_bin) {
+                if (run_cnt) atomicAdd(&h[run_bin], run_cnt);
+                run_bin = b;
+                run_cnt = 0;
+            }
+            run_cnt++;
         }
-    }
+    });
+    if (run_cnt) atomicAdd(&h[run_bin], run_cnt);
     __syncthreads();
     for (int i = threadIdx.x; i < kBins; i += blockDim.x)
         if (h[i]) atomicAdd(&ghist[i], h[i]);
 }
 
-// Fix the next digit: the largest d with (entries above d) < need <= (entries at or above d).
-__global__ void select_digit_kernel(uint32_t* ghist, TopState* st, int shift, int bits) {
-    if (threadIdx.x == 0 && st->need > 0) {
-        int32_t need = st->need;
-        int d = (1 << bits) - 1;
-        while (d > 0 && (int32_t)ghist[d] < need) {
-            need -= (int32_t)ghist[d];
+// Fix the next digit: the largest d with (entries above d) < need <= (entries
+// at or above d).  One block of kSelThreads: per-thread sums of kBins /
+// kSelThreads bins, a suffix scan, then the owning thread walks its bins.
+constexpr int kSelThreads = 256;
+__global__ void __launch_bounds__(kSelThreads) select_digit_kernel(uint32_t* ghist, TopState* st, int shift, int bits) {
+    __shared__ uint32_t suf[kSelThreads + 1];
+    constexpr int per = kBins / kSelThreads;
+    const int nb = 1 << bits;
+    const int t = threadIdx.x;
+    const int32_t need = st->need;  // read before the owner thread rewrites it
+    uint32_t mine = 0;
+    for (int j = 0; j < per; j++) {
+        const int b = t * per + j;
+        if (b < nb) mine += ghist[b];
+    }
+    suf[t] = mine;
+    if (t == 0) suf[kSelThreads] = 0;
+    __syncthreads();
+    // inclusive suffix sums: suf[t] = entries in the bins of threads t..end
+    for (int o = 1; o < kSelThreads; o <<= 1) {
+        const uint32_t x = (t + o < kSelThreads) ? suf[t + o] : 0;
+        __syncthreads();
+        suf[t] += x;
+        __syncthreads();
+    }
+    const uint32_t above = suf[t + 1];  // entries in the bins of higher threads
+    if (need > 0 && (int64_t)above < need && (int64_t)suf[t] >= need) {
+        int32_t left = need - (int32_t)above;
+        int d = min(nb, (t + 1) * per) - 1;
+        while (d > t * per && (int32_t)ghist[d] < left) {
+            left -= (int32_t)ghist[d];
             d--;
         }
-        st->need = need;
+        st->need = left;
         st->prefix |= (uint32_t)d << shift;
+        st->mask |= ((1u << bits) - 1u) << shift;
+    } else if (need > 0 && t == 0 && (int64_t)suf[0] < need) {
+        // fewer entries than needed (cannot happen for k <= entries): take digit 0
+        st->need = need - (int32_t)(suf[0] - ghist[0]);
         st->mask |= ((1u << bits) - 1u) << shift;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kBins; i += blockDim.x) ghist[i] = 0;
+    for (int i = t; i < kBins; i += kSelThreads) ghist[i] = 0;
 }
 
 struct Sel {
@@ -98,61 +206,87 @@ struct Sel {
 
 // Entries above the threshold (any order, atomic slots) and the count of
 // ties per block.
+// Entries above the threshold (any order, atomic slots), and the ties per
+// row (each thread adds its count for a row when it moves to another row).
 __global__ void __launch_bounds__(kTabThreads) gather_gt_kernel(const int32_t* __restrict__ tab, int64_t ld, int32_t n,
-                                                                TopState* st, Sel sel, int32_t* __restrict__ blk_eq) {
-    __shared__ int32_t s_eq;
-    if (threadIdx.x == 0) s_eq = 0;
-    __syncthreads();
+                                                                TopState* st, Sel sel, int32_t* __restrict__ rowtie) {
     const uint32_t T = st->prefix;
     const int32_t n_gt = st->k - st->need;
-    int32_t lo, hi, eq = 0;
-    block_rows(n, &lo, &hi);
-    for (int32_t u = lo; u < hi; u++) {
-        const int32_t* row = tab + (size_t)u * (size_t)ld;
-        for (int32_t v = u + 1 + threadIdx.x; v <= n; v += blockDim.x) {
-            const int32_t d = row[v];
-            const uint32_t key = okey(d);
-            if (key > T) {
-                const int32_t slot = atomicAdd(&st->gt_slot, 1);
-                if (slot < n_gt) { sel.u[slot] = u; sel.v[slot] = v; sel.d[slot] = d; }
-            } else if (key == T) {
-                eq++;
+    int32_t cur = 0, eq = 0;
+    scan_upper(tab, ld, n, [&](int32_t u, int32_t v, int32_t d, bool ok) {
+        const uint32_t key = okey(d);
+        if (ok && key > T) {
+            const int32_t slot = atomicAdd(&st->gt_slot, 1);
+            if (slot < n_gt) { sel.u[slot] = u; sel.v[slot] = v; sel.d[slot] = d; }
+        } else if (ok && key == T) {
+            if (u != cur) {
+                if (eq) atomicAdd(&rowtie[cur], eq);
+                cur = u;
+                eq = 0;
             }
+            eq++;
         }
-    }
-    for (int o = 16; o; o >>= 1) eq += __shfl_xor_sync(0xffffffffu, eq, o);
-    if ((threadIdx.x & 31) == 0 && eq) atomicAdd(&s_eq, eq);
-    __syncthreads();
-    if (threadIdx.x == 0) blk_eq[blockIdx.x] = s_eq;
+    });
+    if (eq) atomicAdd(&rowtie[cur], eq);
 }
 
-__global__ void scan_blocks_kernel(int32_t* blk, int32_t nb) {
-    if (threadIdx.x == 0) {
-        int32_t run = 0;
-        for (int32_t b = 0; b < nb; b++) {
-            const int32_t c = blk[b];
-            blk[b] = run;
-            run += c;
+// In place exclusive scan of the per-row tie counts (m entries, one block of
+// kScanThreads): rowtie[u] becomes the ties in rows before u.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) scan_rows_kernel(int32_t* rowtie, int32_t m) {
+    __shared__ int32_t w[kScanThreads / 32];
+    __shared__ int32_t carry;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    if (t == 0) carry = 0;
+    __syncthreads();
+    for (int32_t base = 0; base < m; base += kScanThreads) {
+        const int32_t i = base + t;
+        const int32_t x = i < m ? rowtie[i] : 0;
+        int32_t incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
+        if (lane == 31) w[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            const int32_t wv = w[lane];
+            int32_t wi = wv;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += y;
+            }
+            w[lane] = wi - wv;
+        }
+        __syncthreads();
+        const int32_t c = carry;
+        if (i < m) rowtie[i] = c + w[wid] + incl - x;
+        __syncthreads();
+        if (t == kScanThreads - 1) carry = c + w[wid] + incl;
+        __syncthreads();
     }
 }
 
 // The first `need` ties in (u, v) order after the entries above the threshold.
 __global__ void __launch_bounds__(kTabThreads) gather_eq_kernel(const int32_t* __restrict__ tab, int64_t ld, int32_t n,
                                                                 const TopState* st, Sel sel,
-                                                                const int32_t* __restrict__ blk_off) {
+                                                                const int32_t* __restrict__ rowoff) {
     __shared__ int32_t wcnt[kTabThreads / 32];
     __shared__ int32_t s_base;
     const int32_t take = st->need;
     const int32_t n_gt = st->k - take;
     const uint32_t T = st->prefix;
-    if (threadIdx.x == 0) s_base = blk_off[blockIdx.x];
-    __syncthreads();
-    if (s_base >= take) return;  // uniform over the block
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int32_t lo, hi;
     block_rows(n, &lo, &hi);
+    if (threadIdx.x == 0) s_base = rowoff[lo];
+    __syncthreads();
+    // uniform over the block: enough ties before it, or none in its rows
+    if (s_base >= take || rowoff[hi] == s_base) return;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int32_t u = lo; u < hi; u++) {
+        if (rowoff[u + 1] == rowoff[u]) continue;  // no ties in this row (uniform)
         const int32_t* row = tab + (size_t)u * (size_t)ld;
         for (int32_t v0 = u + 1; v0 <= n; v0 += blockDim.x) {
             const int32_t v = v0 + threadIdx.x;
@@ -179,15 +313,19 @@ __global__ void __launch_bounds__(kTabThreads) gather_eq_kernel(const int32_t* _
     }
 }
 
-// Rank sort of the k selected entries: larger delta first, then smaller u, v.
-__global__ void rank_sort_kernel(Sel sel, const TopState* st, int32_t* __restrict__ out_pairs,
-                                 long long* __restrict__ out_d) {
+// Rank sort of the k selected entries: larger delta first, then smaller u, v
+// (entries staged in shared memory).
+__global__ void __launch_bounds__(1024) rank_sort_kernel(Sel sel, const TopState* st, int32_t* __restrict__ out_pairs,
+                                                         long long* __restrict__ out_d) {
+    __shared__ int32_t su[kTopMax], sv[kTopMax], sd[kTopMax];
     const int32_t k = st->k;
+    for (int32_t i = threadIdx.x; i < k; i += blockDim.x) { su[i] = sel.u[i]; sv[i] = sel.v[i]; sd[i] = sel.d[i]; }
+    __syncthreads();
     for (int32_t i = threadIdx.x; i < k; i += blockDim.x) {
-        const int32_t d = sel.d[i], u = sel.u[i], v = sel.v[i];
+        const int32_t d = sd[i], u = su[i], v = sv[i];
         int32_t rank = 0;
         for (int32_t j = 0; j < k; j++) {
-            const int32_t d2 = sel.d[j], u2 = sel.u[j], v2 = sel.v[j];
+            const int32_t d2 = sd[j], u2 = su[j], v2 = sv[j];
             rank += (d2 > d) || (d2 == d && (u2 < u || (u2 == u && v2 < v)));
         }
         out_pairs[2 * rank] = u;
@@ -204,7 +342,7 @@ __global__ void iota_kernel(int32_t* rows, int32_t n) {
 struct TopScratch {
     TopState* st;
     uint32_t* hist;
-    int32_t* blk;
+    int32_t* rowtie;  // n + 2 entries: ties per row, then their exclusive prefix
     Sel sel;
 };
 
@@ -212,7 +350,7 @@ size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 bm_status top_scratch(bm_ctx* ctx, TopScratch* s, void** base_out) {
     const size_t b_st = al256(sizeof(TopState)), b_h = al256(sizeof(uint32_t) * kBins),
-                 b_blk = al256(sizeof(int32_t) * kTabBlocks), b_sel = al256(sizeof(int32_t) * kTopMax);
+                 b_blk = al256(sizeof(int32_t) * ((size_t)ctx->n + 2)), b_sel = al256(sizeof(int32_t) * kTopMax);
     const size_t total = b_st + b_h + b_blk + 3 * b_sel;
     if (ctx->tscr_bytes < total) {
         cudaFree(ctx->tscr);
@@ -227,7 +365,7 @@ bm_status top_scratch(bm_ctx* ctx, TopScratch* s, void** base_out) {
     char* p = (char*)ctx->tscr;
     s->st = (TopState*)p;
     s->hist = (uint32_t*)(p + b_st);
-    s->blk = (int32_t*)(p + b_st + b_h);
+    s->rowtie = (int32_t*)(p + b_st + b_h);
     s->sel.u = (int32_t*)(p + b_st + b_h + b_blk);
     s->sel.v = (int32_t*)(p + b_st + b_h + b_blk + b_sel);
     s->sel.d = (int32_t*)(p + b_st + b_h + b_blk + 2 * b_sel);
@@ -264,14 +402,15 @@ static bm_status bm_table_topk_launch(bm_ctx* ctx, const int32_t* d_tab, int64_t
         for (int p = 0; p < 3; p++) {
             hist_kernel<<<kTabBlocks, kTabThreads, 0, ctx->stream>>>(d_tab, ld, n, S.st, shifts[p], widths[p], S.hist);
             BM_LAUNCH_CHECK(ctx, "hist_kernel");
-            select_digit_kernel<<<1, 256, 0, ctx->stream>>>(S.hist, S.st, shifts[p], widths[p]);
+            select_digit_kernel<<<1, kSelThreads, 0, ctx->stream>>>(S.hist, S.st, shifts[p], widths[p]);
             BM_LAUNCH_CHECK(ctx, "select_digit_kernel");
         }
-        gather_gt_kernel<<<kTabBlocks, kTabThreads, 0, ctx->stream>>>(d_tab, ld, n, S.st, S.sel, S.blk);
+        BM_CUDA(ctx, cudaMemsetAsync(S.rowtie, 0, sizeof(int32_t) * ((size_t)n + 2), ctx->stream));
+        gather_gt_kernel<<<kTabBlocks, kTabThreads, 0, ctx->stream>>>(d_tab, ld, n, S.st, S.sel, S.rowtie);
         BM_LAUNCH_CHECK(ctx, "gather_gt_kernel");
-        scan_blocks_kernel<<<1, 32, 0, ctx->stream>>>(S.blk, kTabBlocks);
-        BM_LAUNCH_CHECK(ctx, "scan_blocks_kernel");
-        gather_eq_kernel<<<kTabBlocks, kTabThreads, 0, ctx->stream>>>(d_tab, ld, n, S.st, S.sel, S.blk);
+        scan_rows_kernel<<<1, kScanThreads, 0, ctx->stream>>>(S.rowtie, n + 2);
+        BM_LAUNCH_CHECK(ctx, "scan_rows_kernel");
+        gather_eq_kernel<<<kTabBlocks, kTabThreads, 0, ctx->stream>>>(d_tab, ld, n, S.st, S.sel, S.rowtie);
         BM_LAUNCH_CHECK(ctx, "gather_eq_kernel");
         rank_sort_kernel<<<1, 1024, 0, ctx->stream>>>(S.sel, S.st, d_pairs, d_deltas);
         BM_LAUNCH_CHECK(ctx, "rank_sort_kernel");
