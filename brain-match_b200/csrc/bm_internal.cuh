@@ -159,12 +159,49 @@ inline HashView hview(const DevGraph& g) { return HashView{g.hash, g.hash_log2, 
 
 // ------------------------------------------------------------------ device
 
-// Weight of B edge g->h (B ids), 0 if absent.  Linear probing read two slots
-// (16 bytes) at a time from the even slot at or below the home slot; in the
-// first pair a slot before the home slot is not part of the probe sequence.
-// The table is at most half full, so an empty slot ends every sequence; the
-// loop is also bounded by the table size.
+// B's edge weights live in an open-addressing table at most half full, so an
+// empty slot ends every linear probe sequence; lookups are also bounded by
+// the table size.  Most lookups are for absent edges, whose sequences have a
+// long tail, so a probe step reads a whole 32-byte sector.
+// One step of the linear probe sequence: the aligned group of four slots (one
+// 32-byte sector) at slot index `grp` (a multiple of 4), from slot `from`
+// of the group on.  Returns true when the lookup is settled (key found, *w
+// its weight, or an empty slot met, *w = 0).
+__device__ __forceinline__ bool bm_hash_group(const HashView& hv, unsigned long long key, unsigned long long grp,
+                                              int from, int32_t* w) {
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(hv.tab + grp);
+    const ulonglong2 a = __ldg(p), b = __ldg(p + 1);
+    const unsigned long long v[4] = {a.x, a.y, b.x, b.y};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (i < from) continue;
+        if (v[i] == BM_HASH_EMPTY) { *w = 0; return true; }
+        if ((v[i] >> 16) == key) { *w = (int32_t)(v[i] & 0xFFFFull); return true; }
+    }
+    return false;
+}
+
+// Weight of B edge g->h (B ids), 0 if absent: linear probing from the home
+// slot, read a 32-byte group of four slots per step (tables hold at least
+// 1,024 slots and start 256-byte aligned).
 __device__ __forceinline__ int32_t bm_hash_get(const HashView& hv, int32_t g, int32_t h) {
+    const unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;
+    const unsigned long long mask = (1ull << hv.log2) - 1ull;
+    const unsigned long long s0 = bm_hash_slot0(key, hv.log2);
+    unsigned long long grp = s0 & ~3ull;
+    int from = (int)(s0 & 3ull);
+    int32_t w = 0;
+    for (unsigned long long it = 0; it <= mask; it += 4) {
+        if (bm_hash_group(hv, key, grp, from, &w)) return w;
+        from = 0;
+        grp = (grp + 4) & mask;
+    }
+    return 0;
+}
+
+// The same lookup reading one 16-byte slot pair per step: fewer registers,
+// for kernels at their register limit that look up rarely.
+__device__ __forceinline__ int32_t bm_hash_get_small(const HashView& hv, int32_t g, int32_t h) {
     const unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;
     const unsigned long long mask = (1ull << hv.log2) - 1ull;
     const unsigned long long s0 = bm_hash_slot0(key, hv.log2);

@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                         }
                         cap = w;
                         if (!a.half && !side_path && (i % CL) == crank) {
-                            const int32_t c = imin(w, bm_hash_get(a.hb, fu, g)) + imin(w, bm_hash_get(a.hb, g, fu));
+                            const int32_t c = imin(w, bm_hash_get_small(a.hb, fu, g)) + imin(w, bm_hash_get_small(a.hb, g, fu));
                             if (c) atomicAdd(acc + x, c);
                         }
                     }

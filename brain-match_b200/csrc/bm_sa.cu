@@ -16,8 +16,9 @@
 // others); the first accepted one in step order is applied and the rest are
 // discarded, so the chain is exactly the one-at-a-time chain for every K (the
 // step counter moves past the accepted proposal, or by K when none is
-// accepted).  K is the tuning knob; the chain's mapping lives in shared memory
-// when it fits.  A launch advances every chain by at most `chunk` proposals;
+// accepted).  K starts at the tuned value and then follows the chain's
+// acceptances (up to 64), so long runs of rejections are evaluated 64 at a
+// time; the chain's mapping lives in shared memory when it fits.  A launch advances every chain by at most `chunk` proposals;
 // the launch is captured once in a CUDA graph and replayed until all chains
 // finish.
 #include <algorithm>
@@ -45,6 +46,12 @@ struct PairDev {
     const int32_t* selfA;
     const int32_t* selfB;
     HashView hb;
+    // B's rows (sorted by neighbour id, zero padding at the end), searched
+    // for the edges of a whole A list at once
+    const int32_t* Bout_ptr;
+    const int32_t* Bin_ptr;
+    const uint32_t* Bout_ent;
+    const uint32_t* Bin_ent;
 };
 
 struct ChainDev {
@@ -62,7 +69,7 @@ struct SaArgs {
     const PairDev* pairs;
     ChainDev* chains;
     int32_t nchains;
-    int32_t K;        // proposals evaluated per iteration (1..16)
+    int32_t K;        // proposals per iteration at the start (1..kSaMaxInitialK); adapts up to kSaMaxK
     int32_t pi_smem;  // 1: the chain's mapping is kept in shared memory
     uint64_t steps;
     uint64_t chunk;
@@ -70,27 +77,16 @@ struct SaArgs {
     double log_ratio;
 };
 
-constexpr int kSaThreads = 256;
-constexpr int kSaMaxK = 16;
-constexpr int kSaUnit = 32;    // list entries per work unit (one per lane)
-constexpr int kSaBatch = 4;    // units a warp takes at once
+constexpr int kSaThreads = 512;
+constexpr int kSaMaxK = 64;         // proposals per iteration, adaptive up to this
+constexpr int kSaMaxInitialK = 16;  // largest settable starting K
+constexpr int kSaItem = 128;        // list entries per work item (four per lane)
+constexpr int kSaRowCap = 512;      // B row entries a warp stages in shared memory (longer rows: hash)
+constexpr int kSaUnitTable = 4096;  // items per iteration with an item -> list table (else binary search)
 
-// First probe of the B hash for (g, h): the two 8-byte slots at or below the
-// home slot, as bm_hash_get reads them first.  Returns true when that settles
-// the lookup (key found or an empty slot met) and sets *w; false means the
-// probe sequence continues and the caller falls back to bm_hash_get.
-__device__ __forceinline__ bool hash_probe_first(const HashView& hv, int32_t g, int32_t h, int32_t* w) {
-    const unsigned long long key = (unsigned long long)g * (unsigned long long)hv.np1 + (unsigned long long)h;
-    const unsigned long long s0 = bm_hash_slot0(key, hv.log2);
-    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(hv.tab + (s0 & ~1ull)));
-    if (!(s0 & 1ull)) {
-        if (v.x == BM_HASH_EMPTY) { *w = 0; return true; }
-        if ((v.x >> 16) == key) { *w = (int32_t)(v.x & 0xFFFFull); return true; }
-    }
-    if (v.y == BM_HASH_EMPTY) { *w = 0; return true; }
-    if ((v.y >> 16) == key) { *w = (int32_t)(v.y & 0xFFFFull); return true; }
-    return false;
-}
+// Dynamic shared memory of the chain kernel: the warps' B-row buffers, then
+// the chain's mapping when it fits.
+constexpr size_t kSaRowBytes = sizeof(uint32_t) * kSaRowCap * (kSaThreads / 32);
 
 // Apply the swap pi(a) <-> pi(b) of one chain with the whole CTA: S updates of
 // every A entry incident to a or b (as apply_kernel in bm_apply.cu), then pi.
@@ -143,199 +139,197 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
 }
 
 // One CTA runs one chain.  Each iteration draws the proposals of steps
-// s..s+K-1 and evaluates all of them at once under the current mapping: the
-// four A lists of each proposal (out(u), in(u), out(v), in(v)) are cut into
-// units of 32 entries that the warps take, four at a time, from a shared
-// counter, so a proposal touching a hub is spread over the whole CTA instead
-// of one warp.  Each entry contributes (the per-pair identity of bm_pairs.cu)
+// s..s+K-1 and evaluates all of them at once under the current mapping.
+// Each entry of the four A lists of a proposal (out(u), in(u), out(v),
+// in(v)) contributes (the per-pair identity of bm_pairs.cu)
 //   out(u): min(w, B(pi v, pi x))   in(u): min(w, B(pi x, pi v))
 //   out(v): min(w, B(pi u, pi x))   in(v): min(w, B(pi x, pi u))
-// plus, for an entry of u whose other end is v, the direct-edge repair
-// min(w, B(pi u, pi v)) + min(w, B(pi v, pi u)); the unit sums meet in a
-// per-proposal shared counter, then
+// so every entry of one list looks up the same B row (B-out or B-in of pi v
+// or pi u).  The lists are cut into items of kSaItem entries; warp w takes
+// items w, w + 16, ..., stages the item's B row in its shared buffer with
+// coalesced loads, and each lane binary-searches pi x in it (rows longer
+// than the buffer use the hash).  For an entry of u whose other end is v,
+// the direct-edge repair min(w, B(pi u, pi v)) + min(w, B(pi v, pi u)) is
+// added; the item sums meet in a per-proposal shared counter, then
 //   delta = sum - S(u) - S(v) + self-loop terms.
 // The first accepted proposal in step order is applied and the rest are
-// discarded, so the chain is the one-at-a-time chain for every K.
-__global__ void __launch_bounds__(kSaThreads) sa_chain_kernel(SaArgs a) {
-    extern __shared__ int32_t s_pi_dyn[];
+// discarded, so the chain is the one-at-a-time chain for every K.  K adapts
+// to the acceptance rate: it doubles (up to kSaMaxK) after an iteration with
+// no acceptance and drops to max(a.K, 2 (j + 1)) after the j-th proposal is
+// accepted; a function of the chain's own history, so replays are exact.
+__global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
+    extern __shared__ __align__(16) uint32_t s_dyn[];
     const int c = blockIdx.x;
     if (c >= a.nchains) return;
+    constexpr int kSeg = 4 * kSaMaxK;
+    constexpr int kW = kSaThreads / 32;
     __shared__ bm_proposal s_prop[kSaMaxK];
-    __shared__ int32_t s_valid[kSaMaxK];
     __shared__ int32_t s_sum[kSaMaxK];
-    __shared__ int32_t s_seglen[4 * kSaMaxK];      // entries per list
-    __shared__ int32_t s_segbase[4 * kSaMaxK];     // offset of each list in its CSR
-    __shared__ int32_t s_acc[kSaMaxK];
     __shared__ long long s_d[kSaMaxK];
-    __shared__ int32_t s_upre[4 * kSaMaxK + 1];    // unit prefix over the lists
-    __shared__ int32_t s_ctr;
+    __shared__ int32_t s_seglen[kSeg];             // entries per list
+    __shared__ int32_t s_segbase[kSeg];            // offset of each list in its CSR
+    __shared__ int32_t s_upre[kSeg + 1];           // unit prefix over the lists
+    __shared__ uint8_t s_unit_seg[kSaUnitTable];   // unit -> list (when the units fit)
+    __shared__ int32_t s_wsum[kW];
     __shared__ int32_t s_first;
-    __shared__ long long s_fdelta;
     ChainDev& ch = a.chains[c];
     const PairDev P = a.pairs[ch.pair];
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int K = a.K;
-    const int nseg = 4 * K;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int32_t* gpi = ch.pi;
     int32_t* pi = gpi;
+    uint32_t* rowbuf = s_dyn + (size_t)warp * kSaRowCap;  // this warp's B-row buffer
     if (a.pi_smem) {
-        for (int32_t i = tid; i <= P.n; i += blockDim.x) s_pi_dyn[i] = gpi[i];
-        pi = s_pi_dyn;
-        __syncthreads();
+        int32_t* s_pi = reinterpret_cast<int32_t*>(s_dyn + (size_t)kSaRowCap * kW);
+        for (int32_t i = tid; i <= P.n; i += blockDim.x) s_pi[i] = gpi[i];
+        pi = s_pi;
     }
     int32_t* ov = ch.ov;
     uint64_t step = ch.step;
     const uint64_t end = min(a.steps, step + a.chunk);
     long long score = ch.score, accepts = ch.accepts;
+    int K = min(max(a.K, 1), kSaMaxK);
+    if (tid == 0) s_first = kSaMaxK;
+    __syncthreads();
     while (step < end) {
-        // ---- proposals and their list lengths
-        if (tid < K) {
-            const uint64_t s = step + (uint64_t)tid;
-            s_valid[tid] = s < end;
-            if (s < end) s_prop[tid] = bm_sa_proposal(ch.key, s, P.n);
-            s_sum[tid] = 0;
-        }
-        if (tid == 0) s_ctr = 0;
-        __syncthreads();
+        const int nseg = 4 * K;
+        // ---- proposals (each list's thread draws its own proposal) and list lengths
+        int32_t units = 0;
         if (tid < nseg) {
             const int w = tid >> 2, kind = tid & 3;
+            const uint64_t sidx = step + (uint64_t)w;
             int32_t len = 0, base = 0;
-            if (s_valid[w]) {
-                const int32_t me = kind < 2 ? s_prop[w].u : s_prop[w].v;
+            if (sidx < end) {
+                const bm_proposal pr = bm_sa_proposal(ch.key, sidx, P.n);
+                if (kind == 0) { s_prop[w] = pr; s_sum[w] = 0; }
+                const int32_t me = kind < 2 ? pr.u : pr.v;
                 const int32_t* ptr = (kind & 1) ? P.Ain_ptr : P.Aout_ptr;
                 base = __ldg(ptr + me);
                 len = __ldg(ptr + me + 1) - base;
             }
             s_seglen[tid] = len;
             s_segbase[tid] = base;
+            units = (len + kSaItem - 1) / kSaItem;
         }
-        __syncthreads();
-        if (tid < 32) {  // unit prefix over at most 64 lists: two per lane
-            const int i0 = 2 * lane, i1 = 2 * lane + 1;
-            const int32_t n0 = i0 < nseg ? (s_seglen[i0] + kSaUnit - 1) / kSaUnit : 0;
-            const int32_t n1 = i1 < nseg ? (s_seglen[i1] + kSaUnit - 1) / kSaUnit : 0;
-            int32_t incl = n0 + n1;
+        // ---- exclusive block scan of the unit counts
+        int32_t incl = units;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            const int32_t excl = incl - n0 - n1;
-            if (i0 <= nseg) s_upre[i0] = excl;
-            if (i1 <= nseg) s_upre[i1] = excl + n0;
-            if (lane == 31) s_upre[nseg] = incl;  // the total (index 64 when K = 16)
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
+        if (lane == 31) s_wsum[warp] = incl;
         __syncthreads();
-        const int32_t U = s_upre[nseg];
-        // ---- evaluate: warps take kSaBatch units at a time
-        for (;;) {
-            int32_t ub = 0;
-            if (lane == 0) ub = atomicAdd(&s_ctr, kSaBatch);
-            ub = __shfl_sync(0xffffffffu, ub, 0);
-            if (ub >= U) break;
-            int32_t val[kSaBatch], wid[kSaBatch];
-            uint32_t ent[kSaBatch];
-            int32_t gx[kSaBatch], fnew[kSaBatch], kindv[kSaBatch];
+        int32_t woff = 0, U = 0;
 #pragma unroll
-            for (int q = 0; q < kSaBatch; q++) {
-                const int32_t unit = ub + q;
-                ent[q] = 0;
-                wid[q] = -1;
-                kindv[q] = 0;
-                fnew[q] = 0;
-                if (unit < U) {
-                    int32_t lo = 0, hi = nseg;  // last list with s_upre[list] <= unit
-                    while (hi - lo > 1) {
-                        const int32_t mid = (lo + hi) >> 1;
-                        if (s_upre[mid] <= unit) lo = mid; else hi = mid;
-                    }
-                    const int w = lo >> 2, kind = lo & 3;
-                    wid[q] = w;
-                    kindv[q] = kind;
-                    const int32_t off = (unit - s_upre[lo]) * kSaUnit + lane;
-                    if (off < s_seglen[lo]) {
-                        const bool out = !(kind & 1);
-                        ent[q] = __ldg((out ? P.Aout_ent : P.Ain_ent) + s_segbase[lo] + off);
-                    }
-                    fnew[q] = kind < 2 ? pi[s_prop[w].v] : pi[s_prop[w].u];
+        for (int w = 0; w < kW; w++) {
+            const int32_t x = s_wsum[w];
+            woff += (w < warp) ? x : 0;
+            U += x;
+        }
+        const int32_t excl = woff + incl - units;
+        if (tid < nseg) s_upre[tid] = excl;
+        if (tid == 0) s_upre[nseg] = U;
+        const bool table = U <= kSaUnitTable;
+        if (table && tid < nseg)
+            for (int32_t x = excl; x < excl + units; x++) s_unit_seg[x] = (uint8_t)tid;
+        __syncthreads();
+        // ---- evaluate: warp w takes items w, w + kW, ...
+        for (int32_t item = warp; item < U; item += kW) {
+            int32_t lo;
+            if (table) {
+                lo = s_unit_seg[item];
+            } else {
+                lo = 0;
+                int32_t hi = nseg;  // last list with s_upre[list] <= item
+                while (hi - lo > 1) {
+                    const int32_t mid = (lo + hi) >> 1;
+                    if (s_upre[mid] <= item) lo = mid; else hi = mid;
                 }
             }
-            // first hash probes of the batch issued together
-            bool done[kSaBatch];
-            int32_t bw[kSaBatch];
+            const int w = lo >> 2, kind = lo & 3;
+            const bm_proposal pr = s_prop[w];
+            const bool out = !(kind & 1);
+            // the item's A entries, four per lane
+            const int32_t e0 = (item - s_upre[lo]) * kSaItem, len = s_seglen[lo], base = s_segbase[lo];
+            const uint32_t* alist = out ? P.Aout_ent : P.Ain_ent;
+            uint32_t ent[kSaItem / 32];
 #pragma unroll
-            for (int q = 0; q < kSaBatch; q++) {
-                done[q] = true;
-                bw[q] = 0;
-                gx[q] = 0;
-                if (ent[q] != 0) {
-                    gx[q] = pi[bm_eid(ent[q])];
-                    const bool out = !(kindv[q] & 1);
-                    done[q] = out ? hash_probe_first(P.hb, fnew[q], gx[q], &bw[q])
-                                  : hash_probe_first(P.hb, gx[q], fnew[q], &bw[q]);
-                }
+            for (int k = 0; k < kSaItem / 32; k++) {
+                const int32_t off = e0 + lane + 32 * k;
+                ent[k] = off < len ? __ldg(alist + base + off) : 0u;
             }
+            // the B row every entry of this list looks up
+            const int32_t g = kind < 2 ? pi[pr.v] : pi[pr.u];
+            const int32_t* rptr = out ? P.Bout_ptr : P.Bin_ptr;
+            const uint32_t* rent = out ? P.Bout_ent : P.Bin_ent;
+            const int32_t rb = __ldg(rptr + g), rl = __ldg(rptr + g + 1) - rb;
+            const bool staged = rl <= kSaRowCap;
+            if (staged)
+                for (int32_t j = lane; j < rl; j += 32) rowbuf[j] = __ldg(rent + rb + j);
+            __syncwarp();
+            int32_t val = 0;
 #pragma unroll
-            for (int q = 0; q < kSaBatch; q++) {
-                val[q] = 0;
-                if (ent[q] != 0) {
-                    const bool out = !(kindv[q] & 1);
-                    if (!done[q]) bw[q] = out ? bm_hash_get(P.hb, fnew[q], gx[q]) : bm_hash_get(P.hb, gx[q], fnew[q]);
-                    const int32_t w = bm_ew(ent[q]);
-                    val[q] = imin(w, bw[q]);
-                    if (kindv[q] < 2 && bm_eid(ent[q]) == s_prop[wid[q]].v) {
-                        const int32_t fu = pi[s_prop[wid[q]].u], fv = pi[s_prop[wid[q]].v];
-                        val[q] += imin(w, bm_hash_get(P.hb, fu, fv)) + imin(w, bm_hash_get(P.hb, fv, fu));
+            for (int k = 0; k < kSaItem / 32; k++) {
+                if (ent[k] == 0) continue;
+                const int32_t x = bm_eid(ent[k]), wa = bm_ew(ent[k]);
+                const int32_t gx = pi[x];
+                int32_t wb = 0;
+                if (staged) {
+                    // first row slot whose id is >= gx (zero padding sorts last)
+                    int32_t l = 0, h = rl;
+                    while (l < h) {
+                        const int32_t mid = (l + h) >> 1;
+                        const uint32_t e = rowbuf[mid];
+                        if (e != 0u && bm_eid(e) < gx) l = mid + 1; else h = mid;
                     }
+                    if (l < rl) {
+                        const uint32_t e = rowbuf[l];
+                        if (e != 0u && bm_eid(e) == gx) wb = bm_ew(e);
+                    }
+                } else {
+                    wb = out ? bm_hash_get(P.hb, g, gx) : bm_hash_get(P.hb, gx, g);
+                }
+                val += imin(wa, wb);
+                if (kind < 2 && x == pr.v) {
+                    const int32_t fu = pi[pr.u], fv = pi[pr.v];
+                    val += imin(wa, bm_hash_get(P.hb, fu, fv)) + imin(wa, bm_hash_get(P.hb, fv, fu));
                 }
             }
-            // a unit lies in one list, hence one proposal: warp sum, one atomic
+            // an item lies in one list, hence one proposal: warp sum, one atomic
 #pragma unroll
-            for (int q = 0; q < kSaBatch; q++) {
-                if (wid[q] < 0) continue;  // uniform over the warp
-                int32_t v = val[q];
-#pragma unroll
-                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0 && v) atomicAdd(&s_sum[wid[q]], v);
-            }
+            for (int o = 16; o; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+            if (lane == 0 && val) atomicAdd(&s_sum[w], val);
+            __syncwarp();  // the buffer is rewritten by the next item
         }
         __syncthreads();
         // ---- deltas and acceptance, one thread per proposal; the first
         // accepted one in step order wins
-        if (tid < K) {
-            int acc = 0;
-            long long d = 0;
-            if (s_valid[tid]) {
-                const bm_proposal pr = s_prop[tid];
-                d = (long long)s_sum[tid] - (long long)ov[pr.u] - (long long)ov[pr.v];
-                if (P.has_self) {
-                    const int32_t fu = pi[pr.u], fv = pi[pr.v];
-                    const int32_t su = __ldg(P.selfA + pr.u), sv = __ldg(P.selfA + pr.v);
-                    const int32_t bu = __ldg(P.selfB + fu), bv = __ldg(P.selfB + fv);
-                    d += imin(su, bv) - imin(su, bu) + imin(sv, bu) - imin(sv, bv);
-                }
-                acc = bm_sa_accept(d, pr.uni, bm_sa_temperature(a.t0, a.log_ratio, step + (uint64_t)tid, a.steps));
+        if (tid < K && step + (uint64_t)tid < end) {
+            const bm_proposal pr = s_prop[tid];
+            long long d = (long long)s_sum[tid] - (long long)ov[pr.u] - (long long)ov[pr.v];
+            if (P.has_self) {
+                const int32_t fu = pi[pr.u], fv = pi[pr.v];
+                const int32_t su = __ldg(P.selfA + pr.u), sv = __ldg(P.selfA + pr.v);
+                const int32_t bu = __ldg(P.selfB + fu), bv = __ldg(P.selfB + fv);
+                d += imin(su, bv) - imin(su, bu) + imin(sv, bu) - imin(sv, bv);
             }
-            s_acc[tid] = acc;
             s_d[tid] = d;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            int first = -1;
-            for (int w = 0; w < K; w++)
-                if (s_acc[w]) { first = w; break; }
-            s_first = first;
-            s_fdelta = first >= 0 ? s_d[first] : 0;
+            if (bm_sa_accept(d, pr.uni, bm_sa_temperature(a.t0, a.log_ratio, step + (uint64_t)tid, a.steps)))
+                atomicMin(&s_first, tid);
         }
         __syncthreads();
         const int first = s_first;
-        if (first >= 0) {
-            chain_apply_block(P, pi, gpi, ov, s_prop[first].u, s_prop[first].v);
-            score += s_fdelta;
+        if (first < K) {
+            const bm_proposal pr = s_prop[first];
+            score += s_d[first];
             accepts++;
             step += (uint64_t)first + 1;
+            K = min(kSaMaxK, max(a.K, 2 * (first + 1)));
+            chain_apply_block(P, pi, gpi, ov, pr.u, pr.v);  // ends with a barrier
+            if (tid == 0) s_first = kSaMaxK;
         } else {
             step = min(end, step + (uint64_t)K);
+            K = min(kSaMaxK, 2 * K);
         }
         __syncthreads();
     }
@@ -384,8 +378,8 @@ struct bm_batch {
     struct Pair {
         int32_t n = 0;
         int64_t m_real_a = 0;
-        int32_t* d[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // Aoptr, Aiptr, selfA, selfB
-        uint32_t* e[2] = {nullptr, nullptr};                                   // Aoent, Aient
+        int32_t* d[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // Aoptr, Aiptr, selfA, selfB, Boptr, Biptr
+        uint32_t* e[4] = {nullptr, nullptr, nullptr, nullptr};                 // Aoent, Aient, Boent, Bient
         unsigned long long* hash = nullptr;
         int hlog2 = 0;
         int has_self = 0;
@@ -394,6 +388,11 @@ struct bm_batch {
     PairDev* d_pairs = nullptr;
     bool dirty = true;
 };
+
+static PairDev pair_dev(const bm_batch::Pair& p) {
+    return PairDev{p.n, p.has_self, p.d[0], p.d[1], p.e[0], p.e[1], p.d[2], p.d[3], HashView{p.hash, p.hlog2, p.n + 1},
+                   p.d[4], p.d[5], p.e[2], p.e[3]};
+}
 
 static void free_pair(bm_batch::Pair& p) {
     for (auto* x : p.d) cudaFree(x);
@@ -445,6 +444,8 @@ extern "C" bm_status bm_batch_add_pair(bm_batch* b, int32_t n, int64_t mA, const
     if ((s = up(ctx, &p.d[0], HA.optr)) != BM_OK || (s = up(ctx, &p.d[1], HA.iptr)) != BM_OK ||
         (s = up(ctx, &p.d[2], HA.self)) != BM_OK || (s = up(ctx, &p.d[3], HB.self)) != BM_OK ||
         (s = up(ctx, &p.e[0], HA.oent)) != BM_OK || (s = up(ctx, &p.e[1], HA.ient)) != BM_OK ||
+        (s = up(ctx, &p.d[4], HB.optr)) != BM_OK || (s = up(ctx, &p.d[5], HB.iptr)) != BM_OK ||
+        (s = up(ctx, &p.e[2], HB.oent)) != BM_OK || (s = up(ctx, &p.e[3], HB.ient)) != BM_OK ||
         (s = up(ctx, &p.hash, HB.htab)) != BM_OK) {
         free_pair(p);
         return s;
@@ -500,18 +501,19 @@ void tune_store(const std::string& key, int32_t cand) {
 
 namespace {
 
-// Shared memory for a chain's mapping when it fits (the largest n + 1 ints of
-// the launch), else the mapping stays in global memory.  Sets the kernel's
-// dynamic shared-memory limit; called before any stream capture.
+// Dynamic shared memory of a chain: the warps' B-row buffers, plus the
+// chain's mapping when it fits (the largest n + 1 ints of the launch), else
+// the mapping stays in global memory.  Sets the kernel's dynamic
+// shared-memory limit; called before any stream capture.
 bm_status chain_smem(bm_ctx* ctx, SaArgs& args, int32_t n_max, size_t* smem) {
     const size_t need = sizeof(int32_t) * ((size_t)n_max + 1);
-    *smem = 0;
+    *smem = kSaRowBytes;
     args.pi_smem = 0;
-    if (need + 8192 <= ctx->smem_optin) {
+    if (kSaRowBytes + need + 16384 <= ctx->smem_optin) {
         args.pi_smem = 1;
-        *smem = need;
-        BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+        *smem += need;
     }
+    BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
     return BM_OK;
 }
 
@@ -550,8 +552,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
         std::vector<PairDev> hp((size_t)np);
         for (int32_t i = 0; i < np; i++) {
             const auto& p = b->pairs[(size_t)i];
-            hp[(size_t)i] = PairDev{p.n, p.has_self, p.d[0], p.d[1], p.e[0], p.e[1], p.d[2], p.d[3],
-                                    HashView{p.hash, p.hlog2, p.n + 1}};
+            hp[(size_t)i] = pair_dev(p);
         }
         cudaFree(b->d_pairs);
         b->d_pairs = nullptr;
@@ -591,7 +592,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
     args.t0 = prm->t0;
     args.log_ratio = log(prm->t_end / prm->t0);
     args.chunk = prm->chunk > 0 ? (uint64_t)prm->chunk : (uint64_t)65536;
-    const int32_t kmax = kSaMaxK;
+    const int32_t kmax = kSaMaxInitialK;
     int32_t K = prm->candidates;
     if (K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates %d above this build's limit %d", K, kmax);
     int32_t n_max = 0;
@@ -792,7 +793,7 @@ extern "C" bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32
         }
     }
     BM_CUDA(ctx, cudaSetDevice(ctx->device));
-    const int32_t kmax = kSaMaxK;
+    const int32_t kmax = kSaMaxInitialK;
     int32_t K = prm->candidates == 0 ? std::min(8, kmax) : prm->candidates;
     if (K < 1 || K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates must be 0 or 1..%d", kmax);
     int32_t n_max = 0;
@@ -811,8 +812,7 @@ extern "C" bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32
             const int64_t k = std::min<int64_t>(16, np - i0);
             for (int64_t j = 0; j < k; j++) {
                 const auto& p = b->pairs[(size_t)(i0 + j)];
-                hp[j] = PairDev{p.n, p.has_self, p.d[0], p.d[1], p.e[0], p.e[1], p.d[2], p.d[3],
-                                HashView{p.hash, p.hlog2, p.n + 1}};
+                hp[j] = pair_dev(p);
             }
             BM_CUDA(ctx, cudaMemcpyAsync(d_pairs + i0, hp, sizeof(PairDev) * (size_t)k, cudaMemcpyHostToDevice, ctx->stream));
             BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -257,7 +257,9 @@ typedef struct bm_sa_params {
     int64_t steps;       /* proposals per chain */
     double t0;           /* starting temperature */
     double t_end;        /* final temperature: T_i = t0 * exp(ln(t_end/t0) * i / steps) */
-    int32_t candidates;  /* proposals evaluated together per iteration, 1..16; 0 = autotuned */
+    int32_t candidates;  /* proposals evaluated together per iteration at the start, 1..16; 0 = autotuned.
+                          * Each chain then adapts it (up to 64) to its own acceptances: doubled after an
+                          * iteration with none, 2 (j + 1) after the j-th is accepted. */
     int64_t chunk;       /* proposals per chain per kernel launch (0 = 65536) */
 } bm_sa_params;
 
