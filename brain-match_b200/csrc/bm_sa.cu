@@ -86,14 +86,64 @@ constexpr int kSaUnitTable = 4096;  // items per iteration with an item -> list 
 
 // Dynamic shared memory of the chain kernel: the warps' B-row buffers, then
 // the chain's mapping when it fits.
-constexpr size_t kSaRowBytes = sizeof(uint32_t) * kSaRowCap * (kSaThreads / 32);
+constexpr size_t kSaRowBytes = sizeof(uint32_t) * kSaRowCap * 2 * (kSaThreads / 32);  // two buffers per warp
+static_assert(kSaRowBytes >= sizeof(uint32_t) * 4 * 4096, "the swap apply stages four rows in the row buffers");
+
+// Weight of entry id `key` in a staged B row (sorted by id, zero padding
+// last), 0 if absent.
+__device__ __forceinline__ int32_t row_weight(const uint32_t* row, int32_t len, int32_t key) {
+    int32_t l = 0, h = len;
+    while (l < h) {
+        const int32_t mid = (l + h) >> 1;
+        const uint32_t e = row[mid];
+        if (e != 0u && bm_eid(e) < key) l = mid + 1; else h = mid;
+    }
+    if (l < len) {
+        const uint32_t e = row[l];
+        if (e != 0u && bm_eid(e) == key) return bm_ew(e);
+    }
+    return 0;
+}
+
+constexpr int kSaApplyRowCap = 4096;  // entries per staged row in the swap apply (4 rows)
 
 // Apply the swap pi(a) <-> pi(b) of one chain with the whole CTA: S updates of
 // every A entry incident to a or b (as apply_kernel in bm_apply.cu), then pi.
-// `pi` is the working copy (shared or global memory), `gpi` the chain's
-// mapping in global memory, updated too.
-__device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, int32_t* ov, int32_t sa, int32_t sb) {
+// Every lookup is in one of four B rows (out and in of pi a and pi b), staged
+// in `stage` (4 x kSaApplyRowCap entries of shared memory; longer rows use
+// the hash).  `pi` is the working copy (shared or global memory), `gpi` the
+// chain's mapping in global memory, updated too.
+__device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, int32_t* ov, int32_t sa, int32_t sb,
+                                  uint32_t* stage) {
     const int32_t fa = pi[sa], fb = pi[sb];
+    // rows: 0 = out(fa), 1 = out(fb), 2 = in(fa), 3 = in(fb)
+    int32_t rlen[4];
+    bool rst[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int32_t g = (r & 1) ? fb : fa;
+        const int32_t* ptr = (r < 2) ? P.Bout_ptr : P.Bin_ptr;
+        const uint32_t* ent = (r < 2) ? P.Bout_ent : P.Bin_ent;
+        const int32_t b = __ldg(ptr + g);
+        rlen[r] = __ldg(ptr + g + 1) - b;
+        rst[r] = rlen[r] <= kSaApplyRowCap;
+        if (rst[r])
+            for (int32_t j = threadIdx.x; j < rlen[r]; j += blockDim.x) stage[r * kSaApplyRowCap + j] = __ldg(ent + b + j);
+    }
+    __syncthreads();
+    // B(g, h) for g in {fa, fb} (rows 0, 1) and B(h, g) (rows 2, 3)
+    auto bout = [&](int32_t g, int32_t h) -> int32_t {
+        const bool a = g == fa;
+        const int32_t len = a ? rlen[0] : rlen[1];
+        const bool st = a ? rst[0] : rst[1];
+        return st ? row_weight(stage + (a ? 0 : kSaApplyRowCap), len, h) : bm_hash_get(P.hb, g, h);
+    };
+    auto bin = [&](int32_t h, int32_t g) -> int32_t {
+        const bool a = g == fa;
+        const int32_t len = a ? rlen[2] : rlen[3];
+        const bool st = a ? rst[2] : rst[3];
+        return st ? row_weight(stage + (a ? 2 : 3) * kSaApplyRowCap, len, h) : bm_hash_get(P.hb, h, g);
+    };
     for (int side = 0; side < 2; side++) {
         const int32_t me = side ? sb : sa, other = side ? sa : sb;
         const int32_t fme = side ? fb : fa, fnew = side ? fa : fb;
@@ -104,11 +154,11 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
                 if (ent == 0) continue;
                 const int32_t x = bm_eid(ent), w = bm_ew(ent);
                 if (x == other) {
-                    const int32_t d = imin(w, bm_hash_get(P.hb, fnew, fme)) - imin(w, bm_hash_get(P.hb, fme, fnew));
+                    const int32_t d = imin(w, bout(fnew, fme)) - imin(w, bout(fme, fnew));
                     if (d) { atomicAdd(ov + me, d); atomicAdd(ov + other, d); }
                 } else {
                     const int32_t gx = pi[x];
-                    const int32_t d = imin(w, bm_hash_get(P.hb, fnew, gx)) - imin(w, bm_hash_get(P.hb, fme, gx));
+                    const int32_t d = imin(w, bout(fnew, gx)) - imin(w, bout(fme, gx));
                     if (d) { atomicAdd(ov + me, d); atomicAdd(ov + x, d); }
                 }
             }
@@ -121,7 +171,7 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
                 const int32_t x = bm_eid(ent), w = bm_ew(ent);
                 if (x == other) continue;
                 const int32_t gx = pi[x];
-                const int32_t d = imin(w, bm_hash_get(P.hb, gx, fnew)) - imin(w, bm_hash_get(P.hb, gx, fme));
+                const int32_t d = imin(w, bin(gx, fnew)) - imin(w, bin(gx, fme));
                 if (d) { atomicAdd(ov + me, d); atomicAdd(ov + x, d); }
             }
         }
@@ -177,9 +227,9 @@ __global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int32_t* gpi = ch.pi;
     int32_t* pi = gpi;
-    uint32_t* rowbuf = s_dyn + (size_t)warp * kSaRowCap;  // this warp's B-row buffer
+    uint32_t* rowbuf = s_dyn + (size_t)warp * 2 * kSaRowCap;  // this warp's two B-row buffers
     if (a.pi_smem) {
-        int32_t* s_pi = reinterpret_cast<int32_t*>(s_dyn + (size_t)kSaRowCap * kW);
+        int32_t* s_pi = reinterpret_cast<int32_t*>(s_dyn + (size_t)kSaRowCap * 2 * kW);
         for (int32_t i = tid; i <= P.n; i += blockDim.x) s_pi[i] = gpi[i];
         pi = s_pi;
     }
@@ -233,73 +283,116 @@ __global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
         if (table && tid < nseg)
             for (int32_t x = excl; x < excl + units; x++) s_unit_seg[x] = (uint8_t)tid;
         __syncthreads();
-        // ---- evaluate: warp w takes items w, w + kW, ...
-        for (int32_t item = warp; item < U; item += kW) {
-            int32_t lo;
-            if (table) {
-                lo = s_unit_seg[item];
-            } else {
-                lo = 0;
-                int32_t hi = nseg;  // last list with s_upre[list] <= item
-                while (hi - lo > 1) {
-                    const int32_t mid = (lo + hi) >> 1;
-                    if (s_upre[mid] <= item) lo = mid; else hi = mid;
-                }
-            }
-            const int w = lo >> 2, kind = lo & 3;
-            const bm_proposal pr = s_prop[w];
-            const bool out = !(kind & 1);
-            // the item's A entries, four per lane
-            const int32_t e0 = (item - s_upre[lo]) * kSaItem, len = s_seglen[lo], base = s_segbase[lo];
-            const uint32_t* alist = out ? P.Aout_ent : P.Ain_ent;
-            uint32_t ent[kSaItem / 32];
+        // ---- evaluate: warp w takes items w, w + kW, ... through a three-stage
+        // pipeline: the B-row bounds and A entries of item i + 2 kW are
+        // loaded, the B row of item i + kW is copied (cp.async) into the
+        // warp's other buffer, and item i is searched, all at once
+        {
+            struct Stage {
+                int32_t item, w, kind, g, rb, rl;
+                uint32_t ent[kSaItem / 32];
+            };
+            auto fetch = [&](int32_t item, Stage& st) {
+                st.item = item;
+                st.rb = 0;
+                st.rl = 0;
+                st.w = 0;
+                st.kind = 0;
+                st.g = 0;
 #pragma unroll
-            for (int k = 0; k < kSaItem / 32; k++) {
-                const int32_t off = e0 + lane + 32 * k;
-                ent[k] = off < len ? __ldg(alist + base + off) : 0u;
-            }
-            // the B row every entry of this list looks up
-            const int32_t g = kind < 2 ? pi[pr.v] : pi[pr.u];
-            const int32_t* rptr = out ? P.Bout_ptr : P.Bin_ptr;
-            const uint32_t* rent = out ? P.Bout_ent : P.Bin_ent;
-            const int32_t rb = __ldg(rptr + g), rl = __ldg(rptr + g + 1) - rb;
-            const bool staged = rl <= kSaRowCap;
-            if (staged)
-                for (int32_t j = lane; j < rl; j += 32) rowbuf[j] = __ldg(rent + rb + j);
-            __syncwarp();
-            int32_t val = 0;
-#pragma unroll
-            for (int k = 0; k < kSaItem / 32; k++) {
-                if (ent[k] == 0) continue;
-                const int32_t x = bm_eid(ent[k]), wa = bm_ew(ent[k]);
-                const int32_t gx = pi[x];
-                int32_t wb = 0;
-                if (staged) {
-                    // first row slot whose id is >= gx (zero padding sorts last)
-                    int32_t l = 0, h = rl;
-                    while (l < h) {
-                        const int32_t mid = (l + h) >> 1;
-                        const uint32_t e = rowbuf[mid];
-                        if (e != 0u && bm_eid(e) < gx) l = mid + 1; else h = mid;
-                    }
-                    if (l < rl) {
-                        const uint32_t e = rowbuf[l];
-                        if (e != 0u && bm_eid(e) == gx) wb = bm_ew(e);
-                    }
+                for (int k = 0; k < kSaItem / 32; k++) st.ent[k] = 0u;
+                if (item >= U) return;
+                int32_t lo;
+                if (table) {
+                    lo = s_unit_seg[item];
                 } else {
-                    wb = out ? bm_hash_get(P.hb, g, gx) : bm_hash_get(P.hb, gx, g);
+                    lo = 0;
+                    int32_t hi = nseg;  // last list with s_upre[list] <= item
+                    while (hi - lo > 1) {
+                        const int32_t mid = (lo + hi) >> 1;
+                        if (s_upre[mid] <= item) lo = mid; else hi = mid;
+                    }
                 }
-                val += imin(wa, wb);
-                if (kind < 2 && x == pr.v) {
-                    const int32_t fu = pi[pr.u], fv = pi[pr.v];
-                    val += imin(wa, bm_hash_get(P.hb, fu, fv)) + imin(wa, bm_hash_get(P.hb, fv, fu));
-                }
-            }
-            // an item lies in one list, hence one proposal: warp sum, one atomic
+                st.w = lo >> 2;
+                st.kind = lo & 3;
+                const bool out = !(st.kind & 1);
+                const int32_t e0 = (item - s_upre[lo]) * kSaItem, len = s_seglen[lo], base = s_segbase[lo];
+                const uint32_t* alist = out ? P.Aout_ent : P.Ain_ent;
 #pragma unroll
-            for (int o = 16; o; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
-            if (lane == 0 && val) atomicAdd(&s_sum[w], val);
-            __syncwarp();  // the buffer is rewritten by the next item
+                for (int k = 0; k < kSaItem / 32; k++) {
+                    const int32_t off = e0 + lane + 32 * k;
+                    if (off < len) st.ent[k] = __ldg(alist + base + off);
+                }
+                const bm_proposal& pr = s_prop[st.w];
+                st.g = st.kind < 2 ? pi[pr.v] : pi[pr.u];
+                const int32_t* rptr = out ? P.Bout_ptr : P.Bin_ptr;
+                st.rb = __ldg(rptr + st.g);
+                st.rl = __ldg(rptr + st.g + 1) - st.rb;
+            };
+            // B rows start on 16-byte boundaries (rows are padded to multiples of 4)
+            auto copy_row = [&](const Stage& st, int buf) {
+                if (st.item < U && st.rl <= kSaRowCap) {
+                    const uint32_t* rent = !(st.kind & 1) ? P.Bout_ent : P.Bin_ent;
+                    const uint32_t dst0 = (uint32_t)__cvta_generic_to_shared(rowbuf + (size_t)buf * kSaRowCap);
+                    for (int32_t j = 4 * lane; j < st.rl; j += 128)
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst0 + 4u * (uint32_t)j),
+                                     "l"(rent + st.rb + j) : "memory");
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            };
+            Stage cur, nxt, far;
+            fetch(warp, cur);
+            fetch(warp + kW, nxt);
+            copy_row(cur, 0);
+            int buf = 0;
+            for (int32_t item = warp; item < U; item += kW) {
+                copy_row(nxt, buf ^ 1);
+                fetch(item + 2 * kW, far);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");  // this item's row has landed
+                __syncwarp();
+                const uint32_t* row = rowbuf + (size_t)buf * kSaRowCap;
+                const bool out = !(cur.kind & 1);
+                const bool staged = cur.rl <= kSaRowCap;
+                const bm_proposal pr = s_prop[cur.w];
+                int32_t val = 0;
+#pragma unroll
+                for (int k = 0; k < kSaItem / 32; k++) {
+                    if (cur.ent[k] == 0) continue;
+                    const int32_t x = bm_eid(cur.ent[k]), wa = bm_ew(cur.ent[k]);
+                    const int32_t gx = pi[x];
+                    int32_t wb = 0;
+                    if (staged) {
+                        // first row slot whose id is >= gx (zero padding sorts last)
+                        int32_t l = 0, h = cur.rl;
+                        while (l < h) {
+                            const int32_t mid = (l + h) >> 1;
+                            const uint32_t e = row[mid];
+                            if (e != 0u && bm_eid(e) < gx) l = mid + 1; else h = mid;
+                        }
+                        if (l < cur.rl) {
+                            const uint32_t e = row[l];
+                            if (e != 0u && bm_eid(e) == gx) wb = bm_ew(e);
+                        }
+                    } else {
+                        wb = out ? bm_hash_get(P.hb, cur.g, gx) : bm_hash_get(P.hb, gx, cur.g);
+                    }
+                    val += imin(wa, wb);
+                    if (cur.kind < 2 && x == pr.v) {
+                        const int32_t fu = pi[pr.u], fv = pi[pr.v];
+                        val += imin(wa, bm_hash_get(P.hb, fu, fv)) + imin(wa, bm_hash_get(P.hb, fv, fu));
+                    }
+                }
+                // an item lies in one list, hence one proposal: warp sum, one atomic
+#pragma unroll
+                for (int o = 16; o; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+                if (lane == 0 && val) atomicAdd(&s_sum[cur.w], val);
+                __syncwarp();  // this buffer is rewritten two items on
+                cur = nxt;
+                nxt = far;
+                buf ^= 1;
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            __syncwarp();
         }
         __syncthreads();
         // ---- deltas and acceptance, one thread per proposal; the first
@@ -325,7 +418,7 @@ __global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
             accepts++;
             step += (uint64_t)first + 1;
             K = min(kSaMaxK, max(a.K, 2 * (first + 1)));
-            chain_apply_block(P, pi, gpi, ov, pr.u, pr.v);  // ends with a barrier
+            chain_apply_block(P, pi, gpi, ov, pr.u, pr.v, s_dyn);  // ends with a barrier
             if (tid == 0) s_first = kSaMaxK;
         } else {
             step = min(end, step + (uint64_t)K);
