@@ -383,22 +383,15 @@ def bf16_peak():
         return 1590.0, "fallback"
 
 
-def learned_compare(device, A, B, init, rows, plain, seconds):
-    """Learned vs plain proposals from the same initial matching: time to the
-    plain search's converged score (record harvest, training and inference
-    included), hit rates of one proposal pass, and the tensor-core scorer's
-    throughput against the measured BF16 peak."""
+def scorer_throughput(device, A, B, init, rows):
+    """The MLP row scorer on 1,184 rows (8 per SM pair of CTAs), inputs
+    resident: tensor-core and SIMT kernels, CUDA events, and the tensor-core
+    kernel against the measured BF16 peak."""
     n = A.n
-
-    def engine():
-        e = bm.Engine(device)
-        e.set_graphs(A, B)
-        e.set_mapping(init)
-        return e
-
-    out = {"plain_seconds": plain["seconds"], "plain_score": plain["score"]}
-    # scorer throughput, inputs resident: 8 rows per SM-pair of CTAs
-    e = engine()
+    out = {}
+    e = bm.Engine(device)
+    e.set_graphs(A, B)
+    e.set_mapping(init)
     m = bm.Mlp(e, seed=1)
     R = min(n, 1184)
     d_rows = e.dev_alloc(4 * R)
@@ -428,6 +421,24 @@ def learned_compare(device, A, B, init, rows, plain, seconds):
     e.dev_free(d_rows)
     e.dev_free(d_sc)
     e.close()
+    return out
+
+
+def learned_compare(device, A, B, init, rows, plain, seconds):
+    """Learned vs plain proposals from the same initial matching: time to the
+    plain search's converged score (record harvest, training and inference
+    included), hit rates of one proposal pass, and the tensor-core scorer's
+    throughput against the measured BF16 peak."""
+    n = A.n
+
+    def engine():
+        e = bm.Engine(device)
+        e.set_graphs(A, B)
+        e.set_mapping(init)
+        return e
+
+    out = {"plain_seconds": plain["seconds"], "plain_score": plain["score"]}
+    out.update(scorer_throughput(device, A, B, init, rows))
 
     def one_pass(mm, uniform):
         _, p, s = mm.search(rows, topk=64, max_sweeps=1, exact_fallback=False, uniform=uniform, seed=7)
@@ -502,7 +513,7 @@ def higher_order(device, A, B, init):
     return out
 
 
-def sa_chains(device, steps):
+def sa_chains(device, steps, candidates=0):
     """Batched annealing chains: 16 pairs with n uniform in 2,000..20,000 and
     80 n edges, 4 chains per pair, T 5 -> 0.01 geometric."""
     rng = np.random.default_rng(3)
@@ -520,9 +531,9 @@ def sa_chains(device, steps):
     chain_pair = np.repeat(np.arange(16), 4).astype(np.int32)
     keys = 1000 + np.arange(64)
     init_pis = [inits[p] for p in chain_pair]
-    batch.sa_run(chain_pair, keys, init_pis, 2000)  # autotune and warm-up
+    batch.sa_run(chain_pair, keys, init_pis, 2000, candidates=candidates)  # autotune and warm-up
     t0 = time.perf_counter()
-    pis, scores, acc, st = batch.sa_run(chain_pair, keys, init_pis, steps, t0=5.0, t_end=0.01)
+    pis, scores, acc, st = batch.sa_run(chain_pair, keys, init_pis, steps, t0=5.0, t_end=0.01, candidates=candidates)
     dt = time.perf_counter() - t0
     out = {"chains": 64, "pairs": 16, "n_range": [min(ns), max(ns)], "steps_per_chain": steps,
            "proposals_per_s": 64 * steps / dt, "seconds": dt, "candidates_per_iteration": int(st.candidates),
@@ -565,6 +576,7 @@ def delta_table(device, A, B, init, plain):
         e.record(b)
         e.sync()
         t_build = e.elapsed_ms(a, b) / 1e3
+        e.table_topk(d_tab, ld, 1024)  # warm-up (scratch allocated on first use)
         t = time.perf_counter()
         e.table_topk(d_tab, ld, 1024)
         t_topk = time.perf_counter() - t
@@ -609,6 +621,25 @@ def plain_search(eng, rows, seconds):
             "score": int(prog.score)}
 
 
+def run_section(args):
+    """One side section of the bench on the full-scale workload, alone."""
+    if args.only == "sa_chains":
+        out = sa_chains(0, args.sa_steps, args.sa_candidates)
+    else:
+        A, B, truth, init, rows = make_workload()
+        if args.only == "initial_matching":
+            out = initial_matching(0, A, B, init)
+        elif args.only == "higher_order":
+            out = higher_order(0, A, B, init)
+        elif args.only == "delta_table":
+            out = delta_table(0, A, B, init, {})
+        elif args.only == "mlp_scorer":
+            out = scorer_throughput(0, A, B, init, rows)
+        else:
+            out = subset_assignment(0, A, B, init, "initial matching")
+    print(json.dumps({"section": args.only, "result": out}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -622,7 +653,15 @@ def main():
     ap.add_argument("--learned-seconds", type=float, default=90.0)
     ap.add_argument("--no-extras", action="store_true", help="skip the k-set and annealing-chain sections")
     ap.add_argument("--sa-steps", type=int, default=1_000_000)
+    ap.add_argument("--sa-candidates", type=int, default=0, help="starting proposals per iteration (0: autotuned)")
+    ap.add_argument("--only", default=None,
+                    choices=["initial_matching", "higher_order", "delta_table", "subset_assignment", "sa_chains",
+                             "mlp_scorer"],
+                    help="run one side section alone and print its result (a profiling target, not a bench line)")
     args = ap.parse_args()
+    if args.only:
+        run_section(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local, dist = dist_setup()
