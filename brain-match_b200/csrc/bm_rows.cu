@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     auto cluster_sum = [&](int32_t gi) -> int4 {
         int4 s4 = reinterpret_cast<const int4*>(acc)[gi];
         for (int q = 1; q < CL; q++) {
-            const int4 t4 = *reinterpret_cast<const int4*>(cluster.map_shared_rank(acc + 4 * gi, (crank + q) % CL));
+            const int rk = crank + q < CL ? crank + q : crank + q - CL;  // (crank + q) mod CL
+            const int4 t4 = *reinterpret_cast<const int4*>(cluster.map_shared_rank(acc + 4 * gi, rk));
             s4.x += t4.x; s4.y += t4.y; s4.z += t4.z; s4.w += t4.w;
         }
         return s4;
