@@ -22,7 +22,8 @@
 // One CTA per set: the members' lists are scanned once with k-1 B lookups per
 // entry (atomics into g in shared memory), then the k! permutations are
 // enumerated in lexicographic order, each thread a contiguous block stepped by
-// next-permutation, and reduced to the best (largest delta, lowest index).
+// the lexicographic successor (the permutation packed in one register), and
+// reduced to the best (largest delta, lowest index).
 #include <climits>
 #include <vector>
 
@@ -66,14 +67,112 @@ __device__ __forceinline__ void decode_perm(int32_t p, int k, int32_t* s) {
     }
 }
 
-__device__ __forceinline__ void next_perm(int k, int32_t* s) {
-    int i = k - 2;
-    while (i >= 0 && s[i] >= s[i + 1]) i--;
-    if (i < 0) return;
-    int j = k - 1;
-    while (s[j] <= s[i]) j--;
-    int32_t t = s[i]; s[i] = s[j]; s[j] = t;
-    for (int a = i + 1, b = k - 1; a < b; a++, b--) { t = s[a]; s[a] = s[b]; s[b] = t; }
+// The permutations [p0, p1) of K members, in lexicographic order, evaluated
+// from the gain table g (shared), the internal entries and the self-loop
+// terms; the best (largest delta, lowest index) is returned in bd, bp.  A
+// permutation is held as K 4-bit fields of one register (field i = s[i]), so
+// that the lexicographic successor is shifts and masks rather than indexed
+// register arrays.
+__device__ __forceinline__ uint32_t nib(uint32_t S, int i) { return (S >> (4 * i)) & 15u; }
+
+template <int K>
+__device__ void enumerate_perms(const KsetArgs& a, int64_t set, int32_t p0, int32_t p1, const int32_t* g,
+                                const int32_t* Bsub, const int32_t* sA, const int32_t* sB, int32_t ni,
+                                const int32_t* ie_i, const int32_t* ie_j, const int32_t* ie_w, long long& bd,
+                                int32_t& bp) {
+    int32_t s0[kMaxK];
+    decode_perm(p0, K, s0);
+    uint32_t S = 0;
+#pragma unroll
+    for (int i = 0; i < K; i++) S |= (uint32_t)s0[i] << (4 * i);
+    long long base = 0;  // sum of g[i][i]
+#pragma unroll
+    for (int i = 0; i < K; i++) base += g[i * K + i];
+    if constexpr (K >= 4) {
+        // Without internal entries, self-loop terms or per-permutation output,
+        // six consecutive permutations (p0 and p1 multiples of 6) share the
+        // first K - 3 fields and order the last three values a < b < c as abc,
+        // acb, bac, bca, cab, cba: one successor step per six, nine table reads.
+        if (ni == 0 && !a.has_self && !a.all && p0 % 6 == 0 && p1 % 6 == 0) {
+            const int32_t* g0 = g + (K - 3) * K;
+            const int32_t* g1 = g + (K - 2) * K;
+            const int32_t* g2 = g + (K - 1) * K;
+            for (int32_t p = p0; p < p1; p += 6) {
+                long long sp = -base;
+#pragma unroll
+                for (int i = 0; i < K - 3; i++) sp += g[i * K + (int)nib(S, i)];
+                const int x = (int)nib(S, K - 3), y = (int)nib(S, K - 2), z = (int)nib(S, K - 1);
+                const long long d6[6] = {sp + g0[x] + g1[y] + g2[z], sp + g0[x] + g1[z] + g2[y],
+                                         sp + g0[y] + g1[x] + g2[z], sp + g0[y] + g1[z] + g2[x],
+                                         sp + g0[z] + g1[x] + g2[y], sp + g0[z] + g1[y] + g2[x]};
+#pragma unroll
+                for (int q = 0; q < 6; q++)
+                    if (d6[q] > bd) { bd = d6[q]; bp = p + q; }
+                // the group's last permutation (suffix z y x), then its successor
+                S = (S & ~(0xFFFu << (4 * (K - 3)))) |
+                    ((uint32_t)z << (4 * (K - 3))) | ((uint32_t)y << (4 * (K - 2))) | ((uint32_t)x << (4 * (K - 1)));
+                int piv = -1;
+#pragma unroll
+                for (int i = 0; i < K - 1; i++)
+                    if (nib(S, i) < nib(S, i + 1)) piv = i;
+                if (piv < 0) break;
+                const uint32_t sv = nib(S, piv);
+                int j = piv + 1;
+#pragma unroll
+                for (int jj = 1; jj < K; jj++)
+                    if (jj > piv && nib(S, jj) > sv) j = jj;
+                const uint32_t sj = nib(S, j);
+                S = (S & ~((15u << (4 * piv)) | (15u << (4 * j)))) | (sj << (4 * piv)) | (sv << (4 * j));
+                uint32_t R = 0;
+#pragma unroll
+                for (int i = 0; i < K; i++) {
+                    const int src = (i > piv) ? (K - 1 - (i - piv - 1)) : i;
+                    R |= nib(S, src) << (4 * i);
+                }
+                S = R;
+            }
+            return;
+        }
+    }
+    for (int32_t p = p0; p < p1; p++) {
+        long long d = -base;
+#pragma unroll
+        for (int i = 0; i < K; i++) d += g[i * K + (int)nib(S, i)];
+        for (int32_t e = 0; e < ni; e++) {
+            const int i = ie_i[e], j = ie_j[e], w = ie_w[e];
+            const int si = (int)nib(S, i), sj = (int)nib(S, j);
+            d += imin(w, Bsub[si * K + sj]) + imin(w, Bsub[i * K + j]) - imin(w, Bsub[si * K + j]) -
+                 imin(w, Bsub[i * K + sj]);
+        }
+        if (a.has_self) {
+#pragma unroll
+            for (int i = 0; i < K; i++) d += imin(sA[i], sB[nib(S, i)]) - imin(sA[i], sB[i]);
+        }
+        if (a.all) a.all[set * a.kfact + p] = d;
+        if (d > bd) { bd = d; bp = p; }
+        // lexicographic successor: pivot = last i with s[i] < s[i+1]; swap it
+        // with the last larger field after it; reverse the fields after it
+        int piv = -1;
+#pragma unroll
+        for (int i = 0; i < K - 1; i++)
+            if (nib(S, i) < nib(S, i + 1)) piv = i;
+        if (piv < 0) break;
+        const uint32_t sp = nib(S, piv);
+        int j = piv + 1;
+#pragma unroll
+        for (int jj = 1; jj < K; jj++)
+            if (jj > piv && nib(S, jj) > sp) j = jj;
+        const uint32_t sj = nib(S, j);
+        S = (S & ~((15u << (4 * piv)) | (15u << (4 * j)))) | (sj << (4 * piv)) | (sp << (4 * j));
+        // reverse fields piv+1 .. K-1
+        uint32_t R = 0;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const int src = (i > piv) ? (K - 1 - (i - piv - 1)) : i;
+            R |= nib(S, src) << (4 * i);
+        }
+        S = R;
+    }
 }
 
 __global__ void __launch_bounds__(kKThreads) kset_kernel(KsetArgs a) {
@@ -149,27 +248,20 @@ __global__ void __launch_bounds__(kKThreads) kset_kernel(KsetArgs a) {
         __syncthreads();
         const int32_t ni = bad ? 0 : n_int;
         // ---- enumerate permutations
-        const int32_t per = (a.kfact + kKThreads - 1) / kKThreads;
+        int32_t per = (a.kfact + kKThreads - 1) / kKThreads;
+        if (k >= 4) per = (per + 5) / 6 * 6;  // whole groups of six (see enumerate_perms)
         const int32_t p0 = tid * per, p1 = min(a.kfact, p0 + per);
         long long bd = LLONG_MIN;
         int32_t bp = INT_MAX;
         if (!bad && p0 < p1) {
-            int32_t s[kMaxK];
-            decode_perm(p0, k, s);
-            for (int32_t p = p0; p < p1; p++) {
-                long long d = 0;
-                for (int i = 0; i < k; i++) d += (long long)g[i * k + s[i]] - g[i * k + i];
-                for (int32_t e = 0; e < ni; e++) {
-                    const int i = ie_i[e], j = ie_j[e], w = ie_w[e];
-                    const int si = s[i], sj = s[j];
-                    d += imin(w, Bsub[si * k + sj]) + imin(w, Bsub[i * k + j]) - imin(w, Bsub[si * k + j]) -
-                         imin(w, Bsub[i * k + sj]);
-                }
-                if (a.has_self)
-                    for (int i = 0; i < k; i++) d += imin(sA[i], sB[s[i]]) - imin(sA[i], sB[i]);
-                if (a.all) a.all[set * a.kfact + p] = d;
-                if (d > bd) { bd = d; bp = p; }
-                next_perm(k, s);
+            switch (k) {
+                case 2: enumerate_perms<2>(a, set, p0, p1, g, Bsub, sA, sB, ni, ie_i, ie_j, ie_w, bd, bp); break;
+                case 3: enumerate_perms<3>(a, set, p0, p1, g, Bsub, sA, sB, ni, ie_i, ie_j, ie_w, bd, bp); break;
+                case 4: enumerate_perms<4>(a, set, p0, p1, g, Bsub, sA, sB, ni, ie_i, ie_j, ie_w, bd, bp); break;
+                case 5: enumerate_perms<5>(a, set, p0, p1, g, Bsub, sA, sB, ni, ie_i, ie_j, ie_w, bd, bp); break;
+                case 6: enumerate_perms<6>(a, set, p0, p1, g, Bsub, sA, sB, ni, ie_i, ie_j, ie_w, bd, bp); break;
+                case 7: enumerate_perms<7>(a, set, p0, p1, g, Bsub, sA, sB, ni, ie_i, ie_j, ie_w, bd, bp); break;
+                default: enumerate_perms<8>(a, set, p0, p1, g, Bsub, sA, sB, ni, ie_i, ie_j, ie_w, bd, bp); break;
             }
         }
         if (bad && a.all)

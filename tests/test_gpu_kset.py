@@ -83,6 +83,29 @@ def test_eight_sets_full_enumeration(golden_cfg1):
     e.close()
 
 
+@pytest.mark.parametrize("k", [4, 5, 6, 7, 8])
+def test_best_permutation_without_full_output(golden_cfg1, k):
+    """Sets without internal entries take the grouped enumeration when no
+    per-permutation output is asked for; best delta and permutation (lowest
+    lexicographic index on ties) equal the full enumeration's and the oracle's."""
+    n, A, B = golden_graphs(golden_cfg1)
+    pi = golden_cfg1["pi_init"]
+    e = make_engine(n, A, B, pi)
+    orc = Oracle(n, A, B)
+    rng = np.random.default_rng(40 + k)
+    sets = np.array([rng.choice(np.arange(1, n + 1), k, replace=False) for _ in range(24)], np.int32)
+    best_f, perm_f, alld = e.kset_eval(k, sets, all_deltas=True)
+    best, perm = e.kset_eval(k, sets)
+    np.testing.assert_array_equal(best, best_f)
+    np.testing.assert_array_equal(perm, perm_f)
+    perms = lex_perms(k)
+    for s in range(sets.shape[0]):
+        assert best[s] == alld[s].max()
+        assert list(perm[s]) == perms[int(np.argmax(alld[s]))]
+        assert orc.perm_delta(pi, sets[s], perm[s]) == best[s]
+    e.close()
+
+
 def test_selfloop_sets_exact(golden_selfloop):
     g = golden_selfloop
     n, A, B = golden_graphs(g)
