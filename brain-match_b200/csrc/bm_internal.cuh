@@ -221,6 +221,22 @@ __device__ __forceinline__ int32_t bm_hash_get_small(const HashView& hv, int32_t
     return 0;
 }
 
+// Weight of neighbour id `key` in a B row staged in shared memory (entries
+// sorted by id, zero padding last), 0 if absent: a binary search.
+__device__ __forceinline__ int32_t bm_row_weight(const uint32_t* row, int32_t len, int32_t key) {
+    int32_t l = 0, h = len;
+    while (l < h) {
+        const int32_t mid = (l + h) >> 1;
+        const uint32_t e = row[mid];
+        if (e != 0u && bm_eid(e) < key) l = mid + 1; else h = mid;
+    }
+    if (l < len) {
+        const uint32_t e = row[l];
+        if (e != 0u && bm_eid(e) == key) return bm_ew(e);
+    }
+    return 0;
+}
+
 __device__ __forceinline__ int32_t imin(int32_t a, int32_t b) { return a < b ? a : b; }
 
 // Kernel launchers implemented across the .cu files.

@@ -19,9 +19,12 @@
 // sum moves every member's external and internal edges as if the other end
 // stayed; the second repairs each internal edge to its true new value.
 //
-// One CTA per set: the members' lists are scanned once with k-1 B lookups per
-// entry (atomics into g in shared memory), then the k! permutations are
-// enumerated in lexicographic order, each thread a contiguous block stepped by
+// One CTA per set: the B rows of the members' images (out and in, B ids,
+// sorted) are staged in shared memory, then the members' lists are scanned
+// once with k-1 lookups per entry, binary searches in the staged rows (the
+// hash for rows that do not fit), atomics into g in shared memory; then the
+// k! permutations are enumerated in lexicographic order, each thread a
+// contiguous block stepped by
 // the lexicographic successor (the permutation packed in one register), and
 // reduced to the best (largest delta, lowest index).
 #include <climits>
@@ -51,7 +54,14 @@ struct KsetArgs {
     int32_t* best_perm;  // nsets * k
     long long* all;      // nsets * kfact, optional
     int32_t* status;     // nonzero: some set was rejected (see bm_kset_eval)
+    // B's rows in B ids (sorted by id): the gains' lookups are staged from them
+    const int32_t* Bout_ptr;
+    const int32_t* Bin_ptr;
+    const uint32_t* Bout_ent0;
+    const uint32_t* Bin_ent0;
 };
+
+constexpr int kKsetRowCap = 8192;  // B-row entries a set stages in shared memory (the rest: hash)
 
 __device__ __forceinline__ void decode_perm(int32_t p, int k, int32_t* s) {
     int32_t avail[kMaxK];
@@ -176,6 +186,8 @@ __device__ void enumerate_perms(const KsetArgs& a, int64_t set, int32_t p0, int3
 }
 
 __global__ void __launch_bounds__(kKThreads) kset_kernel(KsetArgs a) {
+    extern __shared__ uint32_t rowbuf[];  // kKsetRowCap entries
+    __shared__ int32_t r_off[2 * kMaxK], r_len[2 * kMaxK];  // row 2q: B-out(f_q), 2q+1: B-in(f_q); off -1: not staged
     __shared__ int32_t t[kMaxK], f[kMaxK], sA[kMaxK], sB[kMaxK];
     __shared__ int32_t g[kMaxK * kMaxK], Bsub[kMaxK * kMaxK];
     __shared__ int32_t n_int, bad;
@@ -215,6 +227,27 @@ __global__ void __launch_bounds__(kKThreads) kset_kernel(KsetArgs a) {
             const int p = tid / k, q = tid % k;
             Bsub[tid] = (p == q) ? 0 : bm_hash_get(a.hb, f[p], f[q]);
         }
+        // ---- stage the B rows of the members' images (out and in), in order,
+        // while they fit
+        if (tid == 0) {
+            int32_t off = 0;
+            for (int r = 0; r < 2 * k; r++) {
+                const int32_t* ptr = (r & 1) ? a.Bin_ptr : a.Bout_ptr;
+                const int32_t g0 = f[r >> 1];
+                const int32_t len = ptr[g0 + 1] - ptr[g0];
+                r_len[r] = len;
+                r_off[r] = (off + len <= kKsetRowCap) ? off : -1;
+                if (r_off[r] >= 0) off += len;
+            }
+        }
+        __syncthreads();
+        for (int r = 0; r < 2 * k; r++) {
+            if (r_off[r] < 0) continue;
+            const int32_t* ptr = (r & 1) ? a.Bin_ptr : a.Bout_ptr;
+            const uint32_t* ent = ((r & 1) ? a.Bin_ent0 : a.Bout_ent0) + ptr[f[r >> 1]];
+            for (int32_t j = tid; j < r_len[r]; j += kKThreads) rowbuf[r_off[r] + j] = ent[j];
+        }
+        __syncthreads();
         // ---- gains and internal entries: scan each member's out- and in-list
         for (int i = 0; i < k; i++) {
             for (int dir = 0; dir < 2; dir++) {
@@ -235,7 +268,10 @@ __global__ void __launch_bounds__(kKThreads) kset_kernel(KsetArgs a) {
                     }
                     for (int q = 0; q < k; q++) {
                         if (q == i) continue;
-                        const int32_t bw = dir ? bm_hash_get(a.hb, gx, f[q]) : bm_hash_get(a.hb, f[q], gx);
+                        // out: B(f_q, pi x) in B-out(f_q); in: B(pi x, f_q) in B-in(f_q)
+                        const int r = 2 * q + dir;
+                        const int32_t bw = r_off[r] >= 0 ? bm_row_weight(rowbuf + r_off[r], r_len[r], gx)
+                                           : (dir ? bm_hash_get(a.hb, gx, f[q]) : bm_hash_get(a.hb, f[q], gx));
                         const int32_t c = imin(w, bw);
                         if (c) atomicAdd(&g[i * k + q], c);
                     }
@@ -390,6 +426,10 @@ bm_status bm_launch_kset(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t 
     a.n = ctx->n;
     a.k = k;
     a.kfact = factorial(k);
+    a.Bout_ptr = ctx->g[1].out_ptr;
+    a.Bin_ptr = ctx->g[1].in_ptr;
+    a.Bout_ent0 = ctx->g[1].out_ent0;
+    a.Bin_ent0 = ctx->g[1].in_ent0;
     a.sets = d_sets;
     a.nsets = nsets;
     a.best_delta = d_best;
@@ -397,7 +437,7 @@ bm_status bm_launch_kset(bm_ctx* ctx, int32_t k, const int32_t* d_sets, int64_t 
     a.all = d_all;
     a.status = d_status;
     int64_t blocks = nsets < (int64_t)ctx->num_sms * 8 ? nsets : (int64_t)ctx->num_sms * 8;
-    kset_kernel<<<(unsigned)blocks, kKThreads, 0, ctx->stream>>>(a);
+    kset_kernel<<<(unsigned)blocks, kKThreads, sizeof(uint32_t) * kKsetRowCap, ctx->stream>>>(a);
     BM_LAUNCH_CHECK(ctx, "kset_kernel");
     return BM_OK;
 }

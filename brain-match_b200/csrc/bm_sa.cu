@@ -89,22 +89,6 @@ constexpr int kSaUnitTable = 4096;  // items per iteration with an item -> list 
 constexpr size_t kSaRowBytes = sizeof(uint32_t) * kSaRowCap * 2 * (kSaThreads / 32);  // two buffers per warp
 static_assert(kSaRowBytes >= sizeof(uint32_t) * 4 * 4096, "the swap apply stages four rows in the row buffers");
 
-// Weight of entry id `key` in a staged B row (sorted by id, zero padding
-// last), 0 if absent.
-__device__ __forceinline__ int32_t row_weight(const uint32_t* row, int32_t len, int32_t key) {
-    int32_t l = 0, h = len;
-    while (l < h) {
-        const int32_t mid = (l + h) >> 1;
-        const uint32_t e = row[mid];
-        if (e != 0u && bm_eid(e) < key) l = mid + 1; else h = mid;
-    }
-    if (l < len) {
-        const uint32_t e = row[l];
-        if (e != 0u && bm_eid(e) == key) return bm_ew(e);
-    }
-    return 0;
-}
-
 constexpr int kSaApplyRowCap = 4096;  // entries per staged row in the swap apply (4 rows)
 
 // Apply the swap pi(a) <-> pi(b) of one chain with the whole CTA: S updates of
@@ -136,13 +120,13 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
         const bool a = g == fa;
         const int32_t len = a ? rlen[0] : rlen[1];
         const bool st = a ? rst[0] : rst[1];
-        return st ? row_weight(stage + (a ? 0 : kSaApplyRowCap), len, h) : bm_hash_get(P.hb, g, h);
+        return st ? bm_row_weight(stage + (a ? 0 : kSaApplyRowCap), len, h) : bm_hash_get(P.hb, g, h);
     };
     auto bin = [&](int32_t h, int32_t g) -> int32_t {
         const bool a = g == fa;
         const int32_t len = a ? rlen[2] : rlen[3];
         const bool st = a ? rst[2] : rst[3];
-        return st ? row_weight(stage + (a ? 2 : 3) * kSaApplyRowCap, len, h) : bm_hash_get(P.hb, h, g);
+        return st ? bm_row_weight(stage + (a ? 2 : 3) * kSaApplyRowCap, len, h) : bm_hash_get(P.hb, h, g);
     };
     for (int side = 0; side < 2; side++) {
         const int32_t me = side ? sb : sa, other = side ? sa : sb;
