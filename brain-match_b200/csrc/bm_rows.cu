@@ -394,9 +394,10 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                     }
                     it = lo;
                 }
-                cap = it_cap[it];
                 const int32_t s0 = (unit - it_upre[it]) * kSeg;
                 const int32_t nq = (min(it_len[it], s0 + kSeg) - s0) >> 2;
+                // the weight cap, with the unit's count of 32-quad rows above bit 16
+                cap = it_cap[it] | (((nq + 31) >> 5) << 16);
                 const uint4* b4 = reinterpret_cast<const uint4*>(it_base[it] + s0);
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) {
@@ -414,12 +415,14 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             while (ua < uhi) {
                 const int32_t ub = grab();
                 if (ub < uhi) load_unit(ub, qb, capb);
+                const int32_t cw = capa & 0xFFFF;
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) {
+                    if (t > 0 && (capa >> 16) <= t) break;  // warp-uniform: rows past the unit's end
                     const uint32_t e4[4] = {qa[t].x, qa[t].y, qa[t].z, qa[t].w};
 #pragma unroll
                     for (int c = 0; c < 4; c++)
-                        atomicAdd(acc + bm_eid(e4[c]), imin(capa, bm_ew(e4[c])));
+                        atomicAdd(acc + bm_eid(e4[c]), imin(cw, bm_ew(e4[c])));
                 }
 #pragma unroll
                 for (int t = 0; t < kSeg / 128; t++) qa[t] = qb[t];
