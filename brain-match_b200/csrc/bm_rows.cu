@@ -408,6 +408,19 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                     q[t] = (qi < nq) ? __ldg(b4 + qi) : make_uint4(sink, sink, sink, sink);
                 }
             };
+            auto scatter = [&](const uint4 (&q)[kSeg / 128], int32_t cap) {
+                const int32_t cw = cap & 0xFFFF;
+#pragma unroll
+                for (int t = 0; t < kSeg / 128; t++) {
+                    if (t > 0 && (cap >> 16) <= t) break;  // warp-uniform: rows past the unit's end
+                    const uint32_t e4[4] = {q[t].x, q[t].y, q[t].z, q[t].w};
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        atomicAdd(acc + bm_eid(e4[c]), imin(cw, bm_ew(e4[c])));
+                }
+            };
+            // two buffers alternate roles: the next unit's loads are issued
+            // before the current unit's atomics
             uint4 qa[kSeg / 128], qb[kSeg / 128];
             int32_t capa = 0, capb = 0;
             int32_t ua = grab();
@@ -415,19 +428,11 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             while (ua < uhi) {
                 const int32_t ub = grab();
                 if (ub < uhi) load_unit(ub, qb, capb);
-                const int32_t cw = capa & 0xFFFF;
-#pragma unroll
-                for (int t = 0; t < kSeg / 128; t++) {
-                    if (t > 0 && (capa >> 16) <= t) break;  // warp-uniform: rows past the unit's end
-                    const uint32_t e4[4] = {qa[t].x, qa[t].y, qa[t].z, qa[t].w};
-#pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        atomicAdd(acc + bm_eid(e4[c]), imin(cw, bm_ew(e4[c])));
-                }
-#pragma unroll
-                for (int t = 0; t < kSeg / 128; t++) qa[t] = qb[t];
-                capa = capb;
-                ua = ub;
+                scatter(qa, capa);
+                if (ub >= uhi) break;
+                ua = grab();
+                if (ua < uhi) load_unit(ua, qa, capa);
+                scatter(qb, capb);
             }
             if (c0 + kItemChunk < Fs) cluster.sync(); else __syncthreads();
         }
