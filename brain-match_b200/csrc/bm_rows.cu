@@ -377,11 +377,6 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             // padded to multiples of 4 entries and start 16-byte aligned).  The
             // loop is software-pipelined: the next unit's loads are issued
             // before the current unit's shared-memory atomics.
-            auto grab = [&]() -> int32_t {
-                int32_t k = 0;
-                if (lane == 0) asm volatile("atom.shared::cluster.add.u32 %0, [%1], 1;" : "=r"(k) : "r"(gctr));
-                return __shfl_sync(0xffffffffu, k, 0);
-            };
             auto load_unit = [&](int32_t unit, uint4 (&q)[kSeg / 128], int32_t& cap) {
                 int32_t it;
                 if (table) {
@@ -421,18 +416,35 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             };
             // two buffers alternate roles: the next unit's loads are issued
             // before the current unit's atomics
+            // claiming a unit is issued (lane 0's atomic) before the current
+            // unit's scatter and read (the broadcast) after it, so the
+            // atomic's round trip overlaps the scatter
+            auto claim = [&]() -> int32_t {
+                int32_t k = 0;
+                if (lane == 0) asm volatile("atom.shared::cluster.add.u32 %0, [%1], 1;" : "=r"(k) : "r"(gctr));
+                return k;
+            };
+            auto claimed = [&](int32_t k) -> int32_t { return __shfl_sync(0xffffffffu, k, 0); };
             uint4 qa[kSeg / 128], qb[kSeg / 128];
             int32_t capa = 0, capb = 0;
-            int32_t ua = grab();
-            if (ua < uhi) load_unit(ua, qa, capa);
-            while (ua < uhi) {
-                const int32_t ub = grab();
-                if (ub < uhi) load_unit(ub, qb, capb);
-                scatter(qa, capa);
-                if (ub >= uhi) break;
-                ua = grab();
-                if (ua < uhi) load_unit(ua, qa, capa);
-                scatter(qb, capb);
+            int32_t ua = claimed(claim());
+            if (ua < uhi) {
+                load_unit(ua, qa, capa);
+                int32_t nxt = claimed(claim());  // qa holds a unit; nxt is the next to load
+                for (;;) {
+                    const bool hb = nxt < uhi;
+                    if (hb) load_unit(nxt, qb, capb);
+                    const int32_t kb = hb ? claim() : 0;
+                    scatter(qa, capa);
+                    if (!hb) break;
+                    const int32_t nn = claimed(kb);
+                    const bool ha = nn < uhi;
+                    if (ha) load_unit(nn, qa, capa);
+                    const int32_t ka = ha ? claim() : 0;
+                    scatter(qb, capb);
+                    if (!ha) break;
+                    nxt = claimed(ka);
+                }
             }
             if (c0 + kItemChunk < Fs) cluster.sync(); else __syncthreads();
         }
