@@ -194,6 +194,22 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
         int4* acc4 = reinterpret_cast<int4*>(acc);
         for (int32_t i = tid; i < (nv >> 2); i += THREADS) acc4[i] = make_int4(0, 0, 0, 0);
     }
+    {
+        // the per-vertex arrays every row reads at random (pi, the four CSR
+        // pointer arrays, S(v)) are prefetched into L2 once per launch, one
+        // 128-byte line per thread spread over the grid, so the dependent
+        // loads of the first-hop staging and the finalise pass hit L2
+        const int32_t lines = (int32_t)((sizeof(int32_t) * ((size_t)nv + 4) + 127) / 128);
+        const int32_t total = 6 * lines;
+        for (int32_t j = tid * (int32_t)gridDim.x + (int32_t)blockIdx.x; j < total; j += THREADS * (int32_t)gridDim.x) {
+            const int32_t k = j / lines, l = j - k * lines;
+            const int32_t* arr = k == 0 ? a.pi : k == 1 ? a.ov : k == 2 ? a.Aout_ptr : k == 3 ? a.Ain_ptr
+                               : k == 4 ? a.Bout_ptr : a.Bin_ptr;
+            const int32_t lim = (k == 0) ? n + 1 : (k == 1) ? nv : n + 2;  // int32 elements of the array
+            const int32_t e = l * 32;
+            if (e < lim) asm volatile("prefetch.global.L2 [%0];" :: "l"(arr + e));
+        }
+    }
     // Units are shared out across the whole cluster from counters in CTA 0's
     // shared memory (one per chunk parity), so a CTA that shares its SM or
     // also runs the corrections simply takes fewer units.
