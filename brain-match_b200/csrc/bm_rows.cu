@@ -55,6 +55,7 @@ namespace {
 constexpr int kItemChunk = 1024;  // first-hop items staged per pass
 constexpr int kSeg = 512;         // second-hop entries per work unit
 constexpr int kMaxCluster = 8;
+constexpr int kFinBatch = 2;     // groups of four columns a thread finalises per pass
 constexpr int kSideCap = 4096;    // A entries of u whose corrections go through shared memory
 constexpr int kMaxUnits = 4096;   // units per chunk with a unit -> item table (else binary search)
 constexpr int kItemCost = 32;     // work estimate: entries charged per first-hop item
@@ -518,18 +519,7 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             a.colout[(size_t)r * (size_t)a.ncols + j] = (int32_t)c;
         }
     }
-    for (int32_t gi = glo + tid; fin && gi < ghi && !a.cols; gi += THREADS) {
-        int4 s4;
-        if (sc > 1) {
-            s4 = make_int4(0, 0, 0, 0);
-            const int4* base = a.spart + (size_t)(slot - sj) * (size_t)groups + gi;
-            for (int q = 0; q < sc; q++) {
-                const int4 t4 = __ldcg(base + (size_t)q * (size_t)groups);
-                s4.x += t4.x; s4.y += t4.y; s4.z += t4.z; s4.w += t4.w;
-            }
-        } else {
-            s4 = cluster_sum(gi);
-        }
+    auto finish_group = [&](int32_t gi, const int4 s4) {
         const int4 o4 = __ldg(ov4 + gi);
         const int32_t sv[4] = {s4.x, s4.y, s4.z, s4.w};
         const int32_t ovv[4] = {o4.x, o4.y, o4.z, o4.w};
@@ -556,6 +546,48 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             if (a.tab && valid) {
                 a.tab[(size_t)u * (size_t)a.tab_ld + (size_t)v] = (int32_t)d;
                 if (a.tab_sym && v >= 1 && v != u) a.tab[(size_t)v * (size_t)a.tab_ld + (size_t)u] = (int32_t)d;
+            }
+        }
+    };
+    if (fin && !a.cols) {
+        if (sc > 1) {
+            for (int32_t gi = glo + tid; gi < ghi; gi += THREADS) {
+                int4 s4 = make_int4(0, 0, 0, 0);
+                const int4* base = a.spart + (size_t)(slot - sj) * (size_t)groups + gi;
+                for (int q = 0; q < sc; q++) {
+                    const int4 t4 = __ldcg(base + (size_t)q * (size_t)groups);
+                    s4.x += t4.x; s4.y += t4.y; s4.z += t4.z; s4.w += t4.w;
+                }
+                finish_group(gi, s4);
+            }
+        } else {
+            // a thread's groups (kFinBatch per pass) are read from the other
+            // CTAs' accumulators together, so the remote loads overlap
+            for (int32_t g0 = glo + tid; g0 < ghi; g0 += kFinBatch * THREADS) {
+                int4 sb[kFinBatch];
+#pragma unroll
+                for (int b = 0; b < kFinBatch; b++) {
+                    const int32_t gi = g0 + b * THREADS;
+                    sb[b] = gi < ghi ? reinterpret_cast<const int4*>(acc)[gi] : make_int4(0, 0, 0, 0);
+                }
+#pragma unroll
+                for (int q = 1; q < kMaxCluster; q++) {
+                    if (q >= CL) break;
+                    const int rk = crank + q < CL ? crank + q : crank + q - CL;  // (crank + q) mod CL
+#pragma unroll
+                    for (int b = 0; b < kFinBatch; b++) {
+                        const int32_t gi = g0 + b * THREADS;
+                        if (gi < ghi) {
+                            const int4 t4 = *reinterpret_cast<const int4*>(cluster.map_shared_rank(acc + 4 * gi, rk));
+                            sb[b].x += t4.x; sb[b].y += t4.y; sb[b].z += t4.z; sb[b].w += t4.w;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < kFinBatch; b++) {
+                    const int32_t gi = g0 + b * THREADS;
+                    if (gi < ghi) finish_group(gi, sb[b]);
+                }
             }
         }
     }
