@@ -397,6 +397,20 @@ extern "C" bm_status bm_set_row_tiling(bm_ctx* ctx, int32_t ctas_per_row, int32_
     return BM_OK;
 }
 
+extern "C" bm_status bm_set_semantics(bm_ctx* ctx, int32_t mode) {
+    if (!ctx) return BM_INVALID_ARG;
+    if (mode != BM_SEMANTICS_EXACT && mode != BM_SEMANTICS_REF_CPU)
+        return bm_fail(ctx, BM_INVALID_ARG, "semantics must be BM_SEMANTICS_EXACT (0) or BM_SEMANTICS_REF_CPU (1)");
+    ctx->semantics = mode;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_get_semantics(bm_ctx* ctx, int32_t* mode) {
+    if (!ctx || !mode) return BM_INVALID_ARG;
+    *mode = ctx->semantics;
+    return BM_OK;
+}
+
 extern "C" bm_status bm_set_row_split(bm_ctx* ctx, int32_t slots) {
     if (!ctx) return BM_INVALID_ARG;
     if (slots < -1) return bm_fail(ctx, BM_INVALID_ARG, "slots must be -1 (off), 0 (automatic) or a slot count");

@@ -94,6 +94,7 @@ struct bm_ctx {
     // split rows (bm_rows.cu): per-row work estimate, slot partial sums,
     // self-resetting arrival counters and slice reductions
     int32_t row_split = 0;          // 0 = automatic slots, -1 = off, k > 0 = k slots
+    int32_t semantics = 0;          // BM_SEMANTICS_EXACT or BM_SEMANTICS_REF_CPU (pairwise swap deltas)
     int32_t* rwork = nullptr;
     std::vector<int32_t> h_rwork;   // host copy (the split plan is made on the host)
     int4* slots = nullptr;          // slot table of a split launch (device)
@@ -241,8 +242,13 @@ __device__ __forceinline__ int32_t imin(int32_t a, int32_t b) { return a < b ? a
 
 // Kernel launchers implemented across the .cu files.
 bm_status bm_launch_score(bm_ctx* ctx, int64_t* score_out);
+// Recompute the score and hold the tracked score (the sum of accepted
+// deltas) against it; the recomputed score is kept either way.
+bm_status bm_check_score(bm_ctx* ctx);
 bm_status bm_launch_relabel(bm_ctx* ctx);
-bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_out);
+// exact_only: score differences whatever the context's delta semantics (for
+// callers that apply swaps regardless of their deltas and track the score)
+bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_out, bool exact_only = false);
 // Allocate the split-row buffers for the current n and refresh the per-row
 // work estimate (after the mapping is set); refresh alone after many swaps.
 bm_status bm_rows_prepare(bm_ctx* ctx);

@@ -5,7 +5,7 @@
 // kernel) and only improving, independent swaps are applied.  The model has
 // no counterpart in the reference, whose only guided proposal is the
 // degree-weighted random swap of src/graph-re-alignment-gpu-swap.cu:767-887;
-// uniform random partners stay available as the judge of its hit rate.
+// uniform random partners stay available as the yardstick of its hit rate.
 //
 // Numerics: inputs, weights and hidden activations are rounded to BF16;
 // products accumulate in FP32 (SIMT FMA for training, tcgen05 MMA with TMEM
@@ -1795,15 +1795,8 @@ extern "C" bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* M, const int32_t* ro
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     prog->next_row_pos = pos;
     prog->seconds += secs_since(t0);
-    int64_t full = 0;
-    if ((s = bm_launch_score(ctx, &full)) != BM_OK) return s;
-    if (full != ctx->score) {
-        const int64_t tracked = ctx->score;
-        ctx->score = full;
-        prog->score = full;
-        return bm_fail(ctx, BM_PARITY_FAIL, "tracked score %lld != recomputed score %lld", (long long)tracked,
-                       (long long)full);
-    }
+    s = bm_check_score(ctx);
     prog->score = ctx->score;
+    if (s != BM_OK) return s;
     return ret;
 }

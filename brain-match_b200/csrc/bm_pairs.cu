@@ -10,6 +10,14 @@
 //                + sum over A entries between u and v of [min(w, B(f_u,f_v)) + min(w, B(f_v,f_u))]
 //                + self-loop terms.
 //
+// Self-loop terms, with s_x the A self-loop weight of x, b_x = B(f_x, f_x),
+// p = B(f_u, f_v), q = B(f_v, f_u): exact semantics
+//   min(s_u, b_v) - min(s_u, b_u) + min(s_v, b_u) - min(s_v, b_v);
+// reference-delta semantics (what calculate_swap_delta returns: its out- and
+// in-edge loops, :327-388, each meet the self-loop of a swapped vertex and
+// compare the image after the swap, p or q, with the old image's b_x)
+//   min(s_u, p) + min(s_u, q) + min(s_v, p) + min(s_v, q) - 2 min(s_u, b_u) - 2 min(s_v, b_v).
+//
 // The last sum repairs the direct edges u->v and v->u that S(u) and S(v) both
 // counted (the reference handles them at :390-405).  One warp per pair; every
 // lookup of B is one probe sequence in the hash table (L2-resident).
@@ -26,7 +34,8 @@ struct PairArgs {
     const int32_t* pi;
     const int32_t* ov;
     int32_t n;
-    int has_self;
+    int has_self;  // self-loop terms needed (A and B have self-loops; A alone in reference-delta mode)
+    int refcpu;    // reference-delta semantics
 };
 
 __device__ __forceinline__ int64_t pair_delta_warp(const PairArgs& a, int32_t u, int32_t v, int lane) {
@@ -75,7 +84,12 @@ __device__ __forceinline__ int64_t pair_delta_warp(const PairArgs& a, int32_t u,
     if (a.has_self) {
         const int32_t su = __ldg(a.A.self_w + u), sv = __ldg(a.A.self_w + v);
         const int32_t bu = __ldg(a.selfB + fu), bv = __ldg(a.selfB + fv);
-        s += imin(su, bv) - imin(su, bu) + imin(sv, bu) - imin(sv, bv);
+        if (a.refcpu) {
+            const int32_t p = bm_hash_get(a.hb, fu, fv), q = bm_hash_get(a.hb, fv, fu);
+            s += imin(su, p) + imin(su, q) + imin(sv, p) + imin(sv, q) - 2 * imin(su, bu) - 2 * imin(sv, bv);
+        } else {
+            s += imin(su, bv) - imin(su, bu) + imin(sv, bu) - imin(sv, bv);
+        }
     }
     return s;
 }
@@ -95,7 +109,7 @@ pairs_kernel(PairArgs a, const int32_t* __restrict__ pairs, int64_t k, int64_t* 
 
 }  // namespace
 
-bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_out) {
+bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_t* d_out, bool exact_only) {
     if (k <= 0) return BM_OK;
     PairArgs a;
     a.A = gview(ctx->g[0]);
@@ -104,7 +118,8 @@ bm_status bm_launch_pairs(bm_ctx* ctx, const int32_t* d_pairs, int64_t k, int64_
     a.pi = ctx->pi;
     a.ov = ctx->ov;
     a.n = ctx->n;
-    a.has_self = ctx->g[0].has_self && ctx->g[1].has_self;
+    a.refcpu = !exact_only && ctx->semantics == BM_SEMANTICS_REF_CPU;
+    a.has_self = a.refcpu ? ctx->g[0].has_self : (ctx->g[0].has_self && ctx->g[1].has_self);
     int64_t blocks = (k + (kPairThreads / 32) - 1) / (kPairThreads / 32);
     int64_t cap = (int64_t)ctx->num_sms * 16;
     if (blocks > cap) blocks = cap;

@@ -80,7 +80,8 @@ struct RowArgs {
     const uint32_t* Bin_ent;
     const int32_t* selfA;
     const int32_t* selfB;
-    int has_self;
+    int has_self;  // self-loop terms needed (A and B have self-loops; A alone in reference-delta mode)
+    int refcpu;    // reference-delta semantics (selects the REFCPU instantiation)
     HashView hb;
     const int32_t* pi;
     const int32_t* ov;
@@ -154,7 +155,9 @@ __device__ __forceinline__ bm_row_result row_result(int32_t u, const Partial& t)
     return out;
 }
 
-template <int THREADS>
+// REFCPU: reference-delta semantics (a separate instantiation, so the exact
+// one carries none of its code or registers)
+template <int THREADS, bool REFCPU>
 __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     constexpr int NW = THREADS / 32;
     constexpr int IPT = kItemChunk / THREADS;  // items built per thread
@@ -466,6 +469,26 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             if (c0 + kItemChunk < Fs) cluster.sync(); else __syncthreads();
         }
     }
+    if (REFCPU && valid && crank == 0 && P(1) == 0) {
+        // reference-delta semantics: calculate_swap_delta meets the self-loop
+        // of u and of the partner v in its out- and in-edge loops
+        // (src/graph-alignment-optimized.c:327-388) and compares the images
+        // after the swap, B(pi u, pi v) and B(pi v, pi u).  Those are the
+        // entries of B's row and column at pi u, so each adds
+        // min(s_u, b) + min(s_v, b) at its v; the old-image terms are added
+        // per column in the finalise pass.
+        const int32_t fu = __ldg(a.pi + u), su = __ldg(a.selfA + u);
+        const int32_t bo = __ldg(a.Bout_ptr + fu), d3 = __ldg(a.Bout_ptr + fu + 1) - bo;
+        const int32_t bi = __ldg(a.Bin_ptr + fu), d4 = __ldg(a.Bin_ptr + fu + 1) - bi;
+        for (int32_t j = tid; j < d3 + d4; j += THREADS) {
+            const uint32_t e = (j < d3) ? __ldg(a.Bout_ent + bo + j) : __ldg(a.Bin_ent + bi + (j - d3));
+            if (e) {
+                const int32_t v = bm_eid(e), b = bm_ew(e);
+                const int32_t c = imin(su, b) + imin(__ldg(a.selfA + v), b);
+                if (c) atomicAdd(acc + v, c);
+            }
+        }
+    }
     cluster.sync();
 
     // ---- finalise this CTA's slice of v, four consecutive v per thread
@@ -532,7 +555,10 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 d = (long long)sv[c] - ovu - (long long)ovv[c];
                 if (a.has_self) {
                     const int32_t sAv = __ldg(a.selfA + v), sBv = __ldg(a.selfB + __ldg(a.pi + v));
-                    d += imin(sAu, sBv) - imin(sAu, sBu) + imin(sAv, sBu) - imin(sAv, sBv);
+                    if constexpr (REFCPU)
+                        d += -2 * imin(sAu, sBu) - 2 * imin(sAv, sBv);
+                    else
+                        d += imin(sAu, sBv) - imin(sAu, sBu) + imin(sAv, sBu) - imin(sAv, sBv);
                 }
                 if (v >= collo) {
                     if (d > 0) {
@@ -673,10 +699,10 @@ __global__ void __launch_bounds__(kWorkThreads) row_work_kernel(RowArgs a, int32
     if (lane == 0) work[u] = (int32_t)min(s, (long long)INT_MAX);
 }
 
-template <int THREADS>
+template <int THREADS, bool REFCPU>
 bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem) {
     static bool configured[64] = {false};
-    auto kern = rows_kernel<THREADS>;
+    auto kern = rows_kernel<THREADS, REFCPU>;
     if (!configured[ctx->device & 63]) {
         BM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_optin));
         configured[ctx->device & 63] = true;
@@ -700,7 +726,7 @@ bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem) {
 
 template <int THREADS>
 bm_status max_clusters_t(bm_ctx* ctx, int cl, size_t smem, int* out) {
-    auto kern = rows_kernel<THREADS>;
+    auto kern = rows_kernel<THREADS, false>;
     BM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_optin));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(cl * 64), 1, 1);
@@ -859,7 +885,9 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
     args.Bin_ent = B.in_ent;
     args.selfA = A.self_w;
     args.selfB = B.self_w;
-    args.has_self = A.has_self && B.has_self;
+    // one-sided gains (d_cols) are not swaps: they keep the exact rule
+    args.refcpu = (ctx->semantics == BM_SEMANTICS_REF_CPU && !d_cols) ? 1 : 0;
+    args.has_self = args.refcpu ? A.has_self : (A.has_self && B.has_self);
     args.hb = hview(B);
     args.pi = ctx->pi;
     args.ov = ctx->ov;
@@ -933,7 +961,12 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
         ar.full = d_full ? d_full + (size_t)r0 * ((size_t)ctx->n + 1) : nullptr;
         ar.res = d_res ? d_res + r0 : nullptr;
         ar.colout = d_colout ? d_colout + (size_t)r0 * (size_t)ncols : nullptr;
-        st = (ctx->row_threads == 256) ? launch_rows_t<256>(ctx, ar, cl, smem) : launch_rows_t<512>(ctx, ar, cl, smem);
+        if (ar.refcpu)
+            st = (ctx->row_threads == 256) ? launch_rows_t<256, true>(ctx, ar, cl, smem)
+                                           : launch_rows_t<512, true>(ctx, ar, cl, smem);
+        else
+            st = (ctx->row_threads == 256) ? launch_rows_t<256, false>(ctx, ar, cl, smem)
+                                           : launch_rows_t<512, false>(ctx, ar, cl, smem);
         if (st != BM_OK) return st;
     }
     return BM_OK;

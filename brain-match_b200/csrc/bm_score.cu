@@ -75,6 +75,24 @@ bm_status bm_launch_score(bm_ctx* ctx, int64_t* score_out) {
     return BM_OK;
 }
 
+// Exact semantics: the tracked score must equal the recomputed one, and a
+// mismatch is a failed self-check.  Reference-delta semantics: the tracked
+// score sums calculate_swap_delta values, which are not score differences on
+// graphs with self-loops, so the recomputed score replaces it, as the
+// reference's loop re-scores after every accept
+// (src/graph-alignment-optimized.c:571-576).
+bm_status bm_check_score(bm_ctx* ctx) {
+    int64_t full = 0;
+    bm_status s = bm_launch_score(ctx, &full);
+    if (s != BM_OK) return s;
+    const int64_t tracked = ctx->score;
+    ctx->score = full;
+    if (full != tracked && ctx->semantics == BM_SEMANTICS_EXACT)
+        return bm_fail(ctx, BM_PARITY_FAIL, "tracked score %lld != recomputed score %lld", (long long)tracked,
+                       (long long)full);
+    return BM_OK;
+}
+
 bm_status bm_launch_relabel(bm_ctx* ctx) {
     const DevGraph& B = ctx->g[1];
     int blocks = ctx->num_sms * 4;

@@ -564,15 +564,8 @@ extern "C" bm_status bm_search_table(bm_ctx* ctx, int32_t* d_table, int64_t ld, 
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     prog->seconds += std::chrono::duration<double>(clk::now() - t0).count();
     prog->sweeps += rounds;
-    int64_t full = 0;
-    if ((s = bm_launch_score(ctx, &full)) != BM_OK) return s;
-    if (full != ctx->score) {
-        const int64_t tracked = ctx->score;
-        ctx->score = full;
-        prog->score = full;
-        return bm_fail(ctx, BM_PARITY_FAIL, "tracked score %lld != recomputed score %lld", (long long)tracked,
-                       (long long)full);
-    }
+    s = bm_check_score(ctx);
     prog->score = ctx->score;
+    if (s != BM_OK) return s;
     return ret;
 }

@@ -23,6 +23,11 @@
  *   --save-interval S      seconds between checkpoints (default 60)
  *   --rows-per-batch R     rows per launch in search mode (default 2 x SMs)
  *   --device D             CUDA device ordinal (default 0)
+ *   --semantics exact|ref-cpu   swap deltas as score differences (default),
+ *                          or as calculate_swap_delta computes them
+ *                          (:321-408), which differ on graphs with
+ *                          self-loops; ref-cpu with --mode parity makes the
+ *                          reference loop's accepts on such graphs
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -72,12 +77,14 @@ int main(int argc, char** argv) {
     if (argc < 7) {
         LOG_ERROR("Usage: %s <male graph> <female graph> <male ordering> <female ordering> <in mapping> <out mapping> "
                   "[--mode parity|search] [--schedule natural|ordering] [--time-budget S] [--max-accepts K] "
-                  "[--max-sweeps K] [--save-interval S] [--rows-per-batch R] [--device D]",
+                  "[--max-sweeps K] [--save-interval S] [--rows-per-batch R] [--device D] "
+                  "[--semantics exact|ref-cpu]",
                   argv[0]);
         return 1;
     }
     const char* mode = "parity";
     const char* schedule = "natural";
+    const char* semantics = "exact";
     double budget = 0, save_interval = 60;
     long long max_accepts = -1;
     int max_sweeps = -1, device = 0, rows_per_batch = 0;
@@ -93,12 +100,17 @@ int main(int argc, char** argv) {
         else if (!strcmp(a, "--save-interval")) save_interval = atof(v);
         else if (!strcmp(a, "--rows-per-batch")) rows_per_batch = atoi(v);
         else if (!strcmp(a, "--device")) device = atoi(v);
+        else if (!strcmp(a, "--semantics")) semantics = v;
         else { LOG_ERROR("unknown option %s", a); return 1; }
         i++;
     }
     if (strcmp(mode, "parity") && strcmp(mode, "search")) { LOG_ERROR("--mode must be parity or search"); return 1; }
     if (strcmp(schedule, "natural") && strcmp(schedule, "ordering")) {
         LOG_ERROR("--schedule must be natural or ordering");
+        return 1;
+    }
+    if (strcmp(semantics, "exact") && strcmp(semantics, "ref-cpu")) {
+        LOG_ERROR("--semantics must be exact or ref-cpu");
         return 1;
     }
     double t_start = now_s();
@@ -146,7 +158,8 @@ int main(int argc, char** argv) {
     if (st != BM_OK) { LOG_ERROR("bm_ctx_create(%d): %s", device, bm_status_str(st)); return 1; }
     if ((st = bm_set_graph(ctx, BM_SIDE_A, n, gm.m, gm.src, gm.dst, gm.w)) != BM_OK ||
         (st = bm_set_graph(ctx, BM_SIDE_B, n, gf.m, gf.src, gf.dst, gf.w)) != BM_OK ||
-        (st = bm_set_mapping(ctx, pi)) != BM_OK) {
+        (st = bm_set_mapping(ctx, pi)) != BM_OK ||
+        (st = bm_set_semantics(ctx, strcmp(semantics, "ref-cpu") ? BM_SEMANTICS_EXACT : BM_SEMANTICS_REF_CPU)) != BM_OK) {
         LOG_ERROR("%s: %s", bm_status_str(st), bm_ctx_last_error(ctx));
         bm_ctx_destroy(ctx);
         return 1;

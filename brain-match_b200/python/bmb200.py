@@ -151,6 +151,8 @@ def cuda_lib() -> C.CDLL:
             "bm_rows_max_active_clusters": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
             "bm_set_row_tiling": (C.c_int, [vp, C.c_int32, C.c_int32]),
             "bm_set_row_split": (C.c_int, [vp, C.c_int32]),
+            "bm_set_semantics": (C.c_int, [vp, C.c_int32]),
+            "bm_get_semantics": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "bm_get_row_split": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "bm_kset_eval": (C.c_int, [vp, C.c_int32, vp, C.c_int64, vp, vp, vp]),
             "bm_kset_eval_dev": (C.c_int, [vp, C.c_int32, vp, C.c_int64, vp, vp, vp]),
@@ -650,6 +652,20 @@ class Engine:
         v = C.c_int32()
         self._chk(self.L.bm_get_row_split(self.h, C.byref(v)), "bm_get_row_split")
         return v.value
+
+    SEMANTICS = {"exact": 0, "ref-cpu": 1}
+
+    def set_semantics(self, mode: str = "exact") -> None:
+        """Pairwise swap deltas as score differences ("exact") or as the
+        reference's calculate_swap_delta computes them ("ref-cpu")."""
+        if mode not in self.SEMANTICS:
+            raise ValueError(f"semantics must be one of {sorted(self.SEMANTICS)}")
+        self._chk(self.L.bm_set_semantics(self.h, self.SEMANTICS[mode]), "bm_set_semantics")
+
+    def semantics(self) -> str:
+        v = C.c_int32()
+        self._chk(self.L.bm_get_semantics(self.h, C.byref(v)), "bm_get_semantics")
+        return {i: k for k, i in self.SEMANTICS.items()}[v.value]
 
     def launch_count(self) -> int:
         return int(self.L.bm_launch_count(self.h))

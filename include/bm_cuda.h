@@ -19,7 +19,9 @@
  * (duplicate A edges count once per entry), B is a matrix (the last duplicate
  * weight wins, src/graph-alignment-optimized.c:185).  Self-loops are scored
  * exactly; on graphs without self-loops this equals calculate_swap_delta
- * (src/graph-alignment-optimized.c:321-408) for every pair.
+ * (src/graph-alignment-optimized.c:321-408) for every pair.  The optional
+ * reference-delta mode (bm_set_semantics) reproduces calculate_swap_delta
+ * itself on graphs with self-loops.
  *
  * Limits: n <= 131071, 0 <= w <= 32767 (the reference stores B weights as
  * int16), fewer than 2^31 edges per graph, at most one self-loop per A vertex.
@@ -443,7 +445,7 @@ typedef struct bm_learned_params {
     int32_t topk;             /* partners proposed per row, 1..64 (0: 64) */
     int32_t rows_per_batch;   /* rows per launch (0: 2 x SMs) */
     int32_t refresh_batches;  /* feature table refreshed every this many batches (0: 1) */
-    int32_t uniform;          /* 1: uniform random partners instead of the model (the judge) */
+    int32_t uniform;          /* 1: uniform random partners instead of the model (the yardstick for the hit rate) */
     int32_t exact_fallback;   /* 1: after a pass with at most fallback_accepts accepts, an exact row pass
                                  runs; a pass of it without accepts ends the search (converged) */
     int32_t fallback_accepts; /* threshold of the above (0: only passes without accepts) */
@@ -492,6 +494,26 @@ bm_status bm_event_elapsed_ms(bm_ctx* ctx, void* ev_start, void* ev_stop, float*
 int64_t bm_launch_count(const bm_ctx* ctx);
 /* PCI bus id of the context's device ("0000:1b:00.0"), for NVML queries. */
 bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len);
+
+/* Delta semantics of pairwise swaps.  BM_SEMANTICS_EXACT (default): the
+ * score difference.  BM_SEMANTICS_REF_CPU: the value calculate_swap_delta
+ * (src/graph-alignment-optimized.c:321-408) returns, which differs from the
+ * score difference only when a swapped A vertex x has a self-loop of weight
+ * s: its out-edge loop (:327-340) and in-edge loop (:343-356) each meet the
+ * self-loop and compare min(s, B(f1, f2)) or min(s, B(f2, f1)) against
+ * min(s, B(f_x, f_x)) of the old image.  The mode applies to every pairwise
+ * swap delta (bm_delta_pairs, bm_delta_rows, bm_rows_best, the delta table
+ * and the schedules that accept swaps by them), so bm_sweep_parity makes the
+ * reference loop's accepts on such graphs; the score a schedule reports is
+ * re-computed at its end, as the reference re-scores after every accept
+ * (:571-576), instead of being checked against the sum of the deltas.
+ * Permutation sets, 3-rotations, annealing chains and one-sided gains stay
+ * exact.  Duplicate A edges between the two swapped vertices still count once
+ * per list entry (the reference counts the matrix's last weight once). */
+#define BM_SEMANTICS_EXACT 0
+#define BM_SEMANTICS_REF_CPU 1
+bm_status bm_set_semantics(bm_ctx* ctx, int32_t mode);
+bm_status bm_get_semantics(bm_ctx* ctx, int32_t* mode);
 
 /* Tuning knobs of the row kernel: CTAs per row (1..8: a thread-block cluster
  * sharing the row through distributed shared memory) and threads per CTA

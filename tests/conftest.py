@@ -42,6 +42,11 @@ def golden_selfloop():
     return load_golden("golden_selfloop.npz")
 
 
+@pytest.fixture(scope="session")
+def golden_selfloop_ref():
+    return load_golden("golden_selfloop_ref.npz")
+
+
 def make_engine(n, A, B, pi):
     """An engine holding graphs A, B (edge-array triples) and mapping pi."""
     import bmb200 as bm

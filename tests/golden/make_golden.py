@@ -99,12 +99,64 @@ def make_selfloop_case(name, seed=17, n=40, m=400):
     print(name, "scores", scores[:3])
 
 
+def make_selfloop_ref_case(name, seed=23, n=300, m=3000, loops=75):
+    """A pair with self-loops on a quarter of the vertices of each graph, no
+    duplicate edges and weights 1..8: the inputs where calculate_swap_delta
+    differs from the score difference (a self-loop of a swapped vertex counted
+    once as an out-edge and once as an in-edge, both against the old image).
+    Records the reference's pair deltas, whole-row deltas and its serial loop
+    with the re-score of every accept (optimize_mapping :571-576), so that the
+    engine's reference-delta mode can be pinned to the reference itself."""
+    rng = np.random.default_rng(seed)
+
+    def graph():
+        s = rng.integers(1, n + 1, m).astype(np.int32)
+        d = rng.integers(1, n + 1, m).astype(np.int32)
+        lv = rng.choice(np.arange(1, n + 1), loops, replace=False).astype(np.int32)
+        s, d = np.concatenate([s, lv]), np.concatenate([d, lv])
+        _, first = np.unique(s.astype(np.int64) * (n + 1) + d, return_index=True)
+        keep = np.sort(first)
+        return s[keep], d[keep], rng.integers(1, 9, keep.shape[0]).astype(np.int32)
+
+    A, B = graph(), graph()
+    ref = Reference(n, A, B)
+    init = np.concatenate([[0], rng.permutation(n) + 1]).astype(np.int32)
+    pairs = rng.integers(1, n + 1, size=(2000, 2)).astype(np.int32)
+    rows = rng.choice(np.arange(1, n + 1), size=4, replace=False).astype(np.int32)
+    out = {
+        "n": np.int64(n), "a_src": A[0], "a_dst": A[1], "a_w": A[2], "b_src": B[0], "b_dst": B[1], "b_w": B[2],
+        "pi_init": init, "score_init": np.int64(ref.score(init)),
+        "pairs": pairs, "pair_deltas": ref.pairs(init, pairs), "rows": rows, "row_deltas": ref.rows(init, rows),
+    }
+    # bounded: with these deltas a swap and its reverse can both look
+    # improving, so the loop need not converge
+    pi_f, score_f, log, sweeps, conv = ref.serial(init, max_sweeps=8, verify=True)
+    out.update({"serial_max_sweeps": np.int64(8), "serial_pi": pi_f, "serial_score": np.int64(score_f), "serial_accepts": np.int64(len(log)),
+                "serial_log": log, "serial_sweeps": np.int64(sweeps), "serial_converged": np.int64(conv)})
+    pi_k, score_k, _, _, _ = ref.serial(init, max_accepts=100, verify=True)
+    out.update({"serial100_pi": pi_k, "serial100_score": np.int64(score_k)})
+    ref.close()
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, {k: (v if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items() if k in
+                 ("n", "score_init", "serial_score", "serial_accepts", "serial_sweeps", "serial_converged")})
+
+
+CASES = {
+    "golden_small.npz": lambda: make_pair_case("golden_small.npz", 1, 11, 300, 3000, 3000, 6, max_sweeps=-1,
+                                               log_cap=1 << 16, verify=True),
+    "golden_cfg1.npz": lambda: make_pair_case("golden_cfg1.npz", 1, 1, 2000, 40000, 5000, 4, max_sweeps=1,
+                                              log_cap=3000, verify=False),
+    "golden_selfloop.npz": lambda: make_selfloop_case("golden_selfloop.npz"),
+    "golden_selfloop_ref.npz": lambda: make_selfloop_ref_case("golden_selfloop_ref.npz"),
+}
+
+
 def main():
+    """Make every fixture, or only those named on the command line."""
     if not ref_available():
         raise SystemExit("oracle/_ref/libref.so missing: run make -C oracle where the reference sources exist")
-    make_pair_case("golden_small.npz", 1, 11, 300, 3000, 3000, 6, max_sweeps=-1, log_cap=1 << 16, verify=True)
-    make_pair_case("golden_cfg1.npz", 1, 1, 2000, 40000, 5000, 4, max_sweeps=1, log_cap=3000, verify=False)
-    make_selfloop_case("golden_selfloop.npz")
+    for name in (sys.argv[1:] or list(CASES)):
+        CASES[name]()
 
 
 if __name__ == "__main__":

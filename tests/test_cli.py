@@ -27,6 +27,13 @@ def test_unknown_option_exits_1(tmp_path):
     assert r.returncode == 1
 
 
+def test_bad_semantics_exits_1(tmp_path):
+    r = run([os.path.join(bm.BIN_DIR, "bm-align")] + [str(tmp_path / f"x{i}.csv") for i in range(6)] +
+            ["--semantics", "approx"])
+    assert r.returncode == 1
+    assert "--semantics must be exact or ref-cpu" in r.stderr
+
+
 def test_bm_gen_writes_reference_formats(tmp_path):
     r = run([os.path.join(bm.BIN_DIR, "bm-gen"), "1", "5", str(tmp_path), "--n", "150", "--m", "1200"])
     assert r.returncode == 0, r.stderr

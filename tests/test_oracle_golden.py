@@ -56,6 +56,30 @@ def test_oracle_selfloop_scores(golden_selfloop):
         assert orc.delta(pi, u, v) == rd  # the reference's own (inexact here) delta, restated
 
 
+def test_oracle_selfloop_reference_deltas(golden_selfloop_ref):
+    """On a pair with self-loops (no duplicates) the restated
+    calculate_swap_delta equals the reference's own deltas, pairs, whole rows
+    and the accept sequence of the serial loop, although those deltas are not
+    score differences there."""
+    g = golden_selfloop_ref
+    n, A, B = golden_graphs(g)
+    orc = Oracle(n, A, B)
+    assert orc.score(g["pi_init"]) == int(g["score_init"])
+    deltas = orc.pairs(g["pi_init"], g["pairs"])
+    np.testing.assert_array_equal(deltas, g["pair_deltas"])
+    exact = np.array([orc.exact_delta(g["pi_init"], u, v) if u != v else 0 for u, v in g["pairs"]])
+    assert (exact != deltas).sum() > 100  # the fixture exercises the self-loop rule
+    np.testing.assert_array_equal(orc.rows(g["pi_init"], g["rows"]), g["row_deltas"])
+    pi, _, log, sweeps, conv = orc.serial(g["pi_init"], max_sweeps=int(g["serial_max_sweeps"]))
+    np.testing.assert_array_equal(log, g["serial_log"])
+    np.testing.assert_array_equal(pi, g["serial_pi"])
+    assert (sweeps, conv) == (int(g["serial_sweeps"]), int(g["serial_converged"]))
+    assert orc.score(pi) == int(g["serial_score"])  # the reference re-scores every accept
+    pi100, _, _, _, _ = orc.serial(g["pi_init"], max_accepts=100)
+    np.testing.assert_array_equal(pi100, g["serial100_pi"])
+    assert orc.score(pi100) == int(g["serial100_score"])
+
+
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built (reference sources absent)")
 def test_oracle_matches_live_reference():
     import bmb200 as bm
