@@ -95,7 +95,10 @@ bm_status bm_get_mapping(bm_ctx* ctx, int32_t* pi);
  * Replaces calculate_alignment_score (src/graph-alignment-optimized.c:292-307)
  * and score-matching's calculate_score_sparse (src/score-matching.c:558-597). */
 bm_status bm_score(bm_ctx* ctx, int64_t* score);
-/* Score tracked incrementally by the engine (sum of applied deltas). */
+/* Score tracked incrementally by the engine (sum of applied deltas).  In the
+ * reference-delta mode (bm_set_semantics) the deltas need not be score
+ * differences, so between a schedule's end-of-call re-score and the next
+ * one it may differ from bm_score. */
 bm_status bm_tracked_score(bm_ctx* ctx, int64_t* score);
 /* Per-vertex overlap S(v) = sum of min(w, w_B) over non-self A entries incident
  * to v (each edge counts at both ends), host array of n+1 int32. */
