@@ -22,7 +22,8 @@ initial matching), written in the reference's CSV formats.
     python oracle/ref_e2e.py [--seconds 600] [--threads 0] [--workdir DIR]
 
 The CSV files and the reference's output mapping go to DIR (default
-oracle/_ref/e2e, beside the binary).  Prints one JSON line.
+oracle/_ref/e2e, beside the binary) and are deleted at the end unless --keep
+is given.  Prints one JSON line.
 """
 from __future__ import annotations
 
@@ -96,6 +97,7 @@ def main():
     ap.add_argument("--seconds", type=float, default=600.0)
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--workdir", default=None)
+    ap.add_argument("--keep", action="store_true", help="keep the generated CSV files")
     args = ap.parse_args()
     if not os.path.exists(REF_BIN):
         raise SystemExit(f"{REF_BIN} missing: run make -C oracle where the reference sources exist")
@@ -107,6 +109,7 @@ def main():
     n = max(A.n, B.n)
     A.n = B.n = n
     init = bm.read_mapping(os.path.join(work, "init_mapping.csv"), n)[0]
+    init_score = bm.host_score(A, B, init)
     out_path = os.path.join(work, "ref_out_mapping.csv")
     if os.path.exists(out_path):
         os.remove(out_path)
@@ -153,11 +156,17 @@ def main():
                 os.killpg(proc.pid, signal.SIGKILL)
                 proc.wait()
     lines.join(timeout=5)
+    if not args.keep:
+        for name in ("gm.csv", "gf.csv", "gm_order.csv", "gf_order.csv", "init_mapping.csv", "truth_mapping.csv",
+                     "ref_out_mapping.csv"):
+            path = os.path.join(work, name)
+            if os.path.exists(path):
+                os.remove(path)
     print(json.dumps({
         "binary": "graph-alignment-optimized-parallel (unmodified reference)",
         "workload": "bm-gen config 2 seed 2 (n = 18,524, ~3M edges per graph, greedy initial matching)",
         "threads": threads, "cpu": cpu_model(), "seconds": args.seconds,
-        "initial_score_reference": lines.initial, "initial_score_host": bm.host_score(A, B, init),
+        "initial_score_reference": lines.initial, "initial_score_host": init_score,
         "s_to_optimisation_start": lines.t_opt,
         "saves_columns": ["s since start", "rows done", "score (host re-score of the saved mapping)"],
         "saves": saves,
