@@ -55,3 +55,7 @@ def test_null_context_is_rejected():
     assert L.bm_set_mapping(None, None) == bm.BM_INVALID_ARG
     assert L.bm_score(None, None) == bm.BM_INVALID_ARG
     assert L.bm_launch_count(None) == 0
+    m = C.c_int32(-1)
+    assert L.bm_set_semantics(None, 1) == bm.BM_INVALID_ARG
+    assert L.bm_get_semantics(None, C.byref(m)) == bm.BM_INVALID_ARG and m.value == -1
+    assert L.bm_set_row_split(None, 0) == bm.BM_INVALID_ARG
