@@ -97,3 +97,46 @@ def test_oracle_matches_live_reference():
         np.testing.assert_array_equal(l1, l2)
         assert s1 == s2
         ref.close()
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("seed", [31, 32, 33])
+def test_oracle_matches_live_reference_with_loops_and_duplicates(seed):
+    """Random pairs with self-loops (at most one per A vertex), duplicate edges
+    and zero weights: the restated calculate_swap_delta, whole rows and one
+    serial sweep equal the reference's own, quirks included."""
+    n, m = 200, 2500
+    rng = np.random.default_rng(seed)
+
+    def graph(one_loop_per_vertex):
+        s = rng.integers(1, n + 1, m).astype(np.int32)
+        d = rng.integers(1, n + 1, m).astype(np.int32)
+        lv = rng.choice(np.arange(1, n + 1), 40, replace=False).astype(np.int32)
+        dup = rng.integers(0, m, 300)
+        s, d = np.concatenate([s, lv, s[dup]]), np.concatenate([d, lv, d[dup]])
+        w = rng.integers(0, 9, s.shape[0]).astype(np.int32)
+        if one_loop_per_vertex:
+            seen, keep = set(), []
+            for i in range(s.shape[0]):
+                if s[i] == d[i]:
+                    if s[i] in seen:
+                        continue
+                    seen.add(int(s[i]))
+                keep.append(i)
+            s, d, w = s[keep], d[keep], w[keep]
+        return s, d, w
+
+    A, B = graph(True), graph(False)
+    orc, ref = Oracle(n, A, B), Reference(n, A, B)
+    pi = np.concatenate([[0], rng.permutation(n) + 1]).astype(np.int32)
+    assert orc.score(pi) == ref.score(pi)
+    pairs = rng.integers(1, n + 1, size=(3000, 2)).astype(np.int32)
+    np.testing.assert_array_equal(orc.pairs(pi, pairs), ref.pairs(pi, pairs))
+    rows = np.array([1, 77, 200], np.int32)
+    np.testing.assert_array_equal(orc.rows(pi, rows), ref.rows(pi, rows))
+    p1, s1, l1, _, _ = orc.serial(pi, max_sweeps=1)
+    p2, s2, l2, _, _ = ref.serial(pi, max_sweeps=1)
+    np.testing.assert_array_equal(l1, l2)
+    np.testing.assert_array_equal(p1, p2)
+    assert s1 == s2
+    ref.close()
