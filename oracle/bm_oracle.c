@@ -16,6 +16,8 @@
  *                   (bounded: the reference loops forever)
  *   orc_rows_omp    the OpenMP m2 sweep        src/graph-alignment-optimized-parallel.c:544
  *                   (deltas only, no applies)
+ *   orc_sim_sweep   the similarity-filtered    src/graph-alignment.c:489-595
+ *                   pass of the graph-alignment variant
  *   orc_mlp         FP64 replica of the engine's learned-proposal MLP (no
  *                   reference counterpart), the checker of its gradients
  * Parity is pinned by tests/golden/ fixtures produced by the reference's own
@@ -43,6 +45,9 @@ typedef struct {
     int32_t* iptr;  /* n+2: in-lists (EdgeMap reverse_edges) */
     int32_t* ifrom;
     int32_t* iw;
+    /* vertices in order of first appearance (from, then to, of each edge) */
+    int32_t* nodes;
+    int32_t nnodes;
     /* matrix lookups: key (s,d) -> last weight */
     uint64_t* hkey;
     int32_t* hval;
@@ -71,6 +76,7 @@ void orc_graph_free(orc_graph* g) {
     free(g->optr); free(g->oto); free(g->ow);
     free(g->iptr); free(g->ifrom); free(g->iw);
     free(g->hkey); free(g->hval);
+    free(g->nodes);
     free(g);
 }
 
@@ -91,7 +97,8 @@ orc_graph* orc_graph_new(int32_t n, int64_t m, const int32_t* src, const int32_t
     while (cap < (uint64_t)(2 * m + 16)) cap <<= 1;
     g->hkey = (uint64_t*)malloc(sizeof(uint64_t) * cap);
     g->hval = (int32_t*)malloc(sizeof(int32_t) * cap);
-    if (!g->optr || !g->iptr || !g->oto || !g->ow || !g->ifrom || !g->iw || !g->hkey || !g->hval) {
+    g->nodes = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n + 1));
+    if (!g->optr || !g->iptr || !g->oto || !g->ow || !g->ifrom || !g->iw || !g->hkey || !g->hval || !g->nodes) {
         orc_graph_free(g);
         return NULL;
     }
@@ -115,6 +122,15 @@ orc_graph* orc_graph_new(int32_t n, int64_t m, const int32_t* src, const int32_t
     }
     free(fo);
     free(fi);
+    /* add_node (src/graph-alignment.c:159-174) for from, then to */
+    uint8_t* seen = (uint8_t*)calloc((size_t)n + 1, 1);
+    if (!seen) { orc_graph_free(g); return NULL; }
+    for (int64_t e = 0; e < m; e++) {
+        const int32_t v2[2] = {src[e], dst[e]};
+        for (int k = 0; k < 2; k++)
+            if (!seen[v2[k]]) { seen[v2[k]] = 1; g->nodes[g->nnodes++] = v2[k]; }
+    }
+    free(seen);
     return g;
 }
 
@@ -246,6 +262,79 @@ void orc_pairs(const orc_graph* gm, const orc_graph* gf, const int32_t* mapping,
         int32_t u = pairs[2 * i], v = pairs[2 * i + 1];
         out[i] = (u == v) ? 0 : orc_swap_delta(gm, gf, mapping, u, v);
     }
+}
+
+/* Per-vertex metrics of calculate_node_metrics (src/graph-alignment.c:235-272)
+ * for the vertices the graph lists: degree counts, the weight total of both
+ * directions, that total divided by the out- and by the in-degree, and the
+ * ordering rank.  Vertices the graph does not list keep zeros. */
+typedef struct {
+    int32_t indeg, outdeg, wsum, rank;
+    double avg_in, avg_out;
+} orc_vmetrics;
+
+static orc_vmetrics* orc_metrics(const orc_graph* g, const int32_t* rank) {
+    orc_vmetrics* mt = (orc_vmetrics*)calloc((size_t)g->n + 1, sizeof(orc_vmetrics));
+    if (!mt) return NULL;
+    for (int32_t i = 0; i < g->nnodes; i++) {
+        const int32_t v = g->nodes[i];
+        orc_vmetrics* x = &mt[v];
+        x->outdeg = g->optr[v + 1] - g->optr[v];
+        for (int32_t j = g->optr[v]; j < g->optr[v + 1]; j++) x->wsum += g->ow[j];
+        x->indeg = g->iptr[v + 1] - g->iptr[v];
+        for (int32_t j = g->iptr[v]; j < g->iptr[v + 1]; j++) x->wsum += g->iw[j];
+        if (x->outdeg > 0) x->avg_out = (double)x->wsum / x->outdeg;
+        if (x->indeg > 0) x->avg_in = (double)x->wsum / x->indeg;
+        x->rank = rank[v];
+    }
+    return mt;
+}
+
+/* calculate_node_similarity (src/graph-alignment.c:274-284), the same
+ * operations in the same order: 0.7 x (5|d in| + 5|d out| + |d avg in| +
+ * |d avg out|) + 0.3 x |d rank|, negated. */
+static double orc_similarity(const orc_vmetrics* a, const orc_vmetrics* b) {
+    double s = 5 * fabs((double)(a->indeg - b->indeg)) + 5 * fabs((double)(a->outdeg - b->outdeg)) +
+               fabs(a->avg_in - b->avg_in) + fabs(a->avg_out - b->avg_out);
+    double o = fabs((double)(a->rank - b->rank));
+    s = 0.7 * s + 0.3 * o;
+    return -s;
+}
+
+/* The single pass of optimize_mapping in the graph-alignment variant
+ * (src/graph-alignment.c:512-578): m1 and m2 run over gm's vertices in order
+ * of first appearance; a swap is evaluated only when the similarity of the
+ * swapped images is higher than the current one (:545-553), and a positive
+ * delta is applied at once.  rank_m, rank_f: ordering ranks per vertex (0 for
+ * vertices absent from the ordering).  The variant reads B weights by list
+ * scan (first duplicate); this restatement uses the last, so the two agree on
+ * graphs without duplicate edges.  Returns the number of accepts. */
+int64_t orc_sim_sweep(const orc_graph* gm, const orc_graph* gf, int32_t* mapping, const int32_t* rank_m,
+                      const int32_t* rank_f) {
+    orc_vmetrics* mm = orc_metrics(gm, rank_m);
+    orc_vmetrics* mf = orc_metrics(gf, rank_f);
+    int64_t accepts = -1;
+    if (mm && mf) {
+        accepts = 0;
+        for (int32_t i = 0; i < gm->nnodes; i++) {
+            const int32_t m1 = gm->nodes[i];
+            for (int32_t j = 0; j < gm->nnodes; j++) {
+                const int32_t m2 = gm->nodes[j];
+                if (m1 == m2) continue;
+                const int32_t f1 = mapping[m1], f2 = mapping[m2];
+                const double cur = orc_similarity(&mm[m1], &mf[f1]) + orc_similarity(&mm[m2], &mf[f2]);
+                const double swp = orc_similarity(&mm[m1], &mf[f2]) + orc_similarity(&mm[m2], &mf[f1]);
+                if (swp > cur && orc_swap_delta(gm, gf, mapping, m1, m2) > 0) {
+                    mapping[m1] = f2;
+                    mapping[m2] = f1;
+                    accepts++;
+                }
+            }
+        }
+    }
+    free(mm);
+    free(mf);
+    return accepts;
 }
 
 /* Simulated-annealing chain of simulated_annealing

@@ -47,6 +47,11 @@ def golden_selfloop_ref():
     return load_golden("golden_selfloop_ref.npz")
 
 
+@pytest.fixture(scope="session")
+def golden_simfilter():
+    return load_golden("golden_simfilter.npz")
+
+
 def make_engine(n, A, B, pi):
     """An engine holding graphs A, B (edge-array triples) and mapping pi."""
     import bmb200 as bm

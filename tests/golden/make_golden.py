@@ -141,6 +141,66 @@ def make_selfloop_ref_case(name, seed=23, n=300, m=3000, loops=75):
                  ("n", "score_init", "serial_score", "serial_accepts", "serial_sweeps", "serial_converged")})
 
 
+def simfilter_inputs(seed, n=300, m=3000, loops=0):
+    """A pair for the similarity-filtered variant: the generator's pair (or,
+    with loops > 0, a random pair with that many self-loops per graph and no
+    duplicate edges), the largest id present in both graphs (the variant sizes
+    its arrays by each graph's largest id), and orderings by weighted degree."""
+    if loops:
+        rng = np.random.default_rng(seed)
+
+        def graph():
+            s_ = rng.integers(1, n + 1, m).astype(np.int32)
+            d_ = rng.integers(1, n + 1, m).astype(np.int32)
+            lv = rng.choice(np.arange(1, n + 1), loops, replace=False).astype(np.int32)
+            s_, d_ = np.concatenate([s_, lv]), np.concatenate([d_, lv])
+            _, first = np.unique(s_.astype(np.int64) * (n + 1) + d_, return_index=True)
+            keep = np.sort(first)
+            return [s_[keep], d_[keep], rng.integers(1, 9, keep.shape[0]).astype(np.int32)]
+
+        A, B = graph(), graph()
+        init = np.concatenate([[0], rng.permutation(n) + 1]).astype(np.int32)
+    else:
+        Ag, Bg, _, init = bm.gen_pair(1, n=n, m_target=m, seed=seed)
+        A, B = [Ag.src, Ag.dst, Ag.w], [Bg.src, Bg.dst, Bg.w]
+    for G in (A, B):
+        if max(int(G[0].max()), int(G[1].max())) < n:
+            G[0] = np.append(G[0], n).astype(np.int32)
+            G[1] = np.append(G[1], 1).astype(np.int32)
+            G[2] = np.append(G[2], 1).astype(np.int32)
+    rank_m = bm.ordering_by_weighted_degree(bm.Graph(n, *A))
+    rank_f = bm.ordering_by_weighted_degree(bm.Graph(n, *B))
+    return n, tuple(A), tuple(B), init, rank_m, rank_f
+
+
+def ref_simfilter_pass(A, B, init, rank_m, rank_f):
+    """One pass of the reference variant (its orderings read from CSV files
+    written beside the reference libraries)."""
+    from oracle_bind import ReferenceGA
+    tmp = os.path.join(REPO, "oracle", "_ref", "ga_tmp")
+    os.makedirs(tmp, exist_ok=True)
+    pm, pf = os.path.join(tmp, "order_m.csv"), os.path.join(tmp, "order_f.csv")
+    bm.write_ordering(pm, rank_m)
+    bm.write_ordering(pf, rank_f)
+    ref = ReferenceGA(A, B)
+    try:
+        pi = ref.sweep(init, pm, pf, os.path.join(tmp, "out_mapping.csv"))
+        return pi, ref.score(pi)
+    finally:
+        ref.close()
+
+
+def make_simfilter_case(name, seed=13):
+    """The similarity-filtered single pass of src/graph-alignment.c on a
+    300-vertex pair: its final mapping and score."""
+    n, A, B, init, rank_m, rank_f = simfilter_inputs(seed)
+    pi, score = ref_simfilter_pass(A, B, init, rank_m, rank_f)
+    np.savez_compressed(os.path.join(HERE, name), n=np.int64(n), a_src=A[0], a_dst=A[1], a_w=A[2], b_src=B[0],
+                        b_dst=B[1], b_w=B[2], pi_init=init, rank_m=rank_m, rank_f=rank_f, pass_pi=pi,
+                        pass_score=np.int64(score))
+    print(name, "moved", int((pi != init).sum()), "score", score)
+
+
 CASES = {
     "golden_small.npz": lambda: make_pair_case("golden_small.npz", 1, 11, 300, 3000, 3000, 6, max_sweeps=-1,
                                                log_cap=1 << 16, verify=True),
@@ -148,6 +208,7 @@ CASES = {
                                               log_cap=3000, verify=False),
     "golden_selfloop.npz": lambda: make_selfloop_case("golden_selfloop.npz"),
     "golden_selfloop_ref.npz": lambda: make_selfloop_ref_case("golden_selfloop_ref.npz"),
+    "golden_simfilter.npz": lambda: make_simfilter_case("golden_simfilter.npz"),
 }
 
 

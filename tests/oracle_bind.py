@@ -16,10 +16,12 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(REPO, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_SO = os.path.join(ORACLE_DIR, "_ref", "libref.so")
+REF_GA_SO = os.path.join(ORACLE_DIR, "_ref", "libref_ga.so")
 
 vp = C.c_void_p
 _orc = None
 _ref = None
+_ref_ga = None
 
 
 def _p(a):
@@ -49,6 +51,8 @@ def oracle_lib() -> C.CDLL:
         L.orc_rows_omp.argtypes = [vp, vp, vp, vp, C.c_int32, vp, C.c_int32]
         L.orc_pairs.restype = None
         L.orc_pairs.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
+        L.orc_sim_sweep.restype = C.c_int64
+        L.orc_sim_sweep.argtypes = [vp, vp, vp, vp, vp]
         L.orc_perm_delta.restype = C.c_int64
         L.orc_perm_delta.argtypes = [vp, vp, vp, vp, C.c_int32, vp]
         L.orc_sa_run.restype = C.c_int64
@@ -59,6 +63,27 @@ def oracle_lib() -> C.CDLL:
 
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+def ref_ga_available() -> bool:
+    return os.path.exists(REF_GA_SO)
+
+
+def ref_ga_lib() -> C.CDLL:
+    global _ref_ga
+    if _ref_ga is None:
+        L = C.CDLL(REF_GA_SO)
+        L.refga_build.restype = C.c_int
+        L.refga_build.argtypes = [C.c_int, C.c_longlong, vp, vp, vp]
+        L.refga_free.restype = None
+        L.refga_max_node.restype = C.c_int
+        L.refga_max_node.argtypes = [C.c_int]
+        L.refga_score.restype = C.c_int
+        L.refga_score.argtypes = [vp]
+        L.refga_sweep.restype = C.c_int
+        L.refga_sweep.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p, vp]
+        _ref_ga = L
+    return _ref_ga
 
 
 def ref_lib() -> C.CDLL:
@@ -134,6 +159,16 @@ class Oracle:
         out = np.zeros((rows.shape[0], self.n + 1), np.int64)
         self.L.orc_rows_omp(self.gm, self.gf, _p(pi), _p(rows), rows.shape[0], _p(out), threads)
         return out
+
+    def sim_sweep(self, pi, rank_m, rank_f):
+        """The similarity-filtered pass of the graph-alignment variant;
+        returns (pi after the pass, accepts)."""
+        pi = _i32(pi).copy()
+        rm, rf = _i32(rank_m), _i32(rank_f)
+        acc = self.L.orc_sim_sweep(self.gm, self.gf, _p(pi), _p(rm), _p(rf))
+        if acc < 0:
+            raise MemoryError("orc_sim_sweep failed")
+        return pi, int(acc)
 
     def perm_delta(self, pi, verts, perm) -> int:
         pi, verts, perm = _i32(pi), _i32(verts), _i32(perm)
@@ -234,3 +269,33 @@ def mlp_oracle(w, x, y=None, rounding=True):
     if st != 0:
         raise MemoryError("orc_mlp failed")
     return out, grads, loss.value
+
+
+class ReferenceGA:
+    """The reference's similarity-filtered variant (src/graph-alignment.c,
+    oracle/_ref/libref_ga.so): graphs built by its add_edge, one pass of its
+    optimize_mapping.  Its orderings are read from CSV files by the variant."""
+
+    def __init__(self, A, B):
+        L = ref_ga_lib()
+        self.L = L
+        for which, g in ((0, A), (1, B)):
+            s, d, w = (_i32(x) for x in g)
+            if L.refga_build(which, s.shape[0], _p(s), _p(d), _p(w)) != 0:
+                raise RuntimeError("refga_build failed")
+
+    def close(self):
+        self.L.refga_free()
+
+    def max_node(self, which: int) -> int:
+        return int(self.L.refga_max_node(which))
+
+    def score(self, pi) -> int:
+        return int(self.L.refga_score(_p(_i32(pi))))
+
+    def sweep(self, pi, ord_m: str, ord_f: str, out_path: str) -> np.ndarray:
+        pi = _i32(pi)
+        out = np.zeros_like(pi)
+        if self.L.refga_sweep(_p(pi), pi.shape[0], ord_m.encode(), ord_f.encode(), out_path.encode(), _p(out)) != 0:
+            raise RuntimeError("refga_sweep failed")
+        return out
