@@ -512,7 +512,9 @@ bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len);
  * (:571-576), instead of being checked against the sum of the deltas.
  * Permutation sets, 3-rotations, annealing chains and one-sided gains stay
  * exact.  Duplicate A edges between the two swapped vertices still count once
- * per list entry (the reference counts the matrix's last weight once). */
+ * per list entry (the reference counts the matrix's last weight once).  The
+ * mode applies to deltas computed after the call: a delta table built before
+ * it keeps its values until rebuilt or refreshed. */
 #define BM_SEMANTICS_EXACT 0
 #define BM_SEMANTICS_REF_CPU 1
 bm_status bm_set_semantics(bm_ctx* ctx, int32_t mode);
