@@ -16,7 +16,9 @@ e2e    = the same through the public C ABI bm_rows_best with host buffers
          (rows in, row results out), wall clock per call
 --impl reference times the reference's own calculate_swap_delta under its
 OpenMP m2 sweep (oracle/_ref, compiled from the reference sources; the
-restated oracle if that library is absent) on a bounded sample of rows.
+restated oracle if that library is absent) on the same row batches.  Its
+process loads no library of this engine: a child process writes the workload
+(generator and greedy matching) to a temporary file, read back with numpy.
 Under torchrun every rank takes disjoint row batches (weak scaling); only a
 barrier and a max of the timings cross ranks (gloo), there is no data-path
 collective.
@@ -87,6 +89,27 @@ def make_workload():
     return A, B, truth, init, rows
 
 
+WORKLOAD_KEYS = ("a_src", "a_dst", "a_w", "b_src", "b_dst", "b_w", "init", "rows")
+
+
+def write_workload(path):
+    """The workload as plain arrays (the reference arm's input)."""
+    A, B, truth, init, rows = make_workload()
+    np.savez(path, n=np.int64(A.n), a_src=A.src, a_dst=A.dst, a_w=A.w, b_src=B.src, b_dst=B.dst, b_w=B.w, init=init,
+             rows=rows)
+
+
+def read_workload_isolated():
+    """The workload made by a child process and read back with numpy, so the
+    calling process loads no library of this engine."""
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "workload.npz")
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--write-workload", path], check=True,
+                       env=dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0"))
+        z = np.load(path)
+        return int(z["n"]), {k: np.ascontiguousarray(z[k]) for k in WORKLOAD_KEYS}
+
+
 def algorithmic_bytes_per_row(A: bm.Graph, B: bm.Graph, pi: np.ndarray) -> np.ndarray:
     """Bytes the whole-row algorithm must read for each row u (1-indexed array):
     4 B per second-hop list entry, 16 B per first-hop item (entry, pointer
@@ -152,7 +175,7 @@ class ClockSampler:
             return None
         names = sorted(k for k, bit in self.REASONS.items() if self.reasons & bit)
         return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": names,
-                "samples": len(self.samples), "source": "NVML, 2 ms polling during the timed region"}
+                "samples": len(self.samples), "source": "NVML, 2 ms polling during the warm-up and timed steps"}
 
 
 def measured_peaks():
@@ -206,39 +229,60 @@ def step_starts(n: int, steps: int, offset: float = 0.0):
     return [int(((s + offset) * n) // steps) % n for s in range(steps)]
 
 
+def bench_config(n, mA, mB, R, ws):
+    """The `config` of a bench line; both arms print the same one."""
+    return {"workload": WORKLOAD, "n": n, "edges_A": mA, "edges_B": mB, "rows_per_step": R,
+            "candidates_per_step": R * (n - 1), "l2": "flushed before every step",
+            "parallelism": f"row batches sharded over {ws} rank(s), no data-path collective"}
+
+
 def run_reference(args, ws, rank, dist):
+    """The reference's calculate_swap_delta under its OpenMP m2 sweep on the
+    bench's own row batches (all partners of each row), all host threads.
+    Rank 0 alone runs it.  A step is the same batch as in the engine's arm
+    when K such steps fit --ref-budget seconds, else the first rows of it."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(REPO, "tests"))
     from oracle_bind import Oracle, Reference, ref_available
-    A, B, truth, init, rows = make_workload()
-    n = A.n
+    n, w = read_workload_isolated()
+    init, rows = w["init"], w["rows"]
+    R = args.rows_per_step
     threads = os.cpu_count() or 1
-    Ae, Be = (A.src, A.dst, A.w), (B.src, B.dst, B.w)
+    Ae, Be = (w["a_src"], w["a_dst"], w["a_w"]), (w["b_src"], w["b_dst"], w["b_w"])
     if ref_available():
         impl, kind = Reference(n, Ae, Be), "reference"
     else:
         impl, kind = Oracle(n, Ae, Be), "port"
     for st in step_starts(n, args.warmup, 0.5):
         impl.rows(init, rows[st:st + 1], threads)
+    # rows per step: the whole batch if K steps fit the budget (estimated from
+    # one timed row), else fewer
+    t0 = time.perf_counter()
+    impl.rows(init, rows[:1], threads)
+    est = time.perf_counter() - t0
+    rps = max(1, min(R, int(args.ref_budget / max(1e-9, est * args.steps))))
     total = 0.0
     starts = step_starts(n, args.steps)
     for st in starts:
+        idx = (st + np.arange(rps)) % n
         t0 = time.perf_counter()
-        impl.rows(init, rows[st:st + 1], threads)
+        impl.rows(init, np.ascontiguousarray(rows[idx]), threads)
         total += time.perf_counter() - t0
     if kind == "reference":
         impl.close()
-    v = args.steps * (n - 1) / total
-    base = {"value": v, "unit": "deltas/s", "cores": threads, "kind": kind,
-            "sample": f"one row x {n - 1} partners per step, {args.steps} rows evenly spaced over the ordering pass"}
+    v = args.steps * rps * (n - 1) / total
+    sample = (f"the engine arm's batches: {rps} rows x {n - 1} partners per step" if rps == R else
+              f"the first {rps} of the {R} rows of each of the engine arm's batches x {n - 1} partners per step")
+    base = {"value": v, "unit": "deltas/s", "cores": threads, "kind": kind, "sample": sample}
+    cfg = bench_config(n, int(w["a_src"].shape[0]), int(w["b_src"].shape[0]), R, 1)
+    if rps != R:
+        cfg["reference_rows_per_step"] = rps
     out = {"impl": "reference", "metric": "exact swap-deltas/s", "value": v, "unit": "deltas/s", "n_gpus": ws,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "n": n, "edges_A": A.m, "edges_B": B.m,
-                      "sample_per_step": f"1 row x {n - 1} partners"},
-           "cpu_baseline": base, "e2e": {"value": v, "unit": "deltas/s", "h2d_bytes_per_step": 0,
-                                          "d2h_bytes_per_step": 0}}
+           "config": cfg, "cpu_baseline": base,
+           "e2e": {"value": v, "unit": "deltas/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
 
@@ -272,11 +316,13 @@ def run_ours(args, ws, rank, local, dist):
         eng.rows_best_dev(d_rows + 4 * R * step, None, R, d_res)
         eng.record(ev[step][1])
 
+    # clocks are sampled from the warm-up on: the timed region alone lasts a
+    # few milliseconds, shorter than a few NVML polls
+    clocks = ClockSampler(eng.pci_bus_id())
     for s in range(args.warmup):
         device_step(s)
     eng.sync()
     barrier(dist)
-    clocks = ClockSampler(eng.pci_bus_id())
     t_wall = time.perf_counter()
     launches_a = eng.launch_count()
     for s in range(args.warmup, nsteps):
@@ -316,15 +362,22 @@ def run_ours(args, ws, rank, local, dist):
 
     peak, peak_kind = measured_peaks()
     achieved = total_bytes / (total_ms / 1000.0) / 1e9
+    traffic, traffic_rec = recorded_traffic(args.steps, args.warmup, R)
+    l2 = l2_peak(eng)
     out = {"metric": "exact swap-deltas/s", "value": value, "unit": "deltas/s", "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "n": n, "edges_A": A.m, "edges_B": B.m, "rows_per_step": R,
-                      "candidates_per_step": deltas_step, "l2": "flushed before every step",
-                      "parallelism": f"row batches sharded over {ws} rank(s), no data-path collective"},
+           "config": bench_config(n, A.m, B.m, R, ws),
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak,
-                        "traffic": profiled_traffic(args.steps, args.warmup, R), "peak_source": peak_kind,
+                        "traffic": traffic, "peak_source": peak_kind,
+                        "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of "
+                                           f"{traffic_rec['launches']} timed launches of this command, kernel "
+                                           f"source digest {traffic_rec['kernel_digest']}") if traffic_rec else
+                                          "no ncu record of this kernel source and command",
+                        "l2_peak": l2, "l2_frac": (achieved / l2) if l2 else None,
+                        "l2_peak_source": "measured in this run: 16-byte ld.cg reads of a 64 MiB L2-resident buffer, "
+                                          "20 passes, CUDA events",
                         "kernel": "rows_kernel (whole-row 2-hop scatter, fused row reduction)",
                         "bytes_per_step": total_bytes / args.steps},
            "e2e": {"value": e2e_val, "unit": "deltas/s", "h2d_bytes_per_step": 4 * R,
@@ -334,6 +387,12 @@ def run_ours(args, ws, rank, local, dist):
         out["clocks"] = clk
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(A, B, init, rows, starts[args.warmup:], budget_s=args.ref_seconds)
+    if rank == 0 and ws == 1 and not args.no_reference_gpu:
+        out["reference_gpu"] = reference_gpu(A, B, init, batch(args.warmup))
+        rg = out["reference_gpu"]
+        if "deltas_per_s" in rg:
+            # the engine's row kernel on that same batch, from the timed steps
+            rg["engine_deltas_per_s_same_batch"] = deltas_step / (step_ms[0] / 1e3)
     converged_pi = None
     if rank == 0 and ws == 1 and args.search_seconds > 0:
         out["search"] = plain_search(eng, rows, args.search_seconds)
@@ -344,7 +403,7 @@ def run_ours(args, ws, rank, local, dist):
         out["learned_vs_plain"] = learned_compare(local, A, B, init, rows, out["search"], args.learned_seconds)
     if rank == 0 and ws == 1 and not args.no_extras:
         out["initial_matching"] = initial_matching(local, A, B, init)
-        out["higher_order"] = higher_order(local, A, B, init)
+        out["higher_order"] = higher_order(local, A, B, init, not args.no_reference_gpu)
         out["delta_table"] = delta_table(local, A, B, init, out.get("search", {}))
         out["subset_assignment"] = [subset_assignment(local, A, B, init, "initial matching")]
         if converged_pi is not None:
@@ -355,21 +414,94 @@ def run_ours(args, ws, rank, local, dist):
         print(json.dumps(out), flush=True)
 
 
-def profiled_traffic(steps: int, warmup: int, rows_per_step: int):
-    """DRAM bytes per rows_kernel launch (read + write) from the committed ncu
-    summary of this bench's timed launches, when the summary's configuration
-    is this run's; else None."""
-    path = os.path.join(REPO, "profiles", "rows_kernel_cfg2.md")
+TRAFFIC_RECORD = os.path.join(REPO, "profiles", "rows_kernel_traffic.json")
+ROWS_KERNEL_SOURCES = ("brain-match_b200/csrc/bm_rows.cu", "brain-match_b200/csrc/bm_internal.cuh")
+
+
+def rows_kernel_digest() -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for rel in ROWS_KERNEL_SOURCES:
+        with open(os.path.join(REPO, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def recorded_traffic(steps: int, warmup: int, rows_per_step: int):
+    """DRAM bytes (read + write) per rows_kernel launch from an ncu capture of
+    this bench's own launches (the record names the capture and the digest of
+    the kernel's sources it was taken on); None unless the record is of the
+    current kernel source and of this run's steps, warm-up and batch size."""
     try:
-        with open(path) as f:
-            for line in f:
-                if line.startswith("bench-traffic:"):
-                    rec = json.loads(line.split(":", 1)[1])
-                    if (rec["steps"], rec["warmup"], rec["rows_per_step"]) == (steps, warmup, rows_per_step):
-                        return float(rec["bytes_per_launch"])
+        with open(TRAFFIC_RECORD) as f:
+            rec = json.load(f)
+        if (rec["kernel_digest"] == rows_kernel_digest() and rec["steps"] == steps and rec["warmup"] == warmup
+                and rec["rows_per_step"] == rows_per_step):
+            return float(rec["dram_bytes_per_launch"]), rec
     except (OSError, ValueError, KeyError):
         pass
-    return None
+    return None, None
+
+
+def l2_peak(eng):
+    """Measured L2 read bandwidth of this GPU (GB/s), 64 MiB read 20 times."""
+    g = C.c_double()
+    st = bm.cuda_lib().bm_probe_l2_bandwidth(eng.h, 64 << 20, 20, C.byref(g))
+    return g.value if st == bm.BM_OK else None
+
+
+def reference_gpu(A, B, init, rows_batch):
+    """The reference's own GPU swap-delta kernel (calculateSwapDeltasKernelQuick,
+    src/graph-re-alignment-gpu.cu:139-248, compiled for sm_100a into
+    oracle/_ref/librefgpu.so) on one of the timed batches: the rows as its
+    changed vertices, every partner, dense int16 matrices as its driver builds
+    them; CUDA events around three launches after one warm-up."""
+    path = os.path.join(REPO, "oracle", "_ref", "librefgpu.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/librefgpu.so not built"}
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.refgpu_quick.restype = C.c_int
+    L.refgpu_quick.argtypes = [C.c_int, C.c_longlong, vp, vp, vp, C.c_longlong, vp, vp, vp, vp, vp, C.c_int, C.c_int,
+                               C.POINTER(C.c_float), vp, vp]
+    L.refgpu_total_pairs.restype = C.c_longlong
+    L.refgpu_total_pairs.argtypes = [C.c_int, C.c_int]
+    r = np.ascontiguousarray(rows_batch, np.int32)
+    ms = C.c_float()
+    st = L.refgpu_quick(A.n, A.m, A.src.ctypes.data, A.dst.ctypes.data, A.w.ctypes.data, B.m, B.src.ctypes.data,
+                        B.dst.ctypes.data, B.w.ctypes.data, init.ctypes.data, r.ctypes.data, len(r), 3, C.byref(ms),
+                        None, None)
+    if st != 0:
+        return {"unavailable": f"reference kernel returned CUDA error {st}"}
+    pairs = int(L.refgpu_total_pairs(A.n, len(r)))
+    return {"kernel": "calculateSwapDeltasKernelQuick", "rows": len(r), "pairs_per_launch": pairs,
+            "ms_per_launch": ms.value, "deltas_per_s": pairs / (ms.value / 1e3),
+            "timing": "CUDA events, 3 launches after one warm-up, inputs resident"}
+
+
+def reference_gpu3(A, B, init, rows, batch=4096):
+    """The reference's own 3-vertex GPU kernel (calculateThreeNodeSwapKernel,
+    src/graph-re-alignment-gpu-3-swap.cu:43-305, oracle/_ref/librefgpu3.so) on
+    the first `batch` triplets of its enumeration around six rows: triplets/s,
+    each with five permutations over dense int16 matrices."""
+    path = os.path.join(REPO, "oracle", "_ref", "librefgpu3.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/librefgpu3.so not built"}
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.refgpu3_triplets.restype = C.c_int
+    L.refgpu3_triplets.argtypes = [C.c_int, C.c_longlong, vp, vp, vp, C.c_longlong, vp, vp, vp, vp, vp, C.c_int,
+                                   C.c_int, C.c_int, C.POINTER(C.c_float), vp, vp]
+    changed = np.ascontiguousarray(rows[A.n // 4:A.n // 4 + 6], np.int32)
+    ms = C.c_float()
+    st = L.refgpu3_triplets(A.n, A.m, A.src.ctypes.data, A.dst.ctypes.data, A.w.ctypes.data, B.m, B.src.ctypes.data,
+                            B.dst.ctypes.data, B.w.ctypes.data, init.ctypes.data, changed.ctypes.data, 6, batch, 1,
+                            C.byref(ms), None, None)
+    if st != 0:
+        return {"unavailable": f"reference kernel returned CUDA error {st}"}
+    return {"kernel": "calculateThreeNodeSwapKernel", "triplets": batch, "ms_per_launch": ms.value,
+            "sets_per_s": batch / (ms.value / 1e3), "permutations_per_set": 5,
+            "timing": "CUDA events, one launch after one warm-up, inputs resident"}
 
 
 MLP_FLOP_PER_PAIR = 2 * (24 * 128 + 128 * 128 + 128)
@@ -479,7 +611,7 @@ def learned_compare(device, A, B, init, rows, plain, seconds):
     return out
 
 
-def higher_order(device, A, B, init):
+def higher_order(device, A, B, init, reference_kernels=True):
     """Exact k-set permutation deltas on the full-scale pair: 4,096 random
     8-subsets (8! = 40,320 permutations each) and 65,536 3-vertex sets along
     2-paths u -> x -> y (all 6 permutations), best permutation per set."""
@@ -509,7 +641,25 @@ def higher_order(device, A, B, init):
         out[f"k{k}"] = {"sets": int(len(sets)), "sets_per_s": len(sets) / dt,
                         "permutation_deltas_per_s": len(sets) * nperm / dt, "improving_sets": int((best > 0).sum()),
                         "seconds": dt, "timing": "host call, transfers included"}
+    # device time of the 3-sets alone, for the reference kernel beside it
+    d_sets = e.dev_alloc(sets3.nbytes)
+    e.h2d(d_sets, sets3)
+    d_best = e.dev_alloc(8 * len(sets3))
+    d_perm = e.dev_alloc(4 * 3 * len(sets3))
+    d_status = e.dev_alloc(4)
+    e.h2d(d_status, np.zeros(1, np.int32))
+    a, b = e.event(), e.event()
+    e.kset_eval_dev(3, d_sets, len(sets3), d_best, d_perm, d_status)
+    e.record(a)
+    e.kset_eval_dev(3, d_sets, len(sets3), d_best, d_perm, d_status)
+    e.record(b)
+    e.sync()
+    ms = e.elapsed_ms(a, b)
+    out["k3"]["device_sets_per_s"] = len(sets3) / (ms / 1e3)
     e.close()
+    if reference_kernels:
+        order = bm.rows_from_ordering(bm.ordering_by_weighted_degree(A))
+        out["k3_reference_gpu"] = reference_gpu3(A, B, init, order)
     return out
 
 
@@ -647,7 +797,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows-per-step", type=int, default=57)
-    ap.add_argument("--ref-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=12.0, help="budget of the engine arm's cpu_baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="budget of the reference arm's timed steps (seconds); larger K get fewer rows per step")
+    ap.add_argument("--write-workload", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU kernels on the same batches")
     ap.add_argument("--search-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned-seconds", type=float, default=90.0)
@@ -659,6 +814,9 @@ def main():
                              "mlp_scorer"],
                     help="run one side section alone and print its result (a profiling target, not a bench line)")
     args = ap.parse_args()
+    if args.write_workload:
+        write_workload(args.write_workload)
+        return
     if args.only:
         run_section(args)
         return

@@ -1,5 +1,6 @@
 // bm_api.cu — context lifecycle, graph upload, mapping state and device
 // utilities of the C ABI declared in include/bm_cuda.h.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -43,15 +44,58 @@ extern "C" const char* bm_status_str(bm_status s) {
 
 extern "C" const char* bm_ctx_last_error(const bm_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
 
+// ------------------------------------------------------- counted allocation
+
+static std::atomic<unsigned long long> g_alloc_calls{0};
+
+cudaError_t bm_cuda_malloc_raw(void** p, size_t bytes) {
+    g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
+    return cudaMalloc(p, bytes);
+}
+
+cudaError_t bm_cuda_free(void* p) {
+    if (!p) return cudaSuccess;  // releasing nothing: no runtime call, not counted
+    g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
+    return cudaFree(p);
+}
+
+cudaError_t bm_cuda_host_malloc_raw(void** p, size_t bytes) {
+    g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
+    return cudaMallocHost(p, bytes);
+}
+
+cudaError_t bm_cuda_host_alloc(void** p, size_t bytes, unsigned flags) {
+    g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
+    return cudaHostAlloc(p, bytes, flags);
+}
+
+cudaError_t bm_cuda_host_free(void* p) {
+    if (!p) return cudaSuccess;
+    g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
+    return cudaFreeHost(p);
+}
+
+extern "C" uint64_t bm_alloc_count(void) { return (uint64_t)g_alloc_calls.load(std::memory_order_relaxed); }
+
+extern "C" bm_status bm_device_memory(bm_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes) {
+    if (!ctx || !free_bytes || !total_bytes) return BM_INVALID_ARG;
+    BM_CUDA(ctx, cudaSetDevice(ctx->device));
+    size_t f = 0, t = 0;
+    BM_CUDA(ctx, cudaMemGetInfo(&f, &t));
+    *free_bytes = f;
+    *total_bytes = t;
+    return BM_OK;
+}
+
 // --------------------------------------------------------------- lifecycle
 
 static void free_graph(DevGraph& g) {
-    cudaFree(g.out_ptr); cudaFree(g.in_ptr);
-    cudaFree(g.out_ent); cudaFree(g.in_ent);
-    cudaFree(g.self_w);
-    cudaFree(g.out_twin); cudaFree(g.in_twin);
-    cudaFree(g.out_ent0); cudaFree(g.in_ent0);
-    cudaFree(g.hash);
+    bm_cuda_free(g.out_ptr); bm_cuda_free(g.in_ptr);
+    bm_cuda_free(g.out_ent); bm_cuda_free(g.in_ent);
+    bm_cuda_free(g.self_w);
+    bm_cuda_free(g.out_twin); bm_cuda_free(g.in_twin);
+    bm_cuda_free(g.out_ent0); bm_cuda_free(g.in_ent0);
+    bm_cuda_free(g.hash);
     g = DevGraph();
 }
 
@@ -80,10 +124,19 @@ extern "C" bm_status bm_ctx_create(int device, bm_ctx** out) {
         delete ctx;
         return BM_CUDA_ERROR;
     }
-    if (cudaMalloc(&ctx->d_score, 64) != cudaSuccess) {
+    if (bm_cuda_malloc(&ctx->d_score, 64) != cudaSuccess) {
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return BM_OOM;
+    }
+    // resolves (and so makes resident) the static scratch of the
+    // allocation-free chain entry point on this device
+    const bm_status nst = bm_noalloc_setup(ctx);
+    if (nst != BM_OK) {
+        bm_cuda_free(ctx->d_score);
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return nst;
     }
     *out = ctx;
     return BM_OK;
@@ -95,14 +148,14 @@ extern "C" void bm_ctx_destroy(bm_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     free_graph(ctx->g[0]);
     free_graph(ctx->g[1]);
-    cudaFree(ctx->pi); cudaFree(ctx->pinv); cudaFree(ctx->ov);
-    cudaFree(ctx->d_score);
-    cudaFree(ctx->stage);
-    cudaFree(ctx->flush_buf);
-    cudaFree(ctx->tscr);
-    cudaFree(ctx->rwork); cudaFree(ctx->spart); cudaFree(ctx->scnt); cudaFree(ctx->rpart); cudaFree(ctx->slots);
-    if (ctx->hstage) cudaFreeHost(ctx->hstage);
-    if (ctx->h_slots) cudaFreeHost(ctx->h_slots);
+    bm_cuda_free(ctx->pi); bm_cuda_free(ctx->pinv); bm_cuda_free(ctx->ov);
+    bm_cuda_free(ctx->d_score);
+    bm_cuda_free(ctx->stage);
+    bm_cuda_free(ctx->flush_buf);
+    bm_cuda_free(ctx->tscr);
+    bm_cuda_free(ctx->rwork); bm_cuda_free(ctx->spart); bm_cuda_free(ctx->scnt); bm_cuda_free(ctx->rpart); bm_cuda_free(ctx->slots);
+    if (ctx->hstage) bm_cuda_host_free(ctx->hstage);
+    if (ctx->h_slots) bm_cuda_host_free(ctx->h_slots);
     if (ctx->slots_ev) cudaEventDestroy(ctx->slots_ev);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -127,11 +180,11 @@ extern "C" bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len) {
 bm_status bm_stage(bm_ctx* ctx, size_t bytes) {
     if (ctx->stage_bytes >= bytes) return BM_OK;
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    cudaFree(ctx->stage);
+    bm_cuda_free(ctx->stage);
     ctx->stage = nullptr;
     ctx->stage_bytes = 0;
     size_t sz = bytes < (1u << 20) ? (1u << 20) : bytes;
-    BM_CUDA(ctx, cudaMalloc(&ctx->stage, sz));
+    BM_CUDA(ctx, bm_cuda_malloc(&ctx->stage, sz));
     ctx->stage_bytes = sz;
     return BM_OK;
 }
@@ -139,11 +192,11 @@ bm_status bm_stage(bm_ctx* ctx, size_t bytes) {
 bm_status bm_hstage(bm_ctx* ctx, size_t bytes) {
     if (ctx->hstage_bytes >= bytes) return BM_OK;
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (ctx->hstage) cudaFreeHost(ctx->hstage);
+    if (ctx->hstage) bm_cuda_host_free(ctx->hstage);
     ctx->hstage = nullptr;
     ctx->hstage_bytes = 0;
     size_t sz = bytes < (1u << 20) ? (1u << 20) : bytes;
-    BM_CUDA(ctx, cudaMallocHost(&ctx->hstage, sz));
+    BM_CUDA(ctx, bm_cuda_host_malloc(&ctx->hstage, sz));
     ctx->hstage_bytes = sz;
     return BM_OK;
 }
@@ -161,7 +214,7 @@ bm_status bm_require_mapped(bm_ctx* ctx) {
 template <typename T>
 static bm_status upload(bm_ctx* ctx, T** d, const T* h, size_t count) {
     size_t bytes = sizeof(T) * (count > 0 ? count : 1);
-    BM_CUDA(ctx, cudaMalloc((void**)d, bytes));
+    BM_CUDA(ctx, bm_cuda_malloc((void**)d, bytes));
     if (count > 0) BM_CUDA(ctx, cudaMemcpy(*d, h, sizeof(T) * count, cudaMemcpyHostToDevice));
     return BM_OK;
 }
@@ -250,17 +303,17 @@ extern "C" bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* pi) {
     }
     BM_CUDA(ctx, cudaSetDevice(ctx->device));
     if (!ctx->pi) {
-        BM_CUDA(ctx, cudaMalloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
-        BM_CUDA(ctx, cudaMalloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
-        BM_CUDA(ctx, cudaMalloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
     } else {
         // sizes may have changed with a new graph
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        cudaFree(ctx->pi); cudaFree(ctx->pinv); cudaFree(ctx->ov);
+        bm_cuda_free(ctx->pi); bm_cuda_free(ctx->pinv); bm_cuda_free(ctx->ov);
         ctx->pi = ctx->pinv = ctx->ov = nullptr;
-        BM_CUDA(ctx, cudaMalloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
-        BM_CUDA(ctx, cudaMalloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
-        BM_CUDA(ctx, cudaMalloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
     }
     BM_CUDA(ctx, cudaMemcpyAsync(ctx->pi, h.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
     BM_CUDA(ctx, cudaMemcpyAsync(ctx->pinv, hinv.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
@@ -309,14 +362,14 @@ extern "C" bm_status bm_get_overlap(bm_ctx* ctx, int32_t* ov) {
 extern "C" bm_status bm_dev_alloc(bm_ctx* ctx, int64_t bytes, void** d_ptr) {
     if (!ctx || !d_ptr || bytes < 0) return BM_INVALID_ARG;
     BM_CUDA(ctx, cudaSetDevice(ctx->device));
-    BM_CUDA(ctx, cudaMalloc(d_ptr, (size_t)(bytes > 0 ? bytes : 1)));
+    BM_CUDA(ctx, bm_cuda_malloc(d_ptr, (size_t)(bytes > 0 ? bytes : 1)));
     return BM_OK;
 }
 
 extern "C" bm_status bm_dev_free(bm_ctx* ctx, void* d_ptr) {
     if (!ctx) return BM_INVALID_ARG;
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    BM_CUDA(ctx, cudaFree(d_ptr));
+    BM_CUDA(ctx, bm_cuda_free(d_ptr));
     return BM_OK;
 }
 
@@ -336,13 +389,13 @@ extern "C" bm_status bm_memcpy_d2h(bm_ctx* ctx, void* h_dst, const void* d_src, 
 
 extern "C" bm_status bm_host_alloc_pinned(int64_t bytes, void** h_ptr) {
     if (!h_ptr || bytes < 0) return BM_INVALID_ARG;
-    cudaError_t e = cudaMallocHost(h_ptr, (size_t)(bytes > 0 ? bytes : 1));
+    cudaError_t e = bm_cuda_host_malloc(h_ptr, (size_t)(bytes > 0 ? bytes : 1));
     if (e != cudaSuccess) { cudaGetLastError(); return e == cudaErrorMemoryAllocation ? BM_OOM : BM_CUDA_ERROR; }
     return BM_OK;
 }
 
 extern "C" bm_status bm_host_free_pinned(void* h_ptr) {
-    if (cudaFreeHost(h_ptr) != cudaSuccess) { cudaGetLastError(); return BM_CUDA_ERROR; }
+    if (bm_cuda_host_free(h_ptr) != cudaSuccess) { cudaGetLastError(); return BM_CUDA_ERROR; }
     return BM_OK;
 }
 
@@ -352,10 +405,82 @@ extern "C" bm_status bm_l2_flush(bm_ctx* ctx) {
         int l2 = 0;
         cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device);
         size_t bytes = (size_t)(l2 > 0 ? l2 : (128 << 20)) * 2;
-        BM_CUDA(ctx, cudaMalloc(&ctx->flush_buf, bytes));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->flush_buf, bytes));
         ctx->flush_bytes = bytes;
     }
     BM_CUDA(ctx, cudaMemsetAsync(ctx->flush_buf, ctx->launches & 0xff, ctx->flush_bytes, ctx->stream));
+    return BM_OK;
+}
+
+// L2 read bandwidth: every thread streams 16-byte loads through L2 (ld.cg,
+// not cached in L1) over a buffer smaller than L2, after one pass that makes
+// it resident.  Each block reads a contiguous slice, four loads in flight per
+// thread; the XOR of everything read is stored only if it matches an
+// impossible value, so the loads cannot be removed.
+namespace {
+constexpr int kL2Threads = 512;
+
+__global__ void __launch_bounds__(kL2Threads) l2_read_kernel(const uint4* __restrict__ p, int64_t n4,
+                                                             unsigned* __restrict__ sink) {
+    const int64_t per_block = (n4 + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = per_block * blockIdx.x;
+    const int64_t hi = lo + per_block < n4 ? lo + per_block : n4;
+    unsigned x = 0;
+    int64_t i = lo + threadIdx.x;
+    for (; i + 3 * kL2Threads < hi; i += 4 * kL2Threads) {
+        const uint4 a = __ldcg(p + i), b = __ldcg(p + i + kL2Threads), c = __ldcg(p + i + 2 * kL2Threads),
+                    d = __ldcg(p + i + 3 * kL2Threads);
+        x ^= a.x ^ a.y ^ a.z ^ a.w ^ b.x ^ b.y ^ b.z ^ b.w ^ c.x ^ c.y ^ c.z ^ c.w ^ d.x ^ d.y ^ d.z ^ d.w;
+    }
+    for (; i < hi; i += kL2Threads) {
+        const uint4 a = __ldcg(p + i);
+        x ^= a.x ^ a.y ^ a.z ^ a.w;
+    }
+    if (x == 0x9E3779B9u) sink[threadIdx.x] = x;
+}
+}  // namespace
+
+extern "C" bm_status bm_probe_l2_bandwidth(bm_ctx* ctx, int64_t bytes, int32_t reps, double* gbs) {
+    if (!ctx || !gbs || bytes < (1 << 20) || reps < 1) return BM_INVALID_ARG;
+    int l2 = 0;
+    BM_CUDA(ctx, cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device));
+    if (l2 > 0 && bytes > (int64_t)l2)
+        return bm_fail(ctx, BM_INVALID_ARG, "%lld bytes do not fit the %d-byte L2", (long long)bytes, l2);
+    BM_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int64_t n4 = bytes / 16;
+    void* buf = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bm_status st = BM_OK;
+    float ms = 0.f;
+    auto fail = [&](cudaError_t e, const char* what) {
+        if (st == BM_OK) st = bm_cuda_fail(ctx, e, what);
+    };
+    cudaError_t e = bm_cuda_malloc(&buf, (size_t)n4 * 16 + 4096);
+    if (e != cudaSuccess) return bm_cuda_fail(ctx, e, "cudaMalloc (L2 probe)");
+    unsigned* sink = reinterpret_cast<unsigned*>(static_cast<char*>(buf) + (size_t)n4 * 16);
+    const unsigned blocks = (unsigned)ctx->num_sms * 4;
+    if ((e = cudaMemsetAsync(buf, 1, (size_t)n4 * 16, ctx->stream)) != cudaSuccess) fail(e, "cudaMemsetAsync");
+    if (st == BM_OK && (e = cudaEventCreate(&e0)) != cudaSuccess) fail(e, "cudaEventCreate");
+    if (st == BM_OK && (e = cudaEventCreate(&e1)) != cudaSuccess) fail(e, "cudaEventCreate");
+    if (st == BM_OK) {
+        l2_read_kernel<<<blocks, kL2Threads, 0, ctx->stream>>>(static_cast<const uint4*>(buf), n4, sink);
+        ctx->launches++;
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < reps; r++) {
+            l2_read_kernel<<<blocks, kL2Threads, 0, ctx->stream>>>(static_cast<const uint4*>(buf), n4, sink);
+            ctx->launches++;
+        }
+        cudaEventRecord(e1, ctx->stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) fail(e, "l2_read_kernel");
+        else if ((e = cudaEventSynchronize(e1)) != cudaSuccess) fail(e, "cudaEventSynchronize");
+        else if ((e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) fail(e, "cudaEventElapsedTime");
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(ctx->stream);
+    bm_cuda_free(buf);
+    if (st != BM_OK) return st;
+    *gbs = (double)n4 * 16.0 * reps / (ms / 1e3) / 1e9;
     return BM_OK;
 }
 
@@ -394,6 +519,13 @@ extern "C" bm_status bm_set_row_tiling(bm_ctx* ctx, int32_t ctas_per_row, int32_
         return bm_fail(ctx, BM_INVALID_ARG, "threads must be 256 or 512");
     if (ctas_per_row) ctx->row_ctas = ctas_per_row;
     if (threads) ctx->row_threads = threads;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_set_wait_limit(bm_ctx* ctx, int64_t cycles) {
+    if (!ctx) return BM_INVALID_ARG;
+    if (cycles < 0) return bm_fail(ctx, BM_INVALID_ARG, "the wait bound must be >= 0 cycles (0: defaults)");
+    ctx->wait_limit = cycles;
     return BM_OK;
 }
 

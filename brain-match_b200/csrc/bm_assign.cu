@@ -36,9 +36,12 @@ constexpr int kLapMaxK = 4096;
 constexpr int kLapIdBits = 13;  // person index in a bid key (k <= 4096 < 2^13)
 constexpr int kPermThreads = 256;
 
-// Bounded auction: ~10 s of SM clock at most; status 1 means it ran out.
+// Bounded auction: `limit` SM clock cycles at most (by default kAuctionLimit,
+// ~10 s); status 1 means it ran out.
+constexpr long long kAuctionLimit = 20000000000ll;
 __global__ void __launch_bounds__(kLapThreads) auction_kernel(const int32_t* __restrict__ a, int32_t k, long long eps0,
-                                                              int32_t* __restrict__ assign, int32_t* __restrict__ status) {
+                                                              int32_t* __restrict__ assign, int32_t* __restrict__ status,
+                                                              long long limit) {
     extern __shared__ unsigned long long lsm[];
     long long* price = reinterpret_cast<long long*>(lsm);
     unsigned long long* bid = lsm + k;
@@ -62,7 +65,7 @@ __global__ void __launch_bounds__(kLapThreads) auction_kernel(const int32_t* __r
             for (int32_t i = tid; i < k; i += kLapThreads)
                 if (pobj[i] < 0) ulist[atomicAdd(&s_nu, 1)] = i;
             for (int32_t j = tid; j < k; j += kLapThreads) bid[j] = 0ull;
-            if (tid == 0 && clock64() - t0 > 20000000000ll) s_fail = 1;
+            if (tid == 0 && clock64() - t0 > limit) s_fail = 1;
             __syncthreads();
             const int32_t nu = s_nu;
             if (nu == 0 || s_fail) break;
@@ -189,7 +192,9 @@ bm_status lap_device(bm_ctx* ctx, const int32_t* d_a, int32_t k, int32_t* d_assi
     BM_CUDA(ctx, cudaFuncSetAttribute(auction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long c = std::max(1ll, max_abs) * ((long long)k + 1);
     const long long eps0 = std::max(1ll, c / 5);
-    auction_kernel<<<1, kLapThreads, smem, ctx->stream>>>(d_a, k, eps0, d_assign, d_status);
+    auction_kernel<<<1, kLapThreads, smem, ctx->stream>>>(d_a, k, eps0, d_assign, d_status,
+                                                          ctx->wait_limit > 0 ? (long long)ctx->wait_limit
+                                                                              : kAuctionLimit);
     BM_LAUNCH_CHECK(ctx, "auction_kernel");
     return BM_OK;
 }

@@ -141,11 +141,11 @@ void build_adj(int32_t n, int64_t m, const int32_t* from, const int32_t* to, std
 
 struct DevBuf {
     std::vector<void*> p;
-    ~DevBuf() { for (void* x : p) cudaFree(x); }
+    ~DevBuf() { for (void* x : p) bm_cuda_free(x); }
     template <typename T>
     bool get(T** out, size_t count) {
         void* d = nullptr;
-        if (cudaMalloc(&d, sizeof(T) * std::max<size_t>(count, 1)) != cudaSuccess) {
+        if (bm_cuda_malloc(&d, sizeof(T) * std::max<size_t>(count, 1)) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }

@@ -110,8 +110,33 @@ struct bm_ctx {
     // host copy of A's adjacency (independence tests of batched swaps)
     std::vector<int32_t> hA_optr, hA_iptr;
     std::vector<uint32_t> hA_oent, hA_ient;
+    // device address of the allocation-free chain entry point's static
+    // scratch on this context's device (bm_noalloc_setup, at creation)
+    unsigned char* noalloc_scratch = nullptr;
+    // bound of the device-side waits (MMA completions of the tensor-core
+    // scorer, the auction), SM clock cycles; 0 = each kernel's default
+    int64_t wait_limit = 0;
     std::string err;
 };
+
+// Every device and pinned-host allocation or release the library makes goes
+// through these wrappers, which count the calls (bm_alloc_count), so a test
+// can show that an entry point allocates nothing.
+cudaError_t bm_cuda_malloc_raw(void** p, size_t bytes);
+cudaError_t bm_cuda_free(void* p);
+cudaError_t bm_cuda_host_malloc_raw(void** p, size_t bytes);
+cudaError_t bm_cuda_host_alloc(void** p, size_t bytes, unsigned flags);
+cudaError_t bm_cuda_host_free(void* p);
+template <class T>
+inline cudaError_t bm_cuda_malloc(T** p, size_t bytes) { return bm_cuda_malloc_raw(reinterpret_cast<void**>(p), bytes); }
+template <class T>
+inline cudaError_t bm_cuda_host_malloc(T** p, size_t bytes) { return bm_cuda_host_malloc_raw(reinterpret_cast<void**>(p), bytes); }
+
+// Look up the device address of the static scratch of bm_sa_run_noalloc on
+// ctx's device (current) and keep it in the context.  Run once by
+// bm_ctx_create: the lookup loads the module holding the array, the only step
+// of that entry point that can reserve device memory.
+bm_status bm_noalloc_setup(bm_ctx* ctx);
 
 // Set the error string and return a status.
 bm_status bm_fail(bm_ctx* ctx, bm_status s, const char* fmt, ...);

@@ -667,10 +667,13 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
 
 // Bounded wait for phase `parity` of an mbarrier: try_wait suspends the thread
 // until the phase completes or a hardware time slice passes; the loop gives up
-// after about two seconds of SM clock and returns false.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+// once `limit` SM clock cycles (by default kWaitLimit, about two seconds) have
+// passed, checked before every try, and returns false.
+constexpr long long kWaitLimit = 4000000000ll;
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit = kWaitLimit) {
     const long long t0 = clock64();
     for (;;) {
+        if (clock64() - t0 >= limit) return false;
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -680,7 +683,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
             : "r"(mbar), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > 4000000000ll) return false;
     }
 }
 
@@ -727,6 +729,7 @@ struct TcArgs {
     const int32_t* pi;
     float* scores;  // [nrows x n], row r at r * n, partner v at v - 1
     int32_t* flag;
+    long long wait_limit;  // bound of each MMA-completion wait, SM cycles
 };
 
 // Hidden-layer epilogue: this thread's accumulator row (128 FP32 columns at
@@ -873,7 +876,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
         for (int32_t v0 = 1; v0 <= a.n; v0 += 128) {
             const int32_t v = v0 + tid;
             // layer 1 done: its epilogue fills H with h1
-            if (!__syncthreads_and(mbar_wait(bar1, phase))) { ok = false; break; }
+            if (!__syncthreads_and(mbar_wait(bar1, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
             hidden_epilogue(tm_1, ep, sm, tid);
             tc_handoff();
@@ -895,7 +898,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
                 issue_layer1(phase ^ 1u);
             }
             // layer 2 done: its epilogue writes h2 over h1
-            if (!__syncthreads_and(mbar_wait(bar2, phase))) { ok = false; break; }
+            if (!__syncthreads_and(mbar_wait(bar2, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
             hidden_epilogue(tm_2, ep + 128, sm, tid);
             tc_handoff();
@@ -908,7 +911,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
             }
             last_bar = bar3;
             last_par = phase;
-            if (!__syncthreads_and(mbar_wait(bar3, phase))) { ok = false; break; }
+            if (!__syncthreads_and(mbar_wait(bar3, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
             const float o = tmem_ld1(tm_2);
             if (v <= a.n) out_row[v - 1] = (v != u) ? o + ep[384] : -INFINITY;
@@ -922,7 +925,9 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
-        if (!ok) mbar_wait(last_bar, last_par);  // let the MMAs in flight finish before the columns are freed
+        // let the MMAs in flight finish before the columns are freed (the
+        // default bound, whatever bound the waits above were given)
+        if (!ok) mbar_wait(last_bar, last_par);
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
     }
@@ -1089,10 +1094,10 @@ bm_status check_ids(bm_ctx* ctx, const int32_t* ids, int64_t cnt, const char* wh
 
 bm_status scratch(bm_mlp* M, size_t bytes) {
     if (bytes <= M->scr_bytes) return BM_OK;
-    cudaFree(M->d_scr);
+    bm_cuda_free(M->d_scr);
     M->d_scr = nullptr;
     M->scr_bytes = 0;
-    if (cudaMalloc(&M->d_scr, bytes) != cudaSuccess) {
+    if (bm_cuda_malloc(&M->d_scr, bytes) != cudaSuccess) {
         cudaGetLastError();
         return bm_fail(M->ctx, BM_OOM, "model scratch of %zu bytes", bytes);
     }
@@ -1146,10 +1151,10 @@ bm_status launch_row_scores(bm_mlp* M, const int32_t* d_rows, int32_t nrows) {
     bm_ctx* ctx = M->ctx;
     const size_t need = (size_t)nrows * (size_t)M->n;
     if (need > M->sc_cap) {
-        cudaFree(M->d_sc);
+        bm_cuda_free(M->d_sc);
         M->d_sc = nullptr;
         M->sc_cap = 0;
-        if (cudaMalloc(&M->d_sc, sizeof(float) * need) != cudaSuccess) {
+        if (bm_cuda_malloc(&M->d_sc, sizeof(float) * need) != cudaSuccess) {
             cudaGetLastError();
             return bm_fail(ctx, BM_OOM, "row score buffer of %zu floats", need);
         }
@@ -1166,7 +1171,7 @@ bm_status launch_row_scores(bm_mlp* M, const int32_t* d_rows, int32_t nrows) {
     }
     const DevGraph& B = ctx->g[1];
     TcArgs a{M->d_img, M->d_tab, d_rows, nrows, M->n, B.out_ptr, B.out_ent, B.in_ptr, B.in_ent, ctx->pi, M->d_sc,
-             M->d_flag};
+             M->d_flag, ctx->wait_limit > 0 ? (long long)ctx->wait_limit : kWaitLimit};
     const int grid = std::min(nrows, 2 * ctx->num_sms);
     mlp_rows_tc_kernel<<<grid, kTcThreads, tc_launch_smem(M->n), ctx->stream>>>(a);
     BM_LAUNCH_CHECK(ctx, "mlp_rows_tc_kernel");
@@ -1197,11 +1202,11 @@ bm_status ensure_records(bm_mlp* M, int64_t cap) {
     bm_ctx* ctx = M->ctx;
     uint16_t* nx = nullptr;
     float* ny = nullptr;
-    if (cudaMalloc(&nx, sizeof(uint16_t) * BM_MLP_IN * (size_t)cap) != cudaSuccess ||
-        cudaMalloc(&ny, sizeof(float) * (size_t)cap) != cudaSuccess) {
+    if (bm_cuda_malloc(&nx, sizeof(uint16_t) * BM_MLP_IN * (size_t)cap) != cudaSuccess ||
+        bm_cuda_malloc(&ny, sizeof(float) * (size_t)cap) != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(nx);
-        cudaFree(ny);
+        bm_cuda_free(nx);
+        bm_cuda_free(ny);
         return bm_fail(ctx, BM_OOM, "record store of %lld records", (long long)cap);
     }
     // keep the existing records in ring order, oldest first
@@ -1219,8 +1224,8 @@ bm_status ensure_records(bm_mlp* M, int64_t cap) {
         }
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
-    cudaFree(M->d_rx);
-    cudaFree(M->d_ry);
+    bm_cuda_free(M->d_rx);
+    bm_cuda_free(M->d_ry);
     M->d_rx = nx;
     M->d_ry = ny;
     M->rhead = M->rsize;
@@ -1256,13 +1261,13 @@ bm_status fit_steps(bm_mlp* M, int32_t steps, int32_t batch, float lr, float wd,
     bm_ctx* ctx = M->ctx;
     if (M->rsize == 0) return bm_fail(ctx, BM_INVALID_ARG, "no training records collected");
     if (batch > M->bcap) {
-        cudaFree(M->d_bx);
-        cudaFree(M->d_by);
+        bm_cuda_free(M->d_bx);
+        bm_cuda_free(M->d_by);
         M->d_bx = nullptr;
         M->d_by = nullptr;
         M->bcap = 0;
-        if (cudaMalloc(&M->d_bx, sizeof(uint16_t) * BM_MLP_IN * (size_t)batch) != cudaSuccess ||
-            cudaMalloc(&M->d_by, sizeof(float) * (size_t)batch) != cudaSuccess) {
+        if (bm_cuda_malloc(&M->d_bx, sizeof(uint16_t) * BM_MLP_IN * (size_t)batch) != cudaSuccess ||
+            bm_cuda_malloc(&M->d_by, sizeof(float) * (size_t)batch) != cudaSuccess) {
             cudaGetLastError();
             return bm_fail(ctx, BM_OOM, "minibatch of %d records", batch);
         }
@@ -1295,9 +1300,9 @@ extern "C" void bm_mlp_destroy(bm_mlp* M) {
     // the context may already be gone: synchronise the device, not its stream
     cudaSetDevice(M->device);
     cudaDeviceSynchronize();
-    cudaFree(M->d_w); cudaFree(M->d_m); cudaFree(M->d_v); cudaFree(M->d_g); cudaFree(M->d_loss);
-    cudaFree(M->d_tab); cudaFree(M->d_bdeg); cudaFree(M->d_img); cudaFree(M->d_sc); cudaFree(M->d_flag);
-    cudaFree(M->d_rx); cudaFree(M->d_ry); cudaFree(M->d_bx); cudaFree(M->d_by); cudaFree(M->d_scr);
+    bm_cuda_free(M->d_w); bm_cuda_free(M->d_m); bm_cuda_free(M->d_v); bm_cuda_free(M->d_g); bm_cuda_free(M->d_loss);
+    bm_cuda_free(M->d_tab); bm_cuda_free(M->d_bdeg); bm_cuda_free(M->d_img); bm_cuda_free(M->d_sc); bm_cuda_free(M->d_flag);
+    bm_cuda_free(M->d_rx); bm_cuda_free(M->d_ry); bm_cuda_free(M->d_bx); bm_cuda_free(M->d_by); bm_cuda_free(M->d_scr);
     delete M;
 }
 
@@ -1328,10 +1333,10 @@ extern "C" bm_status bm_mlp_create(bm_ctx* ctx, uint64_t seed, bm_mlp** out) {
     init(kOffW3, BM_MLP_H, 1, BM_MLP_H);
     const size_t pb = sizeof(float) * (size_t)kNParams;
     const size_t tb = sizeof(float) * ((size_t)ctx->n + 1) * BM_FT;
-    if (cudaMalloc(&M->d_w, pb) || cudaMalloc(&M->d_m, pb) || cudaMalloc(&M->d_v, pb) || cudaMalloc(&M->d_g, pb) ||
-        cudaMalloc(&M->d_loss, 256) || cudaMalloc(&M->d_tab, tb) ||
-        cudaMalloc(&M->d_bdeg, sizeof(float2) * ((size_t)ctx->n + 1)) || cudaMalloc(&M->d_img, kImgBytes) ||
-        cudaMalloc(&M->d_flag, 256)) {
+    if (bm_cuda_malloc(&M->d_w, pb) || bm_cuda_malloc(&M->d_m, pb) || bm_cuda_malloc(&M->d_v, pb) || bm_cuda_malloc(&M->d_g, pb) ||
+        bm_cuda_malloc(&M->d_loss, 256) || bm_cuda_malloc(&M->d_tab, tb) ||
+        bm_cuda_malloc(&M->d_bdeg, sizeof(float2) * ((size_t)ctx->n + 1)) || bm_cuda_malloc(&M->d_img, kImgBytes) ||
+        bm_cuda_malloc(&M->d_flag, 256)) {
         cudaGetLastError();
         bm_mlp_destroy(M);
         return bm_fail(ctx, BM_OOM, "bm_mlp_create: device allocation failed");

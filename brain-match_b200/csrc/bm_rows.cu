@@ -750,18 +750,18 @@ bm_status bm_rows_prepare(bm_ctx* ctx) {
     const int32_t smax = 2 * ctx->num_sms;
     if (ctx->split_n != ctx->n || ctx->split_slots_max != smax) {
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        cudaFree(ctx->rwork); cudaFree(ctx->spart); cudaFree(ctx->scnt); cudaFree(ctx->rpart); cudaFree(ctx->slots);
+        bm_cuda_free(ctx->rwork); bm_cuda_free(ctx->spart); bm_cuda_free(ctx->scnt); bm_cuda_free(ctx->rpart); bm_cuda_free(ctx->slots);
         ctx->rwork = nullptr; ctx->spart = nullptr; ctx->scnt = nullptr; ctx->rpart = nullptr; ctx->rcnt = nullptr;
         ctx->slots = nullptr;
         ctx->split_n = 0;
-        BM_CUDA(ctx, cudaMalloc(&ctx->rwork, sizeof(int32_t) * (size_t)ctx->nvec));
-        BM_CUDA(ctx, cudaMalloc(&ctx->spart, sizeof(int32_t) * (size_t)ctx->nvec * (size_t)smax));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->rwork, sizeof(int32_t) * (size_t)ctx->nvec));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->spart, sizeof(int32_t) * (size_t)ctx->nvec * (size_t)smax));
         const size_t cnt_bytes = sizeof(unsigned) * (size_t)smax * (kMaxCluster + 1);
-        BM_CUDA(ctx, cudaMalloc(&ctx->scnt, cnt_bytes));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->scnt, cnt_bytes));
         ctx->rcnt = ctx->scnt + (size_t)smax * kMaxCluster;
-        BM_CUDA(ctx, cudaMalloc(&ctx->rpart, sizeof(Partial) * (size_t)smax * kMaxCluster));
-        BM_CUDA(ctx, cudaMalloc(&ctx->slots, sizeof(int4) * (size_t)smax));
-        if (!ctx->h_slots) BM_CUDA(ctx, cudaHostAlloc((void**)&ctx->h_slots, sizeof(int4) * (size_t)2 * ctx->num_sms,
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->rpart, sizeof(Partial) * (size_t)smax * kMaxCluster));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->slots, sizeof(int4) * (size_t)smax));
+        if (!ctx->h_slots) BM_CUDA(ctx, bm_cuda_host_alloc((void**)&ctx->h_slots, sizeof(int4) * (size_t)2 * ctx->num_sms,
                                                       cudaHostAllocDefault));
         if (!ctx->slots_ev) BM_CUDA(ctx, cudaEventCreateWithFlags(&ctx->slots_ev, cudaEventDisableTiming));
         BM_CUDA(ctx, cudaMemsetAsync(ctx->scnt, 0, cnt_bytes, ctx->stream));

@@ -23,7 +23,6 @@
 // finish.
 #include <algorithm>
 #include <chrono>
-#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -472,9 +471,9 @@ static PairDev pair_dev(const bm_batch::Pair& p) {
 }
 
 static void free_pair(bm_batch::Pair& p) {
-    for (auto* x : p.d) cudaFree(x);
-    for (auto* x : p.e) cudaFree(x);
-    cudaFree(p.hash);
+    for (auto* x : p.d) bm_cuda_free(x);
+    for (auto* x : p.e) bm_cuda_free(x);
+    bm_cuda_free(p.hash);
     p = bm_batch::Pair();
 }
 
@@ -492,13 +491,13 @@ extern "C" void bm_batch_destroy(bm_batch* b) {
     cudaSetDevice(b->device);
     cudaDeviceSynchronize();
     for (auto& p : b->pairs) free_pair(p);
-    cudaFree(b->d_pairs);
+    bm_cuda_free(b->d_pairs);
     delete b;
 }
 
 template <typename T>
 static bm_status up(bm_ctx* ctx, T** d, const std::vector<T>& h) {
-    BM_CUDA(ctx, cudaMalloc((void**)d, sizeof(T) * (h.empty() ? 1 : h.size())));
+    BM_CUDA(ctx, bm_cuda_malloc((void**)d, sizeof(T) * (h.empty() ? 1 : h.size())));
     if (!h.empty()) BM_CUDA(ctx, cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
     return BM_OK;
 }
@@ -631,9 +630,9 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
             const auto& p = b->pairs[(size_t)i];
             hp[(size_t)i] = pair_dev(p);
         }
-        cudaFree(b->d_pairs);
+        bm_cuda_free(b->d_pairs);
         b->d_pairs = nullptr;
-        BM_CUDA(ctx, cudaMalloc(&b->d_pairs, sizeof(PairDev) * (size_t)np));
+        BM_CUDA(ctx, bm_cuda_malloc(&b->d_pairs, sizeof(PairDev) * (size_t)np));
         BM_CUDA(ctx, cudaMemcpy(b->d_pairs, hp.data(), sizeof(PairDev) * (size_t)np, cudaMemcpyHostToDevice));
         b->dirty = false;
     }
@@ -642,12 +641,12 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
     int32_t* d_pi = nullptr;
     int32_t* d_ov = nullptr;
     ChainDev* d_ch = nullptr;
-    BM_CUDA(ctx, cudaMalloc(&d_pi, sizeof(int32_t) * (size_t)tot));
-    BM_CUDA(ctx, cudaMalloc(&d_ov, sizeof(int32_t) * (size_t)tot));
-    BM_CUDA(ctx, cudaMalloc(&d_ch, sizeof(ChainDev) * (size_t)nchains));
+    BM_CUDA(ctx, bm_cuda_malloc(&d_pi, sizeof(int32_t) * (size_t)tot));
+    BM_CUDA(ctx, bm_cuda_malloc(&d_ov, sizeof(int32_t) * (size_t)tot));
+    BM_CUDA(ctx, bm_cuda_malloc(&d_ch, sizeof(ChainDev) * (size_t)nchains));
     struct Guard {
         void* p[3];
-        ~Guard() { for (void* x : p) cudaFree(x); }
+        ~Guard() { for (void* x : p) bm_cuda_free(x); }
     } guard{{d_pi, d_ov, d_ch}};
     BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
     BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
@@ -785,14 +784,18 @@ extern "C" int64_t bm_sa_layout_size(bm_batch* b, int32_t nchains, const int32_t
 // device-wide synchronisation of cudaFree while other streams are busy.
 //
 // Its scratch is the file-scope array below: the pair table, the chain states,
-// and every chain's mapping and per-vertex overlap.  Every GPU that loads this
-// library holds the array until the process exits.  Host code must not use the
-// symbol's name as a device address; the address is obtained once per device
-// with cudaGetSymbolAddress (first call on that device, with the device
-// current) and passed to the kernels.  All calls share the array and it keeps
-// the last call's contents, so each call rewrites what it reads and clears the
-// overlap arrays; calls whose work overlaps on the GPU (two host threads, or
-// two contexts on one device) race and must be serialised by the caller.
+// and every chain's mapping and per-vertex overlap.  Host code must not use the
+// symbol's name as a device address: bm_ctx_create looks the address up with
+// cudaGetSymbolAddress, with the context's device current, and keeps it in the
+// context.  That lookup loads the module that holds the array (the runtime
+// loads modules lazily), so the array is reserved on a device when the first
+// context on it is created and stays reserved until the process exits; the
+// entry point itself never reserves it.  A device reset (cudaDeviceReset)
+// unloads the module and invalidates every context on the device: create a new
+// context after one.  All calls share the array and it keeps the last call's
+// contents, so each call rewrites what it reads and clears the overlap arrays;
+// calls whose work overlaps on the GPU (two host threads, or two contexts on
+// one device) race and must be serialised by the caller.
 
 namespace {
 
@@ -812,20 +815,16 @@ static_assert(sizeof(ChainDev) <= kNoAllocChainBytes, "chain slot too small");
 
 static __device__ __align__(256) unsigned char g_sa_noalloc_scratch[kNoAllocBytes];
 
-static std::mutex g_noalloc_mu;
-static unsigned char* g_noalloc_addr[64] = {nullptr};
-
-// Device address of the scratch array on ctx's device (set up on first use).
-static bm_status noalloc_scratch(bm_ctx* ctx, unsigned char** out) {
-    if (ctx->device < 0 || ctx->device >= 64) return bm_fail(ctx, BM_UNSUPPORTED, "device ordinal above 63");
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[ctx->device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_sa_noalloc_scratch);
-        if (e != cudaSuccess) return bm_cuda_fail(ctx, e, "cudaGetSymbolAddress(g_sa_noalloc_scratch)");
-        g_noalloc_addr[ctx->device] = static_cast<unsigned char*>(p);
-    }
-    *out = g_noalloc_addr[ctx->device];
+bm_status bm_noalloc_setup(bm_ctx* ctx) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sa_noalloc_scratch);
+    if (e != cudaSuccess) return bm_cuda_fail(ctx, e, "cudaGetSymbolAddress(g_sa_noalloc_scratch)");
+    ctx->noalloc_scratch = static_cast<unsigned char*>(p);
+    // the runtime also loads each kernel's code on its first use: load the
+    // entry point's two kernels here, so its first call loads nothing
+    cudaFuncAttributes fa;
+    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_init_kernel));
+    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel));
     return BM_OK;
 }
 
@@ -875,9 +874,9 @@ extern "C" bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32
     if (K < 1 || K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates must be 0 or 1..%d", kmax);
     int32_t n_max = 0;
     for (int32_t c = 0; c < nchains; c++) n_max = std::max(n_max, b->pairs[(size_t)chain_pair[c]].n);
-    unsigned char* base = nullptr;
-    bm_status st = noalloc_scratch(ctx, &base);
-    if (st != BM_OK) return st;
+    unsigned char* base = ctx->noalloc_scratch;  // resolved when the context was created
+    if (!base) return bm_fail(ctx, BM_CUDA_ERROR, "the context holds no address of the static scratch");
+    bm_status st = BM_OK;
     PairDev* d_pairs = reinterpret_cast<PairDev*>(base);
     ChainDev* d_ch = reinterpret_cast<ChainDev*>(base + kNoAllocOffChains);
     int32_t* d_pi = reinterpret_cast<int32_t*>(base + kNoAllocOffPi);

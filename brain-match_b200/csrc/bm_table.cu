@@ -353,10 +353,10 @@ bm_status top_scratch(bm_ctx* ctx, TopScratch* s, void** base_out) {
                  b_blk = al256(sizeof(int32_t) * ((size_t)ctx->n + 2)), b_sel = al256(sizeof(int32_t) * kTopMax);
     const size_t total = b_st + b_h + b_blk + 3 * b_sel;
     if (ctx->tscr_bytes < total) {
-        cudaFree(ctx->tscr);
+        bm_cuda_free(ctx->tscr);
         ctx->tscr = nullptr;
         ctx->tscr_bytes = 0;
-        if (cudaMalloc(&ctx->tscr, total) != cudaSuccess) {
+        if (bm_cuda_malloc(&ctx->tscr, total) != cudaSuccess) {
             cudaGetLastError();
             return bm_fail(ctx, BM_OOM, "top-K scratch");
         }

@@ -142,6 +142,10 @@ def cuda_lib() -> C.CDLL:
             "bm_host_alloc_pinned": (C.c_int, [C.c_int64, C.POINTER(vp)]),
             "bm_host_free_pinned": (C.c_int, [vp]),
             "bm_l2_flush": (C.c_int, [vp]),
+            "bm_alloc_count": (C.c_uint64, []),
+            "bm_set_wait_limit": (C.c_int, [vp, C.c_int64]),
+            "bm_probe_l2_bandwidth": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double)]),
+            "bm_device_memory": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
             "bm_event_create": (C.c_int, [vp, C.POINTER(vp)]),
             "bm_event_destroy": (C.c_int, [vp, vp]),
             "bm_event_record": (C.c_int, [vp, vp]),
@@ -717,6 +721,9 @@ class Engine:
 
     def rows_best_dev(self, d_rows: int, d_col: int | None, nrows: int, d_out: int) -> None:
         self._chk(self.L.bm_rows_best_dev(self.h, d_rows, d_col, nrows, d_out), "bm_rows_best_dev")
+
+    def kset_eval_dev(self, k: int, d_sets: int, nsets: int, d_best: int, d_perm: int, d_status: int) -> None:
+        self._chk(self.L.bm_kset_eval_dev(self.h, k, d_sets, nsets, d_best, d_perm, d_status), "bm_kset_eval_dev")
 
     def delta_rows_dev(self, d_rows: int, nrows: int, d_out: int) -> None:
         self._chk(self.L.bm_delta_rows_dev(self.h, d_rows, nrows, d_out), "bm_delta_rows_dev")

@@ -294,14 +294,18 @@ int64_t bm_sa_layout_size(bm_batch* b, int32_t nchains, const int32_t* chain_pai
  * under a fixed budget, or a serving path that must not take cudaFree's
  * device-wide synchronisation).  The batch itself is built beforehand with
  * bm_batch_add_pair, which does allocate.  All scratch lives in one static
- * device array of 8,486,912 bytes that every GPU loading the library holds
- * until exit; it limits a call to 256 pairs, 1,024 chains and a total of
- * 2^20 mapping entries (sum over chains of n + 1); larger requests return
- * BM_INVALID_ARG.  The first call on a device looks up the array's device
- * address and should come before any stream capture on that device.  Calls
- * share the array: calls that overlap on the GPU race and must be serialised
- * by the caller.  candidates == 0 uses 8 (no autotuning: the tuner would
- * allocate).  Arguments and outputs as bm_sa_run, without stats. */
+ * device array of 8,486,912 bytes.  bm_ctx_create looks up its device address
+ * (which loads the module holding it), so the array is reserved on a device
+ * when the first context on it is created and held until the process exits;
+ * the entry point itself reserves nothing, on its first call too
+ * (bm_alloc_count does not move).  A device reset invalidates the contexts
+ * on the device; create a new one after it.  The array limits a call to 256
+ * pairs, 1,024 chains and a total of 2^20 mapping entries (sum over chains
+ * of n + 1); larger requests return BM_INVALID_ARG.  Calls share the array
+ * and it keeps the last call's contents: calls that overlap on the GPU race
+ * and must be serialised by the caller.  candidates == 0 uses 8 (no
+ * autotuning: the tuner would allocate).  Arguments and outputs as
+ * bm_sa_run, without stats. */
 bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32_t* chain_pair, const uint64_t* chain_key,
                             const int32_t* init_pi, const bm_sa_params* params, int32_t* final_pi,
                             int64_t* final_score, int64_t* accepts);
@@ -497,6 +501,28 @@ bm_status bm_event_elapsed_ms(bm_ctx* ctx, void* ev_start, void* ev_stop, float*
 int64_t bm_launch_count(const bm_ctx* ctx);
 /* PCI bus id of the context's device ("0000:1b:00.0"), for NVML queries. */
 bm_status bm_device_pci_bus_id(bm_ctx* ctx, char* buf, int32_t len);
+/* Device and pinned-host allocations and releases (cudaMalloc, cudaFree,
+ * cudaMallocHost, cudaHostAlloc, cudaFreeHost) the library has made in this
+ * process, over all contexts.  A diagnostic: an entry point that allocates
+ * nothing leaves it unchanged. */
+uint64_t bm_alloc_count(void);
+/* L2 read bandwidth of the context's device in GB/s: a read kernel streams a
+ * buffer of `bytes` (1 MiB .. the L2 size) through L2 `reps` times after one
+ * pass that makes it resident, timed with CUDA events.  The roofline
+ * denominator of kernels whose working set stays in L2; no reference
+ * counterpart (a measurement utility). */
+bm_status bm_probe_l2_bandwidth(bm_ctx* ctx, int64_t bytes, int32_t reps, double* gbs);
+/* Bound, in SM clock cycles, of the context's device-side waits: each
+ * MMA-completion wait of the tensor-core MLP scorer (default 4e9, about two
+ * seconds) and the auction of bm_lap_solve / bm_subset_assign (default 2e10).
+ * 0 restores the defaults.  A wait that runs out makes its call return
+ * BM_TIMEOUT and leaves the context usable: the scorer sets an error flag,
+ * waits (with the default bound) for the MMAs it issued, frees its tensor
+ * memory and returns; the flag is cleared when it is reported.  A testing and
+ * diagnosis aid; the reference has no counterpart (its kernels do not wait). */
+bm_status bm_set_wait_limit(bm_ctx* ctx, int64_t cycles);
+/* Free and total memory of the context's device (cudaMemGetInfo). */
+bm_status bm_device_memory(bm_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
 
 /* Delta semantics of pairwise swaps.  BM_SEMANTICS_EXACT (default): the
  * score difference.  BM_SEMANTICS_REF_CPU: the value calculate_swap_delta

@@ -8,6 +8,9 @@ Run in a checkout where the reference sources are present:
 
 Each fixture holds the graph pair itself (so it does not depend on the
 generator staying unchanged), the mappings, and the reference's outputs.
+golden_greedy.npz is the exception: its pairs are too large to store, so it
+holds their generator parameters and edge checksums beside the matchings the
+reference's greedy-match binary (oracle/_ref/greedy-match) wrote for them.
 """
 from __future__ import annotations
 
@@ -209,7 +212,50 @@ CASES = {
     "golden_selfloop.npz": lambda: make_selfloop_case("golden_selfloop.npz"),
     "golden_selfloop_ref.npz": lambda: make_selfloop_ref_case("golden_selfloop_ref.npz"),
     "golden_simfilter.npz": lambda: make_simfilter_case("golden_simfilter.npz"),
+    "golden_greedy.npz": lambda: make_greedy_case("golden_greedy.npz"),
 }
+
+
+GREEDY_REF = os.path.join(REPO, "oracle", "_ref", "greedy-match")
+# (config, seed, n, edges): generated pairs on which the reference's
+# greedy-match runs in seconds to minutes (its loader and 2-hop counts are
+# quadratic); every vertex has an edge, so its node list is 1..n
+GREEDY_CASES = ((1, 7, 3000, 60000), (3, 9, 2500, 200000), (2, 5, 4000, 640000))
+
+
+def edge_digest(g):
+    """A checksum of an edge list, so a test notices a changed generator."""
+    h = (g.src.astype(np.uint64) * np.uint64(1000003) + g.dst.astype(np.uint64)) * np.uint64(65599) \
+        + g.w.astype(np.uint64)
+    return np.uint64(np.bitwise_xor.reduce(h * np.uint64(0x9E3779B97F4A7C15)))
+
+
+def run_ref_greedy(A, B, workdir):
+    """The reference's greedy-match binary on A and B written as its CSV input;
+    returns its matching as a 1-indexed array."""
+    import subprocess
+    os.makedirs(workdir, exist_ok=True)
+    ga, gb, out = (os.path.join(workdir, f) for f in ("g1.csv", "g2.csv", "match.csv"))
+    bm.write_graph_csv(ga, A)
+    bm.write_graph_csv(gb, B)
+    subprocess.run([GREEDY_REF, ga, gb, out], check=True, stdout=subprocess.DEVNULL)
+    ref = np.loadtxt(out, delimiter=",", skiprows=1, dtype=np.int64).reshape(-1, 2)
+    pi = np.zeros(A.n + 1, np.int32)
+    pi[ref[:, 0]] = ref[:, 1]
+    return pi
+
+
+def make_greedy_case(name):
+    import tempfile
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for i, (config, seed, n, m) in enumerate(GREEDY_CASES):
+            A, B, truth, init = bm.gen_pair(config, n=n, m_target=m, seed=seed)
+            out[f"case{i}"] = np.array([config, seed, n, m], np.int64)
+            out[f"digest{i}"] = np.array([edge_digest(A), edge_digest(B)], np.uint64)
+            out[f"pi{i}"] = run_ref_greedy(A, B, os.path.join(tmp, str(i)))
+            print(name, i, config, seed, n, m, "matched", int((out[f"pi{i}"][1:] > 0).sum()))
+    np.savez_compressed(os.path.join(HERE, name), **out)
 
 
 def main():

@@ -50,3 +50,14 @@ def test_device_greedy_full_scale():
         td = time.perf_counter() - t
     np.testing.assert_array_equal(got, host)
     print(f"greedy matching n={A.n}: host {th:.3f} s, device {td:.3f} s")
+
+
+@pytest.mark.parametrize("idx", range(3))
+def test_device_greedy_equals_reference_fixture(idx):
+    """The device matching equals the reference greedy-match binary's output
+    (tests/golden/golden_greedy.npz, made by oracle/_ref/greedy-match)."""
+    from test_ref_greedy import fixture_pair, greedy_cases
+    A, B, pi_ref = fixture_pair(greedy_cases()[idx])
+    with bm.Engine(0) as e:
+        got = e.greedy_match(A, B)
+    np.testing.assert_array_equal(got, pi_ref)

@@ -79,3 +79,54 @@ def test_deltas_equal_reference_gpu_kernel(config, nrows):
         os.makedirs(out, exist_ok=True)
         with open(os.path.join(out, f"refkernel_cfg{config}.json"), "w") as f:
             json.dump(res, f)
+
+
+REFGPU3 = os.path.join(REPO, "oracle", "_ref", "librefgpu3.so")
+
+
+def refgpu3():
+    L = C.CDLL(REFGPU3)
+    vp = C.c_void_p
+    L.refgpu3_triplets.restype = C.c_int
+    L.refgpu3_triplets.argtypes = [C.c_int, C.c_longlong, vp, vp, vp, C.c_longlong, vp, vp, vp, vp, vp, C.c_int,
+                                   C.c_int, C.c_int, C.POINTER(C.c_float), vp, vp]
+    return L
+
+
+def run_refgpu3(A, B, pi, changed, batch, iters=1):
+    """The reference's calculateThreeNodeSwapKernel on the first `batch`
+    triplets of its enumeration around the vertices `changed`; returns
+    (triplets (batch x 3), best deltas, ms per launch)."""
+    L = refgpu3()
+    changed = np.ascontiguousarray(changed, np.int32)
+    deltas = np.zeros(batch, np.int32)
+    trip = np.zeros(4 * batch, np.int32)
+    ms = C.c_float()
+    st = L.refgpu3_triplets(A.n, A.m, A.src.ctypes.data, A.dst.ctypes.data, A.w.ctypes.data, B.m, B.src.ctypes.data,
+                            B.dst.ctypes.data, B.w.ctypes.data, pi.ctypes.data, changed.ctypes.data, len(changed),
+                            batch, iters, C.byref(ms), deltas.ctypes.data, trip.ctypes.data)
+    assert st == 0, f"reference 3-vertex kernel failed with CUDA error {st}"
+    return trip.reshape(-1, 4)[:, :3].copy(), deltas.astype(np.int64), ms.value
+
+
+@pytest.mark.skipif(not os.path.exists(REFGPU3), reason="oracle/_ref/librefgpu3.so not built")
+@pytest.mark.parametrize("config,batch", [(1, 2048), (2, 1024)])
+def test_3sets_equal_reference_gpu3_kernel(config, batch):
+    """The best-permutation delta of every triplet the reference's 3-vertex
+    GPU kernel (src/graph-re-alignment-gpu-3-swap.cu:43-305) evaluates, among
+    its enumeration around six rows of the ordering, equals the engine's
+    3-sets (all six permutations; the reference's identity permutation scores
+    0, so both report max(0, best move))."""
+    A, B, truth, init = bm.gen_pair(config)
+    n = A.n
+    order = bm.rows_from_ordering(bm.ordering_by_weighted_degree(A))
+    changed = order[n // 4:n // 4 + 6]
+    trip, d_ref, ms = run_refgpu3(A, B, init, changed, batch)
+    assert (trip > 0).all() and (np.sort(trip, 1)[:, :2] != np.sort(trip, 1)[:, 1:]).all()
+    with bm.Engine(0) as eng:
+        eng.set_graphs(A, B)
+        eng.set_mapping(init)
+        best, perm = eng.kset_eval(3, trip)
+    np.testing.assert_array_equal(np.maximum(best, 0), d_ref)
+    print(json.dumps({"config": config, "triplets": batch, "reference_kernel_ms": ms,
+                      "reference_triplets_per_s": batch / (ms / 1e3), "improving": int((d_ref > 0).sum())}))
