@@ -254,13 +254,14 @@ def run_reference(args, ws, rank, dist):
         impl, kind = Reference(n, Ae, Be), "reference"
     else:
         impl, kind = Oracle(n, Ae, Be), "port"
-    for st in step_starts(n, args.warmup, 0.5):
-        impl.rows(init, rows[st:st + 1], threads)
-    # rows per step: the whole batch if K steps fit the budget (estimated from
-    # one timed row), else fewer
+    # warm-up: one row at each of W evenly spaced positions; their mean time
+    # estimates a row, and the whole batch is timed per step if K steps fit
+    # the budget, else fewer rows of it
     t0 = time.perf_counter()
-    impl.rows(init, rows[:1], threads)
-    est = time.perf_counter() - t0
+    wstarts = step_starts(n, args.warmup, 0.5)
+    for st in wstarts:
+        impl.rows(init, rows[st:st + 1], threads)
+    est = (time.perf_counter() - t0) / max(1, len(wstarts))
     rps = max(1, min(R, int(args.ref_budget / max(1e-9, est * args.steps))))
     total = 0.0
     starts = step_starts(n, args.steps)
@@ -415,7 +416,7 @@ def run_ours(args, ws, rank, local, dist):
 
 
 TRAFFIC_RECORD = os.path.join(REPO, "profiles", "rows_kernel_traffic.json")
-ROWS_KERNEL_SOURCES = ("brain-match_b200/csrc/bm_rows.cu", "brain-match_b200/csrc/bm_internal.cuh")
+ROWS_KERNEL_SOURCES = ("brain-match_b200/csrc/bm_rows.cu",)
 
 
 def rows_kernel_digest() -> str:
@@ -505,6 +506,8 @@ def reference_gpu3(A, B, init, rows, batch=4096):
 
 
 MLP_FLOP_PER_PAIR = 2 * (24 * 128 + 128 * 128 + 128)
+# forward, then dW2 = H1^T dH2, dH1 = dH2 W2^T, dW1 = X^T dH1, dw3 and dh2
+MLP_TRAIN_FLOP_PER_RECORD = MLP_FLOP_PER_PAIR + 2 * 128 * 128 + 2 * 128 * 128 + 2 * 24 * 128 + 3 * 128
 
 
 def bf16_peak():
@@ -545,6 +548,23 @@ def scorer_throughput(device, A, B, init, rows):
         out[f"scorer_{name}"] = {"pairs_per_s": pairs / (ms / 1e3),
                                  "tflops": pairs * MLP_FLOP_PER_PAIR / (ms / 1e3) / 1e12, "ms_per_launch": ms,
                                  "rows_per_launch": R}
+    # training: minibatch steps (gather, gradient, AdamW) of 8,192 records
+    m.reserve_records(1 << 18)
+    m.collect_rows(rows[:1024], per_row=128, seed=3)
+    for backend, steps, name in ((0, 200, "tcgen05"), (1, 20, "simt")):
+        m.set_backend(backend)
+        m.fit(2, batch=8192, lr=1e-3)
+        e.sync()
+        e.record(a)
+        m.fit(steps, batch=8192, lr=1e-3)
+        e.record(b)
+        e.sync()
+        ms = e.elapsed_ms(a, b) / steps
+        out[f"training_{name}"] = {"records_per_s": 8192 / (ms / 1e3), "ms_per_step": ms,
+                                   "tflops": 8192 * MLP_TRAIN_FLOP_PER_RECORD / (ms / 1e3) / 1e12,
+                                   "batch": 8192, "steps": steps,
+                                   "timing": "CUDA events around whole steps: gather, gradient, AdamW"}
+    m.set_backend(0)
     peak, kind = bf16_peak()
     tc = out["scorer_tcgen05"]["tflops"]
     out["roofline_scorer"] = {"bound": "tensor", "achieved": tc, "peak": peak, "unit": "TFLOP/s", "frac": tc / peak,
@@ -798,7 +818,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows-per-step", type=int, default=57)
     ap.add_argument("--ref-seconds", type=float, default=12.0, help="budget of the engine arm's cpu_baseline sample")
-    ap.add_argument("--ref-budget", type=float, default=150.0,
+    ap.add_argument("--ref-budget", type=float, default=240.0,
                     help="budget of the reference arm's timed steps (seconds); larger K get fewer rows per step")
     ap.add_argument("--write-workload", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--no-reference-gpu", action="store_true",

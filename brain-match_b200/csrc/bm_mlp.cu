@@ -50,14 +50,17 @@ constexpr int kOffW3 = kOffB2 + BM_MLP_H;
 constexpr int kOffB3 = kOffW3 + BM_MLP_H;
 constexpr int kNParams = kOffB3 + 1;
 
-// Weight image of the tensor-core kernel: W1, W2 and the output row w3 as
+// Weight image of the tensor-core kernels: W1, W2 and the output row w3 as
 // BF16 in the K-major, no-swizzle operand layout, then the FP32 epilogue
-// vectors b1, b2, (unused), b3.
+// vectors b1, b2, w3 (BF16-rounded), b3, then W2 transposed (the B operand of
+// the backward product dH2 . W2^T of the training kernel).
 constexpr int kImgW1 = 128 * 32 * 2;   // N=128 hidden x K=32 (24 inputs + 8 zero)
 constexpr int kImgW2 = 128 * 128 * 2;  // N=128 out x K=128 in
 constexpr int kImgW3 = 16 * 128 * 2;   // N=16 x K=128: w3 in row 0, zeros elsewhere
 constexpr int kImgEp = (3 * BM_MLP_H + 4) * 4;
-constexpr int kImgBytes = kImgW1 + kImgW2 + kImgW3 + kImgEp;
+constexpr int kImgW2T = 128 * 128 * 2;  // N=128 in x K=128 out
+constexpr int kImgOffW2T = kImgW1 + kImgW2 + kImgW3 + kImgEp;
+constexpr int kImgBytes = kImgOffW2T + kImgW2T;
 
 }  // namespace
 
@@ -568,7 +571,7 @@ constexpr uint32_t kSmW2 = kSmW1 + kImgW1;          // 8192
 constexpr uint32_t kSmW3 = kSmW2 + kImgW2;          // 40960
 constexpr uint32_t kSmH = kSmW3 + kImgW3;           // 45056: h1 / h2 operand (32 KB)
 constexpr uint32_t kSmX = kSmH + 128 * 128 * 2;     // 77824: features operand (8 KB)
-constexpr uint32_t kSmEp = kSmX + 128 * 32 * 2;     // 86016: b1, b2, (unused), b3
+constexpr uint32_t kSmEp = kSmX + 128 * 32 * 2;     // 86016: b1, b2, w3, b3
 constexpr uint32_t kSmBits = kSmEp + kImgEp;        // 87568
 constexpr uint32_t kTcMinSmem = 100 * 1024;         // at most 2 CTAs (2 x 256 TMEM columns) per SM
 static_assert(kSmBits % 16 == 0 && kSmH % 1024 == 0 && kSmX % 1024 == 0, "operand layout");
@@ -691,8 +694,9 @@ __global__ void prep_image_kernel(const float* __restrict__ w, unsigned char* __
     unsigned short* w2 = reinterpret_cast<unsigned short*>(img + kSmW2);
     unsigned short* w3 = reinterpret_cast<unsigned short*>(img + kSmW3);
     float* ep = reinterpret_cast<float*>(img + kImgW1 + kImgW2 + kImgW3);
+    unsigned short* w2t = reinterpret_cast<unsigned short*>(img + kImgOffW2T);
     const int n1 = 128 * 32, n2 = 128 * 128, n3 = 16 * 128;
-    const int total = n1 + n2 + n3 + 3 * 128 + 4;
+    const int total = n1 + n2 + n3 + 3 * 128 + 4 + n2;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         if (t < n1) {
             const int j = t / 32, i = t % 32;  // hidden j (N), input i (K)
@@ -706,12 +710,16 @@ __global__ void prep_image_kernel(const float* __restrict__ w, unsigned char* __
             const int q = t - n1 - n2, j = q / 128, i = q % 128;  // row j (N = 16), in i (K)
             const float v = j == 0 ? bf16r(w[kOffW3 + i]) : 0.f;
             w3[kmajor_off(j, i, 128) / 2] = (unsigned short)(__float_as_uint(v) >> 16);
-        } else {
+        } else if (t < n1 + n2 + n3 + 3 * 128 + 4) {
             const int q = t - n1 - n2 - n3;
             if (q < 128) ep[q] = w[kOffB1 + q];
             else if (q < 256) ep[q] = w[kOffB2 + q - 128];
-            else if (q < 384) ep[q] = 0.f;
+            else if (q < 384) ep[q] = bf16r(w[kOffW3 + q - 256]);
             else ep[q] = (q == 384) ? w[kOffB3] : 0.f;
+        } else {
+            const int q = t - (n1 + n2 + n3 + 3 * 128 + 4), i = q / 128, j = q % 128;  // in i (N), out j (K)
+            const float v = bf16r(w[kOffW2 + i * BM_MLP_H + j]);
+            w2t[kmajor_off(i, j, 128) / 2] = (unsigned short)(__float_as_uint(v) >> 16);
         }
     }
 }
@@ -933,6 +941,363 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     }
 }
 
+// ------------------------------------------- tensor-core training kernel
+//
+// Loss mean((out - y)^2) over k records and its gradient, with every matrix
+// product of the forward and backward passes on the tensor cores (tcgen05
+// MMA, BF16 operands in shared memory, FP32 accumulators in TMEM).  One CTA
+// (128 threads, one record per thread and TMEM lane) takes tiles of 128
+// records; per tile:
+//   1. X = the records' features (K padded to 32) and X^T;
+//   2. layer 1: D1 = X . W1 (TMEM columns 0..127); h1 = bf16(relu(D1 + b1))
+//      into H (record rows) and H1^T (hidden rows);
+//   3. layer 2: D2 = H . W2 (columns 128..255); h2 = bf16(relu(D2 + b2)) into
+//      H2^T (over H), the output o = h2 . w3 + b3, r = o - y, dout = 2 r / k,
+//      dh2 = bf16(h2 > 0 ? dout w3 : 0) into dH2 (record rows) and dH2^T;
+//   4. dH1 = dH2 . W2^T (columns 0..127) and dW2 += H1^T . dH2 (columns
+//      256..383, accumulated over the CTA's tiles); meanwhile thread j sums row
+//      j of dH2^T (db2) and dout . row j of H2^T (dw3);
+//   5. dh1 = bf16(h1 > 0 ? dH1 : 0) into dH1^T (over dH2);
+//   6. dW1^T += dH1^T . X^T (N = 32, columns 384..415); thread j sums row j of
+//      dH1^T (db1).
+// At the end each CTA reads its dW2 and dW1^T accumulators back and adds them,
+// with its bias and w3 sums, into the FP32 gradient (atomics).  Rounding: as
+// the SIMT kernel, plus dh2 and dh1 rounded to BF16 (they are MMA operands);
+// the bias sums use the rounded values.
+//
+// Operands whose K index is the record (H1^T, H2^T, dH2^T, dH1^T, X^T) are
+// written by each thread as its own K column, one 16-bit element per store.
+// Their core matrices are 144 bytes apart along K (the descriptor's leading
+// byte offset) instead of 128, so the four groups of eight lanes of a warp
+// store into distinct banks; the 8-row groups are 16 x 144 = 2,304 bytes
+// apart.
+constexpr int kTrThreads = 128;
+constexpr uint32_t kTLbo = 144, kTSbo = 16 * kTLbo;  // transposed operands
+constexpr uint32_t kTBytes128 = 16 * kTSbo;          // 128 rows: 36,864 bytes
+__host__ __device__ __forceinline__ uint32_t tmajor_off(uint32_t r, uint32_t k) {
+    return (r >> 3) * kTSbo + (k >> 3) * kTLbo + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+constexpr uint32_t kTrW1 = 0;                          // W1 image (8 KB)
+constexpr uint32_t kTrW2 = kTrW1 + kImgW1;             // 8192: W2 image (32 KB)
+constexpr uint32_t kTrW2T = kTrW2 + kImgW2;            // 40960: W2^T image (32 KB)
+constexpr uint32_t kTrXT = kTrW2T + kImgW2T;           // 73728: X^T, feature rows 0..23 (row group 3 holds
+                                                       //   b1, b2, w3, b3 and the tile's dout; it only feeds
+                                                       //   the unused columns 24..31 of dW1^T)
+constexpr uint32_t kTrEp = kTrXT + 3 * kTSbo;          // 80640
+constexpr uint32_t kTrDout = kTrEp + ((kImgEp + 15) & ~15);
+constexpr uint32_t kTrH = kTrXT + 4 * kTSbo;           // 82944: h1 (record rows), then h2^T
+constexpr uint32_t kTrH1T = kTrH + kTBytes128;         // 119808: h1^T
+constexpr uint32_t kTrD = kTrH1T + kTBytes128;         // 156672: X, then dh2 (record rows), then dh1^T
+constexpr uint32_t kTrDT = kTrD + kTBytes128;          // 193536: dh2^T
+constexpr uint32_t kTrBars = kTrDT + kTBytes128;       // 230400: four mbarriers, then the TMEM base slot
+constexpr uint32_t kTrSmem = kTrBars + 48;
+static_assert(kTrDout + 128 * 4 <= kTrH, "epilogue vectors in X^T's spare row group");
+static_assert(kTrXT % 1024 == 0 && kTrH % 16 == 0 && kTrH1T % 16 == 0 && kTrD % 16 == 0 && kTrDT % 16 == 0,
+              "training operand alignment");
+static_assert(kTrSmem <= 227 * 1024, "training kernel shared memory");
+constexpr uint32_t kIdesc32 = idesc_bf16(128, 32);
+
+struct TrArgs {
+    const unsigned char* img;
+    const float* xin;      // k x 24 float features, or
+    const uint16_t* xbf;   // k x 24 BF16 records
+    const float* y;
+    int64_t k;
+    float* g;              // gradient (zeroed by the caller), FP32, parameter order
+    float* loss;           // += mean squared error
+    int32_t* flag;
+    long long wait_limit;
+};
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) { return (uint16_t)(cvt_bf16x2(x, 0.f) & 0xFFFFu); }
+
+// Element (row r, this thread's record p) of a transposed operand.
+__device__ __forceinline__ void st_t(unsigned char* base, uint32_t r, uint32_t p, uint16_t v) {
+    *reinterpret_cast<uint16_t*>(base + tmajor_off(r, p)) = v;
+}
+
+// Sum of row j of a transposed operand (128 BF16 values).
+__device__ __forceinline__ float row_sum_t(const unsigned char* base, uint32_t j) {
+    float s = 0.f;
+#pragma unroll 4
+    for (int c = 0; c < 16; c++) {
+        const uint4 q = *reinterpret_cast<const uint4*>(base + tmajor_off(j, 8 * c));
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) s += __uint_as_float(w[e] << 16) + __uint_as_float(w[e] & 0xFFFF0000u);
+    }
+    return s;
+}
+
+// Row j of a transposed operand dotted with the tile's dout.
+__device__ __forceinline__ float row_dot_t(const unsigned char* base, uint32_t j, const float* dout) {
+    float s = 0.f;
+#pragma unroll 4
+    for (int c = 0; c < 16; c++) {
+        const uint4 q = *reinterpret_cast<const uint4*>(base + tmajor_off(j, 8 * c));
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            s = fmaf(__uint_as_float(w[e] << 16), dout[8 * c + 2 * e], s);
+            s = fmaf(__uint_as_float(w[e] & 0xFFFF0000u), dout[8 * c + 2 * e + 1], s);
+        }
+    }
+    return s;
+}
+
+__global__ void __launch_bounds__(kTrThreads, 1) mlp_train_tc_kernel(TrArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kTrBars);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kTrBars + 32);
+    uint32_t bar[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) bar[b] = smem_u32(&bars[b]);
+    const float* ep = reinterpret_cast<const float*>(sm + kTrEp);  // b1 [0..127], b2 [128..], w3 [256..], b3 [384]
+    float* dsm = reinterpret_cast<float*>(sm + kTrDout);
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(a.img);
+        for (int i = tid; i < (kImgW1 + kImgW2) / 16; i += kTrThreads) reinterpret_cast<uint4*>(sm + kTrW1)[i] = src[i];
+        for (int i = tid; i < kImgW2T / 16; i += kTrThreads)
+            reinterpret_cast<uint4*>(sm + kTrW2T)[i] = src[kImgOffW2T / 16 + i];
+        for (int i = tid; i < kImgEp / 16; i += kTrThreads)
+            reinterpret_cast<uint4*>(sm + kTrEp)[i] = src[(kImgW1 + kImgW2 + kImgW3) / 16 + i];
+    }
+    if (tid == 0) {
+        for (int b = 0; b < 4; b++) mbar_init(bar[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_handoff();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lb = (uint32_t)(warp * 32) << 16;
+    const uint32_t tD1 = tmem, tD2 = tmem + 128u, tW2 = tmem + 256u, tW1 = tmem + 384u;
+    const uint32_t sXT = smem_u32(sm + kTrXT), sH = smem_u32(sm + kTrH), sH1T = smem_u32(sm + kTrH1T),
+                   sD = smem_u32(sm + kTrD), sDT = smem_u32(sm + kTrDT), sW1 = smem_u32(sm + kTrW1),
+                   sW2 = smem_u32(sm + kTrW2), sW2T = smem_u32(sm + kTrW2T);
+    const uint32_t p = (uint32_t)tid;
+    const float scale = 2.0f / (float)a.k;
+    const int64_t tiles = (a.k + 127) / 128;
+    float gb1 = 0.f, gb2 = 0.f, gw3 = 0.f, gb3 = 0.f, lsum = 0.f;
+    uint32_t phase = 0, last_bar = 0, last_par = 0;
+    bool ok = true, first = true;
+    auto wait = [&](int b) -> bool { return __syncthreads_and(mbar_wait(bar[b], phase, a.wait_limit)); };
+    auto commit = [&](int b) {
+        if (tid == 0) mma_commit(bar[b]);
+        last_bar = bar[b];
+        last_par = phase;
+    };
+    for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const int64_t q = t * 128 + tid;
+        const bool valid = q < a.k;
+        // ---- 1. features: X (record rows, K = 32, in D's space) and X^T
+        {
+            float x[BM_MLP_IN];
+            if (valid && a.xbf) {
+                const uint4* r4 = reinterpret_cast<const uint4*>(a.xbf + q * BM_MLP_IN);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const uint4 v4 = r4[c];
+                    const uint32_t w[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        x[8 * c + 2 * e] = __uint_as_float(w[e] << 16);
+                        x[8 * c + 2 * e + 1] = __uint_as_float(w[e] & 0xFFFF0000u);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < BM_MLP_IN; i++) x[i] = valid ? a.xin[q * BM_MLP_IN + i] : 0.f;
+            }
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                uint4 o = make_uint4(0u, 0u, 0u, 0u);
+                if (c < 3) {
+                    o.x = cvt_bf16x2(x[8 * c + 0], x[8 * c + 1]);
+                    o.y = cvt_bf16x2(x[8 * c + 2], x[8 * c + 3]);
+                    o.z = cvt_bf16x2(x[8 * c + 4], x[8 * c + 5]);
+                    o.w = cvt_bf16x2(x[8 * c + 6], x[8 * c + 7]);
+                }
+                *reinterpret_cast<uint4*>(sm + kTrD + kmajor_off(p, 8 * c, 32)) = o;
+            }
+#pragma unroll
+            for (int f = 0; f < BM_MLP_IN; f++) st_t(sm + kTrXT, (uint32_t)f, p, bf16_bits(x[f]));
+        }
+        const float yv = valid ? a.y[q] : 0.f;
+        tc_handoff();
+        // ---- 2. layer 1
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < 2; s++)
+                mma_bf16(tD1, smem_desc(sD + 256u * s, 128u, 512u), smem_desc(sW1 + 256u * s, 128u, 512u), kIdesc128,
+                         s > 0);
+        }
+        commit(0);
+        if (!wait(0)) { ok = false; break; }
+        tc_fence_after();
+        uint32_t m1[4];  // h1 > 0, one bit per hidden unit
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            float d[32];
+            tmem_ld32(tD1 + lb + 32u * c, d);
+            uint32_t hb[16];
+            m1[c] = 0u;
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                hb[e] = cvt_relu_bf16x2(d[2 * e] + ep[32 * c + 2 * e], d[2 * e + 1] + ep[32 * c + 2 * e + 1]);
+                if (hb[e] & 0xFFFFu) m1[c] |= 1u << (2 * e);
+                if (hb[e] >> 16) m1[c] |= 1u << (2 * e + 1);
+            }
+#pragma unroll
+            for (int qd = 0; qd < 4; qd++)
+                *reinterpret_cast<uint4*>(sm + kTrH + kmajor_off(p, 32 * c + 8 * qd, 128)) =
+                    make_uint4(hb[4 * qd], hb[4 * qd + 1], hb[4 * qd + 2], hb[4 * qd + 3]);
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                st_t(sm + kTrH1T, (uint32_t)(32 * c + 2 * e), p, (uint16_t)(hb[e] & 0xFFFFu));
+                st_t(sm + kTrH1T, (uint32_t)(32 * c + 2 * e + 1), p, (uint16_t)(hb[e] >> 16));
+            }
+        }
+        tc_handoff();
+        // ---- 3. layer 2; h2^T over H; output, loss, dh2
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < 8; s++)
+                mma_bf16(tD2, smem_desc(sH + 256u * s, 128u, 2048u), smem_desc(sW2 + 256u * s, 128u, 2048u),
+                         kIdesc128, s > 0);
+        }
+        commit(1);
+        if (!wait(1)) { ok = false; break; }
+        tc_fence_after();
+        float o = ep[384];
+        uint32_t m2[4];  // h2 > 0
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            float d[32];
+            tmem_ld32(tD2 + lb + 32u * c, d);
+            m2[c] = 0u;
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const uint32_t h = cvt_relu_bf16x2(d[2 * e] + ep[128 + 32 * c + 2 * e],
+                                                   d[2 * e + 1] + ep[128 + 32 * c + 2 * e + 1]);
+                const float h0 = __uint_as_float(h << 16), h1v = __uint_as_float(h & 0xFFFF0000u);
+                o = fmaf(h0, ep[256 + 32 * c + 2 * e], o);
+                o = fmaf(h1v, ep[256 + 32 * c + 2 * e + 1], o);
+                if (h & 0xFFFFu) m2[c] |= 1u << (2 * e);
+                if (h >> 16) m2[c] |= 1u << (2 * e + 1);
+                st_t(sm + kTrH, (uint32_t)(32 * c + 2 * e), p, (uint16_t)(h & 0xFFFFu));
+                st_t(sm + kTrH, (uint32_t)(32 * c + 2 * e + 1), p, (uint16_t)(h >> 16));
+            }
+        }
+        const float r = valid ? o - yv : 0.f;
+        const float dout = scale * r;
+        lsum += r * r;
+        dsm[tid] = dout;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            uint32_t db[16];
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const int j = 32 * c + 2 * e;
+                const float d0 = ((m2[c] >> (2 * e)) & 1u) ? dout * ep[256 + j] : 0.f;
+                const float d1 = ((m2[c] >> (2 * e + 1)) & 1u) ? dout * ep[256 + j + 1] : 0.f;
+                db[e] = cvt_bf16x2(d0, d1);
+                st_t(sm + kTrDT, (uint32_t)j, p, (uint16_t)(db[e] & 0xFFFFu));
+                st_t(sm + kTrDT, (uint32_t)(j + 1), p, (uint16_t)(db[e] >> 16));
+            }
+#pragma unroll
+            for (int qd = 0; qd < 4; qd++)
+                *reinterpret_cast<uint4*>(sm + kTrD + kmajor_off(p, 32 * c + 8 * qd, 128)) =
+                    make_uint4(db[4 * qd], db[4 * qd + 1], db[4 * qd + 2], db[4 * qd + 3]);
+        }
+        tc_handoff();
+        // ---- 4. dH1 = dH2 . W2^T and dW2 += H1^T . dH2
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < 8; s++)
+                mma_bf16(tD1, smem_desc(sD + 256u * s, 128u, 2048u), smem_desc(sW2T + 256u * s, 128u, 2048u),
+                         kIdesc128, s > 0);
+#pragma unroll
+            for (int s = 0; s < 8; s++)
+                mma_bf16(tW2, smem_desc(sH1T + 2u * kTLbo * s, kTLbo, kTSbo),
+                         smem_desc(sDT + 2u * kTLbo * s, kTLbo, kTSbo), kIdesc128, (first && s == 0) ? 0u : 1u);
+        }
+        commit(2);
+        gb2 += row_sum_t(sm + kTrDT, p);
+        gw3 += row_dot_t(sm + kTrH, p, dsm);
+        if (tid == 0) {
+            float sd = 0.f;
+            for (int i = 0; i < 128; i++) sd += dsm[i];
+            gb3 += sd;
+        }
+        if (!wait(2)) { ok = false; break; }
+        tc_fence_after();
+        // ---- 5. dh1^T over dH2 (dead after step 4)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            float d[32];
+            tmem_ld32(tD1 + lb + 32u * c, d);
+#pragma unroll
+            for (int e = 0; e < 32; e++)
+                st_t(sm + kTrD, (uint32_t)(32 * c + e), p, ((m1[c] >> e) & 1u) ? bf16_bits(d[e]) : (uint16_t)0);
+        }
+        tc_handoff();
+        // ---- 6. dW1^T += dH1^T . X^T
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < 8; s++)
+                mma_bf16(tW1, smem_desc(sD + 2u * kTLbo * s, kTLbo, kTSbo), smem_desc(sXT + 2u * kTLbo * s, kTLbo, kTSbo),
+                         kIdesc32, (first && s == 0) ? 0u : 1u);
+        }
+        commit(3);
+        gb1 += row_sum_t(sm + kTrD, p);
+        if (!wait(3)) { ok = false; break; }
+        tc_fence_after();
+        first = false;
+        phase ^= 1u;
+    }
+    if (ok && !first) {
+        // this CTA's weight-gradient accumulators: row tid of dW2 (input unit
+        // tid) and of dW1^T (hidden unit tid)
+#pragma unroll 1
+        for (int c = 0; c < 4; c++) {
+            float d[32];
+            tmem_ld32(tW2 + lb + 32u * c, d);
+#pragma unroll
+            for (int e = 0; e < 32; e++)
+                if (d[e] != 0.f) atomicAdd(&a.g[kOffW2 + tid * BM_MLP_H + 32 * c + e], d[e]);
+        }
+        {
+            float d[32];
+            tmem_ld32(tW1 + lb, d);
+#pragma unroll
+            for (int f = 0; f < BM_MLP_IN; f++)
+                if (d[f] != 0.f) atomicAdd(&a.g[f * BM_MLP_H + tid], d[f]);
+        }
+        atomicAdd(&a.g[kOffB1 + tid], gb1);
+        atomicAdd(&a.g[kOffB2 + tid], gb2);
+        atomicAdd(&a.g[kOffW3 + tid], gw3);
+        if (tid == 0) atomicAdd(&a.g[kOffB3], gb3);
+        for (int o = 16; o; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if (lane == 0 && lsum != 0.f) atomicAdd(a.loss, lsum / (float)a.k);
+    }
+    if (!ok && tid == 0) atomicExch(a.flag, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        // let the MMAs in flight finish before the columns are freed (the
+        // default bound, whatever bound the waits above were given)
+        if (!ok) mbar_wait(last_bar, last_par);
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    }
+}
+
 // ------------------------------------------------------------------ top-K
 //
 // For each row of scores, the K largest (ties: lower partner id first),
@@ -1074,6 +1439,10 @@ bm_status set_attrs(bm_mlp* M) {
     if (tcs > ctx->smem_optin)
         return bm_fail(ctx, BM_UNSUPPORTED, "tensor-core scoring needs %u bytes of shared memory", tcs);
     BM_CUDA(ctx, cudaFuncSetAttribute(mlp_rows_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcs));
+    if (kTrSmem > ctx->smem_optin)
+        return bm_fail(ctx, BM_UNSUPPORTED, "tensor-core training needs %u bytes of shared memory", kTrSmem);
+    BM_CUDA(ctx, cudaFuncSetAttribute(mlp_train_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTrSmem));
     return BM_OK;
 }
 
@@ -1124,10 +1493,26 @@ bm_status launch_score_simt(bm_mlp* M, PairSrc P, int64_t k, float* d_out) {
     return BM_OK;
 }
 
+// Gradient of the loss over k records into M->d_g and M->d_loss: on the
+// tensor cores (backend 0, records given as features) or the SIMT kernel.
 bm_status launch_grad(bm_mlp* M, PairSrc P, const float* d_y, int64_t k) {
     bm_ctx* ctx = M->ctx;
     BM_CUDA(ctx, cudaMemsetAsync(M->d_g, 0, sizeof(float) * (size_t)kNParams, ctx->stream));
     BM_CUDA(ctx, cudaMemsetAsync(M->d_loss, 0, sizeof(float), ctx->stream));
+    if (M->backend == 0 && (P.xin || P.xbf)) {
+        if (M->img_dirty) {
+            prep_image_kernel<<<64, 256, 0, ctx->stream>>>(M->d_w, M->d_img);
+            BM_LAUNCH_CHECK(ctx, "prep_image_kernel");
+            M->img_dirty = false;
+        }
+        TrArgs a{M->d_img, P.xin, P.xbf, d_y, k, M->d_g, M->d_loss, M->d_flag,
+                 ctx->wait_limit > 0 ? (long long)ctx->wait_limit : kWaitLimit};
+        const int64_t tiles = (k + 127) / 128;
+        const int grid = (int)std::min<int64_t>(tiles, ctx->num_sms);
+        mlp_train_tc_kernel<<<grid, kTrThreads, kTrSmem, ctx->stream>>>(a);
+        BM_LAUNCH_CHECK(ctx, "mlp_train_tc_kernel");
+        return BM_OK;
+    }
     mlp_grad_kernel<<<simt_grid(ctx, k, 1), kMT, sizeof(GradSmem), ctx->stream>>>(feat_src(ctx, M), P, M->d_w, d_y, k,
                                                                                   M->d_g, M->d_loss);
     BM_LAUNCH_CHECK(ctx, "mlp_grad_kernel");
@@ -1192,7 +1577,7 @@ bm_status check_flag(bm_mlp* M) {
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (f) {
         BM_CUDA(ctx, cudaMemsetAsync(M->d_flag, 0, sizeof(int32_t), ctx->stream));
-        return bm_fail(ctx, BM_TIMEOUT, "tensor-core scoring: an MMA completion wait ran out");
+        return bm_fail(ctx, BM_TIMEOUT, "tensor-core kernel: an MMA completion wait ran out");
     }
     return BM_OK;
 }
@@ -1288,7 +1673,7 @@ bm_status fit_steps(bm_mlp* M, int32_t steps, int32_t batch, float lr, float wd,
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         *loss = l;
     }
-    return BM_OK;
+    return check_flag(M);
 }
 
 }  // namespace
@@ -1546,7 +1931,7 @@ extern "C" bm_status bm_mlp_gradients(bm_mlp* M, const float* x, const float* y,
     BM_CUDA(ctx, cudaMemcpyAsync(&l, M->d_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (loss) *loss = l;
-    return BM_OK;
+    return check_flag(M);
 }
 
 extern "C" bm_status bm_mlp_adamw_step(bm_mlp* M, const float* x, const float* y, int64_t k, float lr,
@@ -1568,7 +1953,7 @@ extern "C" bm_status bm_mlp_adamw_step(bm_mlp* M, const float* x, const float* y
     BM_CUDA(ctx, cudaMemcpyAsync(&l, M->d_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (loss) *loss = l;
-    return BM_OK;
+    return check_flag(M);
 }
 
 extern "C" bm_status bm_mlp_collect_rows(bm_mlp* M, const int32_t* rows, int32_t nrows, int32_t per_row, uint64_t seed,

@@ -28,6 +28,14 @@
  *                          (:321-408), which differ on graphs with
  *                          self-loops; ref-cpu with --mode parity makes the
  *                          reference loop's accepts on such graphs
+ *   --ranks N --rank R     run as rank R of N processes (one per GPU) of a
+ *                          sharded search (bm_search_sharded; --mode search),
+ *                          in place of the reference's MPI drivers; every
+ *                          rank reads the same inputs, rank 0 writes
+ *                          <out mapping> and prints the progress lines
+ *   --addr HOST:PORT       rank 0's address (default 127.0.0.1:29517)
+ *   --comm tcp|nccl        the ranks' transport (default nccl)
+ *   --comm-timeout S       bound of every exchange (default 120)
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -37,7 +45,8 @@
 #include "bm_cuda.h"
 #include "bm_host.h"
 
-#define LOG_INFO(...) do { printf("[INFO] " __VA_ARGS__); printf("\n"); fflush(stdout); } while (0)
+static int g_quiet = 0; /* ranks other than 0 of a sharded run print no progress lines */
+#define LOG_INFO(...) do { if (!g_quiet) { printf("[INFO] " __VA_ARGS__); printf("\n"); fflush(stdout); } } while (0)
 #define LOG_ERROR(...) do { fprintf(stderr, "[ERROR] " __VA_ARGS__); fprintf(stderr, "\n"); } while (0)
 
 static const char* commas(long long v, char* buf) {
@@ -78,16 +87,19 @@ int main(int argc, char** argv) {
         LOG_ERROR("Usage: %s <male graph> <female graph> <male ordering> <female ordering> <in mapping> <out mapping> "
                   "[--mode parity|search] [--schedule natural|ordering] [--time-budget S] [--max-accepts K] "
                   "[--max-sweeps K] [--save-interval S] [--rows-per-batch R] [--device D] "
-                  "[--semantics exact|ref-cpu]",
+                  "[--semantics exact|ref-cpu] [--ranks N --rank R [--addr HOST:PORT] [--comm tcp|nccl] "
+                  "[--comm-timeout S]]",
                   argv[0]);
         return 1;
     }
     const char* mode = "parity";
     const char* schedule = "natural";
     const char* semantics = "exact";
-    double budget = 0, save_interval = 60;
+    double budget = 0, save_interval = 60, comm_timeout = 120;
     long long max_accepts = -1;
-    int max_sweeps = -1, device = 0, rows_per_batch = 0;
+    int max_sweeps = -1, device = 0, rows_per_batch = 0, ranks = 1, rank = 0;
+    const char* addr = "127.0.0.1:29517";
+    const char* comm_kind = "nccl";
     for (int i = 7; i < argc; i++) {
         const char* a = argv[i];
         const char* v = (i + 1 < argc) ? argv[i + 1] : NULL;
@@ -101,6 +113,11 @@ int main(int argc, char** argv) {
         else if (!strcmp(a, "--rows-per-batch")) rows_per_batch = atoi(v);
         else if (!strcmp(a, "--device")) device = atoi(v);
         else if (!strcmp(a, "--semantics")) semantics = v;
+        else if (!strcmp(a, "--ranks")) ranks = atoi(v);
+        else if (!strcmp(a, "--rank")) rank = atoi(v);
+        else if (!strcmp(a, "--addr")) addr = v;
+        else if (!strcmp(a, "--comm")) comm_kind = v;
+        else if (!strcmp(a, "--comm-timeout")) comm_timeout = atof(v);
         else { LOG_ERROR("unknown option %s", a); return 1; }
         i++;
     }
@@ -113,6 +130,10 @@ int main(int argc, char** argv) {
         LOG_ERROR("--semantics must be exact or ref-cpu");
         return 1;
     }
+    if (ranks < 1 || rank < 0 || rank >= ranks) { LOG_ERROR("--rank must lie in 0..--ranks-1"); return 1; }
+    if (strcmp(comm_kind, "tcp") && strcmp(comm_kind, "nccl")) { LOG_ERROR("--comm must be tcp or nccl"); return 1; }
+    if (ranks > 1 && strcmp(mode, "search")) { LOG_ERROR("a multi-rank run needs --mode search"); return 1; }
+    g_quiet = rank != 0;
     double t_start = now_s();
     LOG_INFO("Graph Alignment Tool v1.0");
     LOG_INFO("Starting process with:");
@@ -182,6 +203,17 @@ int main(int argc, char** argv) {
         bm_rows_from_ordering(n, order_m, rows);
     }
 
+    bm_comm* comm = NULL;
+    if (ranks > 1) {
+        st = bm_comm_create(strcmp(comm_kind, "tcp") ? BM_COMM_NCCL : BM_COMM_TCP, rank, ranks, addr, comm_timeout,
+                            ctx, &comm);
+        if (st != BM_OK) {
+            LOG_ERROR("rank %d of %d: %s: %s", rank, ranks, bm_status_str(st), bm_ctx_last_error(ctx));
+            bm_ctx_destroy(ctx);
+            return 1;
+        }
+        LOG_INFO("Rank %d of %d (%s transport, rank 0 at %s)", rank, ranks, comm_kind, addr);
+    }
     int64_t initial = score;
     LOG_INFO("Starting optimization with initial score: %s", commas(initial, b1));
     bm_progress prog;
@@ -197,7 +229,9 @@ int main(int argc, char** argv) {
         int sw_left = max_sweeps >= 0 ? max_sweeps - prog.sweeps : -1;
         if (max_sweeps >= 0 && sw_left <= 0) break;
         int32_t sweeps_before = prog.sweeps;
-        if (!strcmp(mode, "parity"))
+        if (comm)
+            st = bm_search_sharded(ctx, comm, rows, rows ? n : 0, rows_per_batch, -1, chunk, &prog);
+        else if (!strcmp(mode, "parity"))
             st = bm_sweep_parity(ctx, rows, rows ? n : 0, acc_left, sw_left >= 0 ? sweeps_before + sw_left : -1,
                                  chunk, &prog);
         else
@@ -205,7 +239,7 @@ int main(int argc, char** argv) {
                                    sw_left >= 0 ? sweeps_before + sw_left : -1, chunk, 0, &prog);
         if (st != BM_OK && st != BM_TIMEOUT) {
             LOG_ERROR("%s: %s", bm_status_str(st), bm_ctx_last_error(ctx));
-            if (st != BM_PARITY_FAIL) { bm_ctx_destroy(ctx); return 1; }
+            if (st != BM_PARITY_FAIL || comm) { bm_comm_destroy(comm); bm_ctx_destroy(ctx); return 1; }
         }
         double el = now_s() - t0;
         LOG_INFO("Optimization progress:");
@@ -214,15 +248,28 @@ int main(int argc, char** argv) {
         LOG_INFO("  - Improvements found: %s", commas(prog.accepts, b1));
         LOG_INFO("  - Processing speed: %.1f nodes/sec, %.3g deltas/sec", el > 0 ? prog.rows_done / el : 0.0,
                  el > 0 ? prog.evaluated / el : 0.0);
-        if (now_s() - last_save >= save_interval || prog.converged || st == BM_OK) {
+        if (rank == 0 && (now_s() - last_save >= save_interval || prog.converged || st == BM_OK)) {
             bm_get_mapping(ctx, pi);
             if (bm_write_mapping(argv[6], n, pi) != 0) LOG_ERROR("Error creating file: %s", argv[6]);
             last_save = now_s();
         }
         if (prog.converged || st == BM_OK) break;
+        if (comm) {
+            /* the ranks' clocks differ: they stop together when any rank's budget is spent */
+            int64_t stops = 0;
+            const int my_stop = budget > 0 && budget - (now_s() - t0) <= 0;
+            if ((st = bm_comm_allreduce_sum(comm, my_stop, &stops)) != BM_OK) {
+                LOG_ERROR("%s: %s", bm_status_str(st), bm_comm_last_error(comm));
+                bm_comm_destroy(comm);
+                bm_ctx_destroy(ctx);
+                return 1;
+            }
+            if (stops > 0) break;
+        }
     }
+    bm_comm_destroy(comm);
     bm_get_mapping(ctx, pi);
-    if (bm_write_mapping(argv[6], n, pi) != 0) { LOG_ERROR("Error creating file: %s", argv[6]); return 1; }
+    if (rank == 0 && bm_write_mapping(argv[6], n, pi) != 0) { LOG_ERROR("Error creating file: %s", argv[6]); return 1; }
     int64_t final_dev = 0;
     bm_score(ctx, &final_dev);
     int64_t final_host = bm_host_score(&gm, &gf, pi);

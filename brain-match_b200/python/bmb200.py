@@ -143,6 +143,18 @@ def cuda_lib() -> C.CDLL:
             "bm_host_free_pinned": (C.c_int, [vp]),
             "bm_l2_flush": (C.c_int, [vp]),
             "bm_alloc_count": (C.c_uint64, []),
+            "bm_comm_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_char_p, C.c_double, vp,
+                                         C.POINTER(vp)]),
+            "bm_comm_destroy": (None, [vp]),
+            "bm_comm_last_error": (C.c_char_p, [vp]),
+            "bm_comm_barrier": (C.c_int, [vp]),
+            "bm_comm_allreduce_sum": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_int64)]),
+            "bm_comm_allgather_swaps": (C.c_int, [vp, vp, vp, C.c_int32, C.c_int32, vp, vp, C.POINTER(C.c_int32)]),
+            "bm_comm_island_best": (C.c_int, [vp, C.c_int64, vp, C.c_int32, C.POINTER(C.c_int64),
+                                              C.POINTER(C.c_int32)]),
+            "bm_search_sharded": (C.c_int, [vp, vp, vp, C.c_int32, C.c_int32, C.c_int64, C.c_double,
+                                            C.POINTER(Progress)]),
+            "bm_select_independent": (C.c_int, [vp, vp, vp, C.c_int32, vp, C.POINTER(C.c_int32)]),
             "bm_set_wait_limit": (C.c_int, [vp, C.c_int64]),
             "bm_probe_l2_bandwidth": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double)]),
             "bm_device_memory": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
@@ -504,6 +516,16 @@ class Engine:
                   "bm_rows_best")
         return out
 
+    def select_independent(self, pairs, deltas) -> np.ndarray:
+        """bm_select_independent: indices of the chosen candidates."""
+        p = _i32(np.asarray(pairs).reshape(-1))
+        d = np.ascontiguousarray(np.asarray(deltas, np.int64).reshape(-1))
+        chosen = np.zeros(max(1, d.shape[0]), np.int32)
+        nc = C.c_int32()
+        self._chk(self.L.bm_select_independent(self.h, _ptr(p), _ptr(d), d.shape[0], _ptr(chosen), C.byref(nc)),
+                  "bm_select_independent")
+        return chosen[:nc.value].copy()
+
     def apply_swaps(self, pairs, deltas=None) -> None:
         pairs = _i32(pairs).reshape(-1)
         d = None if deltas is None else np.ascontiguousarray(np.asarray(deltas, np.int64))
@@ -730,6 +752,77 @@ class Engine:
 
     def delta_pairs_dev(self, d_pairs: int, k: int, d_out: int) -> None:
         self._chk(self.L.bm_delta_pairs_dev(self.h, d_pairs, k, d_out), "bm_delta_pairs_dev")
+
+
+BM_COMM_TCP = 0
+BM_COMM_NCCL = 1
+
+
+class Comm:
+    """One rank of a sharded search (bm_comm): TCP sockets around rank 0, or
+    NCCL on an Engine's device.  Every method is collective."""
+
+    def __init__(self, kind: int, rank: int, world: int, addr: str | None = None, timeout: float = 60.0,
+                 eng: "Engine | None" = None):
+        self.L = cuda_lib()
+        h = C.c_void_p()
+        st = self.L.bm_comm_create(kind, rank, world, addr.encode() if addr else None, timeout,
+                                   eng.h if eng is not None else None, C.byref(h))
+        if st != BM_OK:
+            msg = self.L.bm_ctx_last_error(eng.h).decode() if eng is not None else ""
+            raise BMError(st, f"bm_comm_create: {msg}")
+        self.h, self.rank, self.world, self.eng = h, rank, world, eng
+
+    def _chk(self, st: int, what: str, ok=(BM_OK,)) -> int:
+        if st not in ok:
+            raise BMError(st, f"{what}: {self.L.bm_comm_last_error(self.h).decode()}")
+        return st
+
+    def barrier(self) -> None:
+        self._chk(self.L.bm_comm_barrier(self.h), "bm_comm_barrier")
+
+    def allreduce_sum(self, v: int) -> int:
+        t = C.c_int64()
+        self._chk(self.L.bm_comm_allreduce_sum(self.h, int(v), C.byref(t)), "bm_comm_allreduce_sum")
+        return t.value
+
+    def allgather_swaps(self, pairs, deltas, cap: int):
+        p = _i32(np.asarray(pairs).reshape(-1))
+        d = np.ascontiguousarray(np.asarray(deltas, np.int64).reshape(-1))
+        ap = np.zeros(2 * max(cap, 1), np.int32)
+        ad = np.zeros(max(cap, 1), np.int64)
+        tot = C.c_int32()
+        self._chk(self.L.bm_comm_allgather_swaps(self.h, _ptr(p), _ptr(d), d.shape[0], cap, _ptr(ap), _ptr(ad),
+                                                 C.byref(tot)), "bm_comm_allgather_swaps")
+        k = tot.value
+        return ap[:2 * k].reshape(-1, 2).copy(), ad[:k].copy()
+
+    def island_best(self, score: int, pi):
+        q = _i32(pi).copy()
+        bs, br = C.c_int64(), C.c_int32()
+        self._chk(self.L.bm_comm_island_best(self.h, int(score), _ptr(q), q.shape[0] - 1, C.byref(bs), C.byref(br)),
+                  "bm_comm_island_best")
+        return bs.value, br.value, q
+
+    def search_sharded(self, rows=None, rows_per_rank=0, max_rounds=-1, time_budget=0.0, prog=None):
+        prog = prog or Progress()
+        r = None if rows is None else _i32(rows)
+        st = self.L.bm_search_sharded(self.eng.h, self.h, None if r is None else _ptr(r),
+                                      0 if r is None else r.shape[0], rows_per_rank, max_rounds, time_budget,
+                                      C.byref(prog))
+        self.eng._chk(st, "bm_search_sharded", ok=(BM_OK, BM_TIMEOUT))
+        return prog, st
+
+    def close(self) -> None:
+        if self.h:
+            self.L.bm_comm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

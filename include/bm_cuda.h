@@ -310,6 +310,57 @@ bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32_t* chain_p
                             const int32_t* init_pi, const bm_sa_params* params, int32_t* final_pi,
                             int64_t* final_score, int64_t* accepts);
 
+/* ----------------------------------------------------- multi-rank search */
+
+/* Ranks of a sharded search, one process per GPU on a node, with no MPI and
+ * no PyTorch: the replacement of the reference's MPI drivers
+ * (src/graph-re-alignment-mpi-omp.c, src/graph-re-alignment-mpi-gpu.cu).
+ * BM_COMM_TCP: host sockets in a star around rank 0, which listens on addr
+ * ("host:port"); the others connect to it (retrying while it starts).  It
+ * needs no GPU (ctx may be NULL for the exchange calls).  BM_COMM_NCCL: NCCL
+ * (libnccl.so.2, loaded when asked for) over NVLink on ctx's device and
+ * stream; rank 0's socket carries only the ncclUniqueId (world 1 needs no
+ * address).  Every call below is collective: every rank makes the same calls
+ * in the same order.  Each wait is bounded by timeout_s: a rank that leaves or
+ * stops answering makes the others' calls return BM_TIMEOUT (an NCCL
+ * communicator is aborted then, and later calls return BM_TIMEOUT at once).
+ * bm_comm_last_error gives the message. */
+typedef struct bm_comm bm_comm;
+enum { BM_COMM_TCP = 0, BM_COMM_NCCL = 1 };
+bm_status bm_comm_create(int32_t kind, int32_t rank, int32_t world, const char* addr, double timeout_s, bm_ctx* ctx,
+                         bm_comm** out);
+void bm_comm_destroy(bm_comm* comm);
+const char* bm_comm_last_error(const bm_comm* comm);
+bm_status bm_comm_barrier(bm_comm* comm);
+/* Sum of value over the ranks (a consistency check of replicated state). */
+bm_status bm_comm_allreduce_sum(bm_comm* comm, int64_t value, int64_t* total);
+/* Candidate swaps of every rank, concatenated in rank order (each rank's in
+ * its own order): all_pairs gets 2 ints and all_deltas one value per
+ * candidate, *total their count (at most cap, else BM_INVALID_ARG). */
+bm_status bm_comm_allgather_swaps(bm_comm* comm, const int32_t* pairs, const int64_t* deltas, int32_t count, int32_t cap,
+                                  int32_t* all_pairs, int64_t* all_deltas, int32_t* total);
+/* Island synchronisation (sync_best_solutions,
+ * src/graph-re-alignment-mpi-omp.c:76-123): every rank adopts the mapping
+ * pi[0..n] of the rank with the best score (the lowest rank on ties), in
+ * place; best_score and best_rank (optional) receive the winner.  Scores
+ * must lie in 0..2^47. */
+bm_status bm_comm_island_best(bm_comm* comm, int64_t score, int32_t* pi, int32_t n, int64_t* best_score,
+                              int32_t* best_rank);
+/* Sharded batched search.  Round r takes world * rows_per_rank consecutive
+ * rows of row_order (cyclically; NULL = 1..n; rows_per_rank 0 = 2 x SMs) and
+ * each rank evaluates every world-th of them, from its rank on, on its GPU
+ * (best improving partner per row, the row argmax of
+ * src/re-alignment-parallel.c:598-618).  The candidates are all-gathered in
+ * rank order and every rank applies bm_select_independent's choice from the
+ * same list, so the replicated mapping stays identical on every rank with
+ * no broadcast.  Stops after max_rounds (-1: none), when a full pass applies
+ * nothing (converged), or after the round in which some rank's time budget
+ * ran out (BM_TIMEOUT; every rank stops there).  Ends with a full re-score
+ * and a comparison of the ranks' mappings (BM_PARITY_FAIL if they differ).
+ * All ranks must pass the same row_order, rows_per_rank and max_rounds. */
+bm_status bm_search_sharded(bm_ctx* ctx, bm_comm* comm, const int32_t* row_order, int32_t nrows,
+                            int32_t rows_per_rank, int64_t max_rounds, double time_budget_s, bm_progress* prog);
+
 /* ------------------------------------------------------------ delta table */
 
 /* The table of every pair's exact delta, the score-lookup engine of

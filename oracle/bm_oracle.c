@@ -407,7 +407,10 @@ int64_t orc_perm_delta(const orc_graph* gm, const orc_graph* gf, const int32_t* 
  * W1, W2 and w3 rounded to BF16 (nearest even); each hidden pre-activation
  * (sum + bias) rounded to FP32, then ReLU, then BF16; sums in FP64.  With
  * rounding == 0 everything stays FP64 (a smooth function, for checking the
- * backward formulas by finite differences).  Parameters packed as W1[24][128]
+ * backward formulas by finite differences).  rounding == 2 also rounds the
+ * backward signals dh2 and dh1 (pre-activation gradients of the two hidden
+ * layers) to BF16, as the tensor-core training kernel does (they are its MMA
+ * operands); the bias gradients then sum the rounded values.  Parameters packed as W1[24][128]
  * b1 W2[128][128] b2 w3 b3.  Writes out[k] when out != NULL and, when grads
  * != NULL, the gradient of mean((out - y)^2) and *loss. */
 #define ORC_IN 24
@@ -474,6 +477,7 @@ int orc_mlp(const float* w, const float* x, const float* y, int64_t k, int round
         for (int j = 0; j < ORC_H; j++) {
             grads[o_w3 + j] += d * h2[j];
             dh2[j] = h2[j] > 0.0 ? d * wr[o_w3 + j] : 0.0;
+            if (rounding == 2) dh2[j] = orc_bf16((float)dh2[j]);
             grads[o_b2 + j] += dh2[j];
         }
         for (int i = 0; i < ORC_H; i++) {
@@ -481,6 +485,7 @@ int orc_mlp(const float* w, const float* x, const float* y, int64_t k, int round
             if (h1[i] > 0.0) {
                 double a = 0.0;
                 for (int j = 0; j < ORC_H; j++) a += wr[o_w2 + i * ORC_H + j] * dh2[j];
+                if (rounding == 2) a = orc_bf16((float)a);
                 grads[o_b1 + i] += a;
                 for (int q = 0; q < ORC_IN; q++) grads[q * ORC_H + i] += xb[q] * a;
             }

@@ -265,7 +265,8 @@ def mlp_oracle(w, x, y=None, rounding=True):
         yy = np.ascontiguousarray(np.asarray(y, dtype=np.float32))
         grads = np.zeros(w.shape[0], np.float64)
     loss = C.c_double()
-    st = L.orc_mlp(_p(w), _p(x), _p(yy), k, int(bool(rounding)), _p(out), _p(grads), C.byref(loss))
+    mode = 2 if rounding == 2 else int(bool(rounding))  # 2: also the backward signals in BF16
+    st = L.orc_mlp(_p(w), _p(x), _p(yy), k, mode, _p(out), _p(grads), C.byref(loss))
     if st != 0:
         raise MemoryError("orc_mlp failed")
     return out, grads, loss.value

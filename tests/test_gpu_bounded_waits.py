@@ -60,3 +60,29 @@ def test_auction_bound_runs_out_and_context_recovers():
 def test_wait_limit_rejects_negative():
     with bm.Engine(0) as eng:
         assert eng.L.bm_set_wait_limit(eng.h, -5) == bm.BM_INVALID_ARG
+
+
+def test_training_mma_wait_runs_out_and_context_recovers(golden_small):
+    """The tensor-core training kernel's MMA-completion waits, run out the
+    same way: BM_TIMEOUT, then the same gradient as before."""
+    n, A, B = golden_graphs(golden_small)
+    eng = make_engine(n, A, B, golden_small["pi_init"])
+    try:
+        m = bm.Mlp(eng, seed=2)
+        rng = np.random.default_rng(9)
+        pairs = rng.integers(1, n + 1, (400, 2)).astype(np.int32)
+        pairs = pairs[pairs[:, 0] != pairs[:, 1]][:300]
+        x = m.pair_features(pairs)
+        y = rng.normal(0.0, 0.5, x.shape[0]).astype(np.float32)
+        g0, l0 = m.gradients(x, y)
+        assert eng.L.bm_set_wait_limit(eng.h, 1) == bm.BM_OK
+        with pytest.raises(bm.BMError) as ex:
+            m.gradients(x, y)
+        assert ex.value.status == bm.BM_TIMEOUT
+        assert eng.L.bm_set_wait_limit(eng.h, 0) == bm.BM_OK
+        g1, l1 = m.gradients(x, y)
+        # the same up to the order of the CTAs' atomic additions
+        assert np.linalg.norm(g1 - g0) <= 1e-5 * np.linalg.norm(g0)
+        assert abs(l1 - l0) <= 1e-6 * max(1.0, abs(l0))
+    finally:
+        eng.close()

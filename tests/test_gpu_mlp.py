@@ -104,18 +104,24 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def test_gradients_match_fp64_oracle(golden_cfg1):
+@pytest.mark.parametrize("backend,npairs", [(0, 512), (0, 1000), (1, 512)])
+def test_gradients_match_fp64_oracle(golden_cfg1, backend, npairs):
+    """Gradients of the tensor-core training kernel (backend 0; its backward
+    signals dh2, dh1 are BF16 MMA operands, and the oracle rounds them too)
+    and of the SIMT kernel (backend 1) against the FP64 replica; 1,000 records
+    leave the last 128-record tile partly filled."""
     n, A, B = golden_graphs(golden_cfg1)
     e = make_engine(n, A, B, golden_cfg1["pi_init"])
     m = bm.Mlp(e, seed=11)
+    m.set_backend(backend)
     rng = np.random.default_rng(5)
-    pairs = rng.integers(1, n + 1, (600, 2)).astype(np.int32)
-    pairs = pairs[pairs[:, 0] != pairs[:, 1]][:512]
+    pairs = rng.integers(1, n + 1, (npairs + 100, 2)).astype(np.int32)
+    pairs = pairs[pairs[:, 0] != pairs[:, 1]][:npairs]
     x = m.pair_features(pairs)
     y = rng.normal(0.0, 0.5, x.shape[0]).astype(np.float32)
     w = m.params()
     g, loss = m.gradients(x, y)
-    out_o, g_o, loss_o = mlp_oracle(w, x, y, rounding=True)
+    out_o, g_o, loss_o = mlp_oracle(w, x, y, rounding=2 if backend == 0 else True)
     # forward of the same features (SIMT kernel) against the replica
     out = m.score_features(x)
     assert np.max(np.abs(out - out_o)) <= 2e-3 * (1 + np.max(np.abs(out_o)))
