@@ -24,12 +24,13 @@
 //
 // Work per row is the number of 2-hop entries (about 10 per delta at the
 // full-scale workload) and every list is read as a coalesced stream.  Load
-// balance: first-hop items are cut into units of kSeg second-hop entries; the
-// warps of all CTAs of a thread-block cluster (1..8 CTAs per row) take the
-// row's units one at a time from a counter in the cluster's first CTA.  Each
-// CTA scatters into its own accumulator; after a cluster barrier each CTA sums
-// one slice of v across the cluster's accumulators through distributed shared
-// memory and finalises it.
+// balance: the second-hop lists of a chunk of first-hop items form one stream
+// of 16-byte quads; the warps of all CTAs of a thread-block cluster (1..8 CTAs
+// per row) claim ranges of kGrain quads from a counter in the cluster's first
+// CTA, and each lane walks its quads with a cursor on the list they fall in.
+// Each CTA scatters into its own accumulator; after a cluster barrier each CTA
+// sums one slice of v across the cluster's accumulators through distributed
+// shared memory and finalises it.
 //
 // Split rows.  A heavy row (a hub: up to 19 chunks of 1,024 first-hop items
 // and 7M 2-hop entries) is bound by its chunk count and its cluster's width.
@@ -53,11 +54,10 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr int kItemChunk = 1024;  // first-hop items staged per pass
-constexpr int kSeg = 512;         // second-hop entries per work unit
+constexpr int kGrain = 512;       // quads (4 second-hop entries each) per claimed range
 constexpr int kMaxCluster = 8;
 constexpr int kFinBatch = 2;     // groups of four columns a thread finalises per pass
 constexpr int kSideCap = 4096;    // A entries of u whose corrections go through shared memory
-constexpr int kMaxUnits = 4096;   // units per chunk with a unit -> item table (else binary search)
 constexpr int kItemCost = 32;     // work estimate: entries charged per first-hop item
 
 struct Partial {
@@ -119,9 +119,8 @@ __host__ __device__ inline size_t rows_smem_bytes(int32_t n) {
     return align16(sizeof(int32_t) * ((size_t)nvec_of(n) + 32))  // acc + one sink slot per lane
            + sizeof(void*) * kItemChunk                  // item base
            + sizeof(int32_t) * kItemChunk * 2            // len, cap
-           + sizeof(int32_t) * (kItemChunk + 4)          // unit prefix
-           + sizeof(int16_t) * kMaxUnits                 // unit -> item
-           + sizeof(int32_t) * 32                        // scan scratch + unit counters
+           + sizeof(int32_t) * (kItemChunk + 4)          // quad prefix
+           + sizeof(int32_t) * 32                        // scan scratch + range counters
            + sizeof(Partial) * (kMaxCluster + 32)        // cluster partials + warp partials
            + sizeof(int32_t) * 4;                        // split plan of this slot
 }
@@ -176,9 +175,8 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     p += sizeof(void*) * kItemChunk;
     int32_t* it_len = (int32_t*)p;
     int32_t* it_cap = it_len + kItemChunk;
-    int32_t* it_upre = it_cap + kItemChunk;
-    int16_t* unit_item = reinterpret_cast<int16_t*>(it_upre + kItemChunk + 4);
-    int32_t* scan_tmp = reinterpret_cast<int32_t*>(unit_item + kMaxUnits);  // [0..15] warp offsets, [29..30] unit counters
+    int32_t* it_upre = it_cap + kItemChunk;  // quad prefix of the items
+    int32_t* scan_tmp = it_upre + kItemChunk + 4;  // [0..15] warp offsets, [29..30] range counters
     Partial* parts = (Partial*)(scan_tmp + 32);  // [kMaxCluster] cluster partials
     Partial* wparts = parts + kMaxCluster;       // [32] warp partials
     int32_t* plan = reinterpret_cast<int32_t*>(wparts + 32);  // row, part, parts, last-arrival flag
@@ -214,9 +212,9 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             if (e < lim) asm volatile("prefetch.global.L2 [%0];" :: "l"(arr + e));
         }
     }
-    // Units are shared out across the whole cluster from counters in CTA 0's
-    // shared memory (one per chunk parity), so a CTA that shares its SM or
-    // also runs the corrections simply takes fewer units.
+    // Quad ranges are shared out across the whole cluster from counters in
+    // CTA 0's shared memory (one per chunk parity), so a CTA that shares its
+    // SM or also runs the corrections simply takes fewer ranges.
     int* cctr = scan_tmp + 29;
     if (crank == 0 && tid == 0) { cctr[0] = 0; cctr[1] = 0; }
     cluster.sync();
@@ -342,9 +340,9 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 it_base[li] = base;
                 it_len[li] = len;
                 it_cap[li] = cap;
-                tsum += (len + kSeg - 1) / kSeg;
+                tsum += len >> 2;  // quads (lists are padded to multiples of 4 entries)
             }
-            // ---- exclusive scan of units over the block
+            // ---- exclusive scan of quads over the block
             int32_t incl = tsum;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -371,100 +369,85 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                     const int32_t li = tid * IPT + k;
                     if (li >= cnt) break;
                     it_upre[li] = run;
-                    run += (it_len[li] + kSeg - 1) / kSeg;
+                    run += it_len[li] >> 2;
                 }
                 if (tid * IPT < cnt && (tid + 1) * IPT >= cnt) it_upre[cnt] = run;
             }
             __syncthreads();
-            // ---- unit -> item table (one shared load per unit instead of a
-            // binary search), when the chunk's units fit
-            const int32_t U = it_upre[cnt];
-            const bool table = U <= kMaxUnits;
-            // this slot's share of the chunk's units
-            const int32_t uhi = U;
-            if (table) {
-#pragma unroll
-                for (int k = 0; k < IPT; k++) {
-                    const int32_t li = tid * IPT + k;
-                    if (li >= cnt) break;
-                    for (int32_t x = it_upre[li]; x < it_upre[li + 1]; x++) unit_item[x] = (int16_t)li;
-                }
-                __syncthreads();
-            }
-            // ---- scatter: warps of every CTA of the cluster take this slot's
-            // units one at a time from the cluster counter.  A unit is at most
-            // kSeg entries of one list, read as 16-byte vectors (lists are
-            // padded to multiples of 4 entries and start 16-byte aligned).  The
-            // loop is software-pipelined: the next unit's loads are issued
-            // before the current unit's shared-memory atomics.
-            auto load_unit = [&](int32_t unit, uint4 (&q)[kSeg / 128], int32_t& cap) {
-                int32_t it;
-                if (table) {
-                    it = unit_item[unit];
-                } else {
-                    int32_t lo = 0, hi = cnt;  // last i with it_upre[i] <= unit
-                    while (hi - lo > 1) {
-                        const int32_t mid = (lo + hi) >> 1;
-                        if (it_upre[mid] <= unit) lo = mid; else hi = mid;
-                    }
-                    it = lo;
-                }
-                const int32_t s0 = (unit - it_upre[it]) * kSeg;
-                const int32_t nq = (min(it_len[it], s0 + kSeg) - s0) >> 2;
-                // the weight cap, with the unit's count of 32-quad rows above bit 16
-                cap = it_cap[it] | (((nq + 31) >> 5) << 16);
-                const uint4* b4 = reinterpret_cast<const uint4*>(it_base[it] + s0);
-#pragma unroll
-                for (int t = 0; t < kSeg / 128; t++) {
-                    const int qi = lane + 32 * t;
-                    // lanes past the unit's end add 0 to their own sink slot
-                    // past the accumulator (no branch around the atomics)
-                    const uint32_t sink = (uint32_t)(nv + lane);
-                    q[t] = (qi < nq) ? __ldg(b4 + qi) : make_uint4(sink, sink, sink, sink);
-                }
-            };
-            auto scatter = [&](const uint4 (&q)[kSeg / 128], int32_t cap) {
-                const int32_t cw = cap & 0xFFFF;
-#pragma unroll
-                for (int t = 0; t < kSeg / 128; t++) {
-                    if (t > 0 && (cap >> 16) <= t) break;  // warp-uniform: rows past the unit's end
-                    const uint32_t e4[4] = {q[t].x, q[t].y, q[t].z, q[t].w};
-#pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        atomicAdd(acc + bm_eid(e4[c]), imin(cw, bm_ew(e4[c])));
-                }
-            };
-            // two buffers alternate roles: the next unit's loads are issued
-            // before the current unit's atomics
-            // claiming a unit is issued (lane 0's atomic) before the current
-            // unit's scatter and read (the broadcast) after it, so the
-            // atomic's round trip overlaps the scatter
+            // ---- scatter: the chunk's second-hop lists form one stream of
+            // Q quads (16-byte vectors; lists are padded to multiples of four
+            // entries and start 16-byte aligned).  Warps of every CTA of the
+            // cluster claim ranges of kGrain quads from the cluster counter;
+            // lane l of a warp handles quads q0 + l + 32 j of its range, and
+            // keeps a cursor on the item (list) its quads fall in, which only
+            // moves forward.  Two quads per lane are loaded while the two
+            // before them are scattered.  Quads past the range are sinks with
+            // cap 0 (each lane its own slot past the accumulator).
+            const int32_t Q = it_upre[cnt];
             auto claim = [&]() -> int32_t {
                 int32_t k = 0;
                 if (lane == 0) asm volatile("atom.shared::cluster.add.u32 %0, [%1], 1;" : "=r"(k) : "r"(gctr));
                 return k;
             };
             auto claimed = [&](int32_t k) -> int32_t { return __shfl_sync(0xffffffffu, k, 0); };
-            uint4 qa[kSeg / 128], qb[kSeg / 128];
-            int32_t capa = 0, capb = 0;
-            int32_t ua = claimed(claim());
-            if (ua < uhi) {
-                load_unit(ua, qa, capa);
-                int32_t nxt = claimed(claim());  // qa holds a unit; nxt is the next to load
-                for (;;) {
-                    const bool hb = nxt < uhi;
-                    if (hb) load_unit(nxt, qb, capb);
-                    const int32_t kb = hb ? claim() : 0;
-                    scatter(qa, capa);
-                    if (!hb) break;
-                    const int32_t nn = claimed(kb);
-                    const bool ha = nn < uhi;
-                    if (ha) load_unit(nn, qa, capa);
-                    const int32_t ka = ha ? claim() : 0;
-                    scatter(qb, capb);
-                    if (!ha) break;
-                    nxt = claimed(ka);
+            int32_t it = 0, st = 0, en = 0, capv = 0;
+            const uint4* bp = nullptr;
+            const uint32_t sink = (uint32_t)(nv + lane);
+            auto fetch = [&](int32_t qq, int32_t qhi, uint4& out, int32_t& capo) {
+                if (qq < qhi) {
+                    while (qq >= en) {
+                        ++it;
+                        st = en;
+                        en = it_upre[it + 1];
+                        bp = reinterpret_cast<const uint4*>(it_base[it]);
+                        capv = it_cap[it];
+                    }
+                    out = __ldg(bp + (qq - st));
+                    capo = capv;
+                } else {
+                    out = make_uint4(sink, sink, sink, sink);
+                    capo = 0;
                 }
+            };
+            auto scatter4 = [&](const uint4& q4, int32_t cw) {
+                const uint32_t e4[4] = {q4.x, q4.y, q4.z, q4.w};
+#pragma unroll
+                for (int c = 0; c < 4; c++) atomicAdd(acc + bm_eid(e4[c]), imin(cw, bm_ew(e4[c])));
+            };
+            int32_t g = claimed(claim());
+            while ((int64_t)g * kGrain < Q) {
+                const int32_t qlo = g * kGrain, qhi = min(Q, qlo + kGrain);
+                const int32_t knext = claim();
+                // cursor: the item holding quad qlo + lane (binary search), set
+                // one item back so the first fetch loads its pointer and cap
+                {
+                    int32_t lo = 0, hi = cnt;  // last i with it_upre[i] <= q
+                    const int32_t q = min(qlo + lane, qhi - 1);
+                    while (hi - lo > 1) {
+                        const int32_t mid = (lo + hi) >> 1;
+                        if (it_upre[mid] <= q) lo = mid; else hi = mid;
+                    }
+                    it = lo - 1;
+                    en = it_upre[lo];
+                    st = en;
+                }
+                uint4 qa[2], qb[2];
+                int32_t ca[2], cb[2];
+                int32_t q = qlo + lane;
+                fetch(q, qhi, qa[0], ca[0]);
+                fetch(q + 32, qhi, qa[1], ca[1]);
+                for (; q < qhi; q += 128) {
+                    fetch(q + 64, qhi, qb[0], cb[0]);
+                    fetch(q + 96, qhi, qb[1], cb[1]);
+                    scatter4(qa[0], ca[0]);
+                    scatter4(qa[1], ca[1]);
+                    if (q + 64 >= qhi) break;
+                    fetch(q + 128, qhi, qa[0], ca[0]);
+                    fetch(q + 160, qhi, qa[1], ca[1]);
+                    scatter4(qb[0], cb[0]);
+                    scatter4(qb[1], cb[1]);
+                }
+                g = claimed(knext);
             }
             if (c0 + kItemChunk < Fs) cluster.sync(); else __syncthreads();
         }

@@ -30,8 +30,12 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "bm_internal.cuh"
 #include "bm_rng.hpp"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -96,8 +100,9 @@ constexpr int kSaApplyRowCap = 4096;  // entries per staged row in the swap appl
 // in `stage` (4 x kSaApplyRowCap entries of shared memory; longer rows use
 // the hash).  `pi` is the working copy (shared or global memory), `gpi` the
 // chain's mapping in global memory, updated too.
+template <int CL>
 __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, int32_t* ov, int32_t sa, int32_t sb,
-                                  uint32_t* stage) {
+                                  uint32_t* stage, int crank) {
     const int32_t fa = pi[sa], fb = pi[sb];
     // rows: 0 = out(fa), 1 = out(fb), 2 = in(fa), 3 = in(fb)
     int32_t rlen[4];
@@ -132,7 +137,7 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
         const int32_t fme = side ? fb : fa, fnew = side ? fa : fb;
         {
             const int32_t b = __ldg(P.Aout_ptr + me), e = __ldg(P.Aout_ptr + me + 1);
-            for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+            for (int32_t j = b + (int32_t)threadIdx.x + crank * (int32_t)blockDim.x; j < e; j += CL * (int32_t)blockDim.x) {
                 const uint32_t ent = __ldg(P.Aout_ent + j);
                 if (ent == 0) continue;
                 const int32_t x = bm_eid(ent), w = bm_ew(ent);
@@ -148,7 +153,7 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
         }
         {
             const int32_t b = __ldg(P.Ain_ptr + me), e = __ldg(P.Ain_ptr + me + 1);
-            for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+            for (int32_t j = b + (int32_t)threadIdx.x + crank * (int32_t)blockDim.x; j < e; j += CL * (int32_t)blockDim.x) {
                 const uint32_t ent = __ldg(P.Ain_ent + j);
                 if (ent == 0) continue;
                 const int32_t x = bm_eid(ent), w = bm_ew(ent);
@@ -159,16 +164,20 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
             }
         }
     }
-    __syncthreads();
+    // every read of the mapping (both CTAs of a pair) before it changes
+    if constexpr (CL > 1) cg::this_cluster().sync(); else __syncthreads();
     if (threadIdx.x == 0) {
-        pi[sa] = fb;
-        pi[sb] = fa;
-        if (gpi != pi) {
+        if (pi != gpi || crank == 0) {
+            pi[sa] = fb;
+            pi[sb] = fa;
+        }
+        if (gpi != pi && crank == 0) {
             gpi[sa] = fb;
             gpi[sb] = fa;
         }
     }
-    __syncthreads();
+    // the mapping and the overlap updates of both CTAs seen by both
+    if constexpr (CL > 1) cg::this_cluster().sync(); else __syncthreads();
 }
 
 // One CTA runs one chain.  Each iteration draws the proposals of steps
@@ -190,9 +199,14 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
 // to the acceptance rate: it doubles (up to kSaMaxK) after an iteration with
 // no acceptance and drops to max(a.K, 2 (j + 1)) after the j-th proposal is
 // accepted; a function of the chain's own history, so replays are exact.
-__global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
+template <int CL>
+__device__ __forceinline__ void sa_chain_body(const SaArgs& a) {
     extern __shared__ __align__(16) uint32_t s_dyn[];
-    const int c = blockIdx.x;
+    // CL CTAs (a cluster) run one chain: they draw the same proposals, split
+    // the evaluation's items and the swap apply's list entries, and read each
+    // other's per-proposal sums through distributed shared memory
+    const int c = blockIdx.x / CL;
+    const int crank = CL > 1 ? (int)cg::this_cluster().block_rank() : 0;
     if (c >= a.nchains) return;
     constexpr int kSeg = 4 * kSaMaxK;
     constexpr int kW = kSaThreads / 32;
@@ -323,14 +337,16 @@ __global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
                 }
                 asm volatile("cp.async.commit_group;" ::: "memory");
             };
+            constexpr int kStride = CL * kW;  // the chain's warps over all its CTAs
+            const int gw = crank * kW + warp;
             Stage cur, nxt, far;
-            fetch(warp, cur);
-            fetch(warp + kW, nxt);
+            fetch(gw, cur);
+            fetch(gw + kStride, nxt);
             copy_row(cur, 0);
             int buf = 0;
-            for (int32_t item = warp; item < U; item += kW) {
+            for (int32_t item = gw; item < U; item += kStride) {
                 copy_row(nxt, buf ^ 1);
-                fetch(item + 2 * kW, far);
+                fetch(item + 2 * kStride, far);
                 asm volatile("cp.async.wait_group 1;" ::: "memory");  // this item's row has landed
                 __syncwarp();
                 const uint32_t* row = rowbuf + (size_t)buf * kSaRowCap;
@@ -378,11 +394,17 @@ __global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
             __syncwarp();
         }
         __syncthreads();
+        if constexpr (CL > 1) cg::this_cluster().sync();  // every CTA's sums are complete
         // ---- deltas and acceptance, one thread per proposal; the first
-        // accepted one in step order wins
+        // accepted one in step order wins (each CTA of a pair decides alike)
         if (tid < K && step + (uint64_t)tid < end) {
             const bm_proposal pr = s_prop[tid];
-            long long d = (long long)s_sum[tid] - (long long)ov[pr.u] - (long long)ov[pr.v];
+            long long sum = s_sum[tid];
+            if constexpr (CL > 1) {
+#pragma unroll
+                for (int q = 1; q < CL; q++) sum += *cg::this_cluster().map_shared_rank(s_sum + tid, (crank + q) % CL);
+            }
+            long long d = sum - (long long)ov[pr.u] - (long long)ov[pr.v];
             if (P.has_self) {
                 const int32_t fu = pi[pr.u], fv = pi[pr.v];
                 const int32_t su = __ldg(P.selfA + pr.u), sv = __ldg(P.selfA + pr.v);
@@ -401,19 +423,29 @@ __global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) {
             accepts++;
             step += (uint64_t)first + 1;
             K = min(kSaMaxK, max(a.K, 2 * (first + 1)));
-            chain_apply_block(P, pi, gpi, ov, pr.u, pr.v, s_dyn);  // ends with a barrier
+            chain_apply_block<CL>(P, pi, gpi, ov, pr.u, pr.v, s_dyn, crank);  // ends with a (cluster) barrier
             if (tid == 0) s_first = kSaMaxK;
         } else {
             step = min(end, step + (uint64_t)K);
             K = min(kSaMaxK, 2 * K);
+            // the other CTA's reads of these sums end before they are reset
+            if constexpr (CL > 1) cg::this_cluster().sync();
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && crank == 0) {
         ch.step = step;
         ch.score = score;
         ch.accepts = accepts;
     }
+}
+
+__global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) { sa_chain_body<1>(a); }
+
+// One chain per pair of CTAs (a cluster of two on two SMs), for batches with
+// fewer chains than half the SMs.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSaThreads, 1) sa_chain_kernel_pair(SaArgs a) {
+    sa_chain_body<2>(a);
 }
 
 // Initial S(v) and score of every chain: a warp per (chain, A vertex).
@@ -590,7 +622,16 @@ bm_status chain_smem(bm_ctx* ctx, SaArgs& args, int32_t n_max, size_t* smem) {
         *smem += need;
     }
     BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+    BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
     return BM_OK;
+}
+
+// One launch of the chains: a CTA per chain, or a pair of CTAs per chain.
+void launch_chains(const SaArgs& args, int32_t ctas_per_chain, size_t smem, cudaStream_t stream) {
+    if (ctas_per_chain == 2)
+        sa_chain_kernel_pair<<<args.nchains * 2, kSaThreads, smem, stream>>>(args);
+    else
+        sa_chain_kernel<<<args.nchains, kSaThreads, smem, stream>>>(args);
 }
 
 }  // namespace
@@ -678,21 +719,32 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
         bm_status st = chain_smem(ctx, args, n_max, &smem);
         if (st != BM_OK) return st;
     }
+    // CTAs per chain: a pair when the chains fill at most half the SMs (the
+    // tuner may keep one); a fixed K keeps the pair rule
+    int32_t CLc = (2 * nchains <= ctx->num_sms) ? 2 : 1;
     if (K == 0) {
         int64_t ntot = 0;
         for (int32_t c = 0; c < nchains; c++) ntot += b->pairs[(size_t)chain_pair[c]].n;
         cudaDeviceProp prop;
         cudaGetDeviceProperties(&prop, ctx->device);
         const std::string key = std::string(prop.name) + "|" + std::to_string(ntot) + "|" + std::to_string(nchains);
-        if (!tune_lookup(key, &K)) {
-            // time a short prefix of the real run for each K and keep the
-            // fastest; the chain does not depend on K, so the prefix is
-            // simply replayed by the real run below
+        int32_t tuned = 0;
+        if (tune_lookup(key, &tuned)) {
+            K = tuned & 0xFF;
+            CLc = (tuned >> 8) == 2 ? 2 : 1;
+            if (CLc == 2 && 2 * nchains > ctx->num_sms) CLc = 1;
+            if (K < 1 || K > kmax) K = 8;
+        } else {
+            // time a short prefix of the real run for each (K, CTAs per
+            // chain) and keep the fastest; the chain depends on neither, so
+            // the prefix is simply replayed by the real run below
             float best_ms = 1e30f;
-            int32_t best_k = 8;
+            int32_t best_k = 8, best_cl = 1;
             std::vector<ChainDev> snap = hc;
-            for (int32_t cand : {1, 2, 4, 8, 16}) {
-                if (cand > kmax) break;
+            const int32_t max_cl = (2 * nchains <= ctx->num_sms) ? 2 : 1;
+            for (int32_t trial = 0; trial < 5 * max_cl; trial++) {
+                const int32_t cand = 1 << (trial % 5), cl = 1 + trial / 5;
+                if (cand > kmax) continue;
                 BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
                 BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
                 BM_CUDA(ctx, cudaMemcpyAsync(d_ch, snap.data(), sizeof(ChainDev) * (size_t)nchains, cudaMemcpyHostToDevice, ctx->stream));
@@ -708,16 +760,17 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
                 BM_CUDA(ctx, cudaEventCreate(&ev.a));
                 BM_CUDA(ctx, cudaEventCreate(&ev.b));
                 BM_CUDA(ctx, cudaEventRecord(ev.a, ctx->stream));
-                sa_chain_kernel<<<nchains, kSaThreads, smem, ctx->stream>>>(t);
+                launch_chains(t, cl, smem, ctx->stream);
                 BM_LAUNCH_CHECK(ctx, "sa_chain_kernel(tune)");
                 BM_CUDA(ctx, cudaEventRecord(ev.b, ctx->stream));
                 BM_CUDA(ctx, cudaEventSynchronize(ev.b));
                 float ms = 0;
                 cudaEventElapsedTime(&ms, ev.a, ev.b);
-                if (ms < best_ms) { best_ms = ms; best_k = cand; }
+                if (ms < best_ms) { best_ms = ms; best_k = cand; best_cl = cl; }
             }
             K = best_k;
-            tune_store(key, K);
+            CLc = best_cl;
+            tune_store(key, K | (CLc << 8));
             // restart from the initial state
             BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
             BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
@@ -734,7 +787,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
         cudaGraphExec_t exec = nullptr;
         args.K = K;
         BM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        sa_chain_kernel<<<nchains, kSaThreads, smem, ctx->stream>>>(args);
+        launch_chains(args, CLc, smem, ctx->stream);
         cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
         if (ce != cudaSuccess) return bm_cuda_fail(ctx, ce, "cudaStreamEndCapture");
         ce = cudaGraphInstantiate(&exec, graph, 0);
@@ -759,6 +812,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
     }
     if (stats) {
         stats->candidates = K;
+        stats->ctas_per_chain = CLc;
         stats->launches = (int64_t)launches;
         stats->seconds = secs;
     }
@@ -825,6 +879,7 @@ bm_status bm_noalloc_setup(bm_ctx* ctx) {
     cudaFuncAttributes fa;
     BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_init_kernel));
     BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel));
+    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel_pair));  // its smem limit is set by every chain call
     return BM_OK;
 }
 

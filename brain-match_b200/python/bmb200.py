@@ -64,7 +64,8 @@ class SaParams(C.Structure):
 
 
 class SaStats(C.Structure):
-    _fields_ = [("candidates", C.c_int32), ("launches", C.c_int64), ("seconds", C.c_double)]
+    _fields_ = [("candidates", C.c_int32), ("ctas_per_chain", C.c_int32), ("launches", C.c_int64),
+                ("seconds", C.c_double)]
 
 
 class LearnedParams(C.Structure):

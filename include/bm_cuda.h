@@ -262,15 +262,19 @@ typedef struct bm_sa_params {
     int64_t steps;       /* proposals per chain */
     double t0;           /* starting temperature */
     double t_end;        /* final temperature: T_i = t0 * exp(ln(t_end/t0) * i / steps) */
-    int32_t candidates;  /* proposals evaluated together per iteration at the start, 1..16; 0 = autotuned.
-                          * Each chain then adapts it (up to 64) to its own acceptances: doubled after an
-                          * iteration with none, 2 (j + 1) after the j-th is accepted. */
+    int32_t candidates;  /* proposals evaluated together per iteration at the start, 1..16; 0 = autotuned
+                          * (with the CTAs per chain: 1, or a pair of CTAs when the chains fill at most
+                          * half the SMs; the tuner times a prefix of the run for each choice and caches
+                          * the best per device, sizes and chain count).  Each chain then adapts it (up
+                          * to 64) to its own acceptances: doubled after an iteration with none,
+                          * 2 (j + 1) after the j-th is accepted. */
     int64_t chunk;       /* proposals per chain per kernel launch (0 = 65536) */
 } bm_sa_params;
 
 typedef struct bm_sa_stats {
-    int32_t candidates;  /* value used */
-    int64_t launches;    /* graph replays */
+    int32_t candidates;      /* value used */
+    int32_t ctas_per_chain;  /* 1, or 2: a pair of CTAs (a cluster) per chain */
+    int64_t launches;        /* graph replays */
     double seconds;      /* wall time of the chain launches */
 } bm_sa_stats;
 

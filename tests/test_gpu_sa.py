@@ -33,6 +33,7 @@ def test_chains_replay_on_cpu(pairs, candidates):
     pis, scores, acc, st = batch.sa_run(chain_pair, keys, inits, steps, t0=5.0, t_end=0.01,
                                         candidates=candidates, chunk=1000)
     assert st.candidates == candidates and st.launches == 6
+    assert st.ctas_per_chain == 2  # 5 chains fill at most half the SMs: a pair of CTAs per chain
     for c, p in enumerate(chain_pair):
         A, B, init = pairs[p]
         orc = Oracle(A.n, (A.src, A.dst, A.w), (B.src, B.dst, B.w))
@@ -73,5 +74,32 @@ def test_uneven_batch_autotuned(tmp_path, monkeypatch):
         assert bm.check_bijection(p1[c]) == 0
         assert s1[c] == bm.host_score(A, B, p1[c])
     assert (tmp_path / "tune.txt").exists()
+    batch.close()
+    eng.close()
+
+
+def test_chains_one_cta_each_replay_on_cpu():
+    """More chains than half the SMs: one CTA per chain (the other kernel
+    instantiation); chains still replay bit for bit."""
+    eng = bm.Engine(0)
+    batch = bm.Batch(eng)
+    pairs = []
+    for seed, n, m in ((51, 160, 1200), (52, 220, 2000)):
+        A, B, truth, init = bm.gen_pair(1, n=n, m_target=m, seed=seed)
+        batch.add_pair(A, B)
+        pairs.append((A, B, init))
+    nch = 80
+    chain_pair = [c % 2 for c in range(nch)]
+    keys = [700 + c for c in range(nch)]
+    inits = [pairs[p][2] for p in chain_pair]
+    steps = 3000
+    pis, scores, acc, st = batch.sa_run(chain_pair, keys, inits, steps, t0=5.0, t_end=0.01, candidates=4, chunk=1000)
+    assert st.ctas_per_chain == 1
+    for c in (0, 1, 41, 79):
+        A, B, init = pairs[chain_pair[c]]
+        orc = Oracle(A.n, (A.src, A.dst, A.w), (B.src, B.dst, B.w))
+        pi_o, s_o, a_o = orc.sa(init, keys[c], steps, 5.0, 0.01)
+        np.testing.assert_array_equal(pis[c], pi_o)
+        assert scores[c] == s_o and acc[c] == a_o
     batch.close()
     eng.close()
