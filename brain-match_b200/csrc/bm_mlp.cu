@@ -60,7 +60,17 @@ constexpr int kImgW3 = 16 * 128 * 2;   // N=16 x K=128: w3 in row 0, zeros elsew
 constexpr int kImgEp = (3 * BM_MLP_H + 4) * 4;
 constexpr int kImgW2T = 128 * 128 * 2;  // N=128 in x K=128 out
 constexpr int kImgOffW2T = kImgW1 + kImgW2 + kImgW3 + kImgEp;
-constexpr int kImgBytes = kImgOffW2T + kImgW2T;
+// The row scorer's image follows, with the biases folded into the products:
+// each layer's input gets two constant-one columns (K = 24, 25 of layer 1's
+// 32; K = 128, 129 of a 144-wide hidden input), and the weights' matching
+// columns hold the bias as a pair of BF16 values, hi = bf16(b) and
+// lo = bf16(b - hi), so the FP32 accumulator receives b to about 2^-16.
+constexpr int kHK = 144;                   // hidden input width of the scorer's layers 2 and 3
+constexpr int kImgW1S = 128 * 32 * 2;      // N=128 hidden x K=32
+constexpr int kImgW2S = 128 * kHK * 2;     // N=128 out x K=144
+constexpr int kImgW3S = 16 * kHK * 2;      // N=16 x K=144: w3 and b3 in row 0
+constexpr int kImgOffS = kImgOffW2T + kImgW2T;
+constexpr int kImgBytes = kImgOffS + kImgW1S + kImgW2S + kImgW3S;
 
 }  // namespace
 
@@ -566,15 +576,16 @@ __global__ void gather_batch_kernel(const uint16_t* __restrict__ rx, const float
 // rewritten only after the MMA that reads it has signalled completion.
 
 constexpr int kTcThreads = 128;
-constexpr uint32_t kSmW1 = 0;
-constexpr uint32_t kSmW2 = kSmW1 + kImgW1;          // 8192
-constexpr uint32_t kSmW3 = kSmW2 + kImgW2;          // 40960
-constexpr uint32_t kSmH = kSmW3 + kImgW3;           // 45056: h1 / h2 operand (32 KB)
-constexpr uint32_t kSmX = kSmH + 128 * 128 * 2;     // 77824: features operand (8 KB)
-constexpr uint32_t kSmEp = kSmX + 128 * 32 * 2;     // 86016: b1, b2, w3, b3
-constexpr uint32_t kSmBits = kSmEp + kImgEp;        // 87568
+constexpr uint32_t kSmW1 = 0;                       // the scorer image: W1 (bias columns 24, 25)
+constexpr uint32_t kSmW2 = kSmW1 + kImgW1S;         // 8192: W2, K = 144 (bias columns 128, 129)
+constexpr uint32_t kSmW3 = kSmW2 + kImgW2S;         // 45056: w3 and b3, K = 144
+constexpr uint32_t kSmH = 49 * 1024;                // 50176: h1 / h2 operand, K = 144 (36 KB)
+constexpr uint32_t kSmX = kSmH + 128 * kHK * 2;     // 87040: features operand, K = 32 (8 KB)
+constexpr uint32_t kSmBits = kSmX + 128 * 32 * 2;   // 95232
 constexpr uint32_t kTcMinSmem = 100 * 1024;         // at most 2 CTAs (2 x 256 TMEM columns) per SM
-static_assert(kSmBits % 16 == 0 && kSmH % 1024 == 0 && kSmX % 1024 == 0, "operand layout");
+static_assert(kSmW3 + kImgW3S <= kSmH && kSmBits % 16 == 0 && kSmH % 1024 == 0 && kSmX % 1024 == 0,
+              "operand layout");
+constexpr uint32_t kBf16One2 = 0x3F803F80u;         // two BF16 ones, packed
 
 __host__ __device__ constexpr uint32_t bits_words(int32_t n) { return (uint32_t)(n + 32) / 32u; }
 __host__ __device__ constexpr uint32_t tc_tail(int32_t n) { return kSmBits + ((2u * bits_words(n) * 4u + 15u) & ~15u); }
@@ -690,13 +701,22 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long l
 }
 
 __global__ void prep_image_kernel(const float* __restrict__ w, unsigned char* __restrict__ img) {
-    unsigned short* w1 = reinterpret_cast<unsigned short*>(img + kSmW1);
-    unsigned short* w2 = reinterpret_cast<unsigned short*>(img + kSmW2);
-    unsigned short* w3 = reinterpret_cast<unsigned short*>(img + kSmW3);
+    // the training image: W1, W2, W3, the epilogue vectors, W2^T
+    unsigned short* w1 = reinterpret_cast<unsigned short*>(img);
+    unsigned short* w2 = reinterpret_cast<unsigned short*>(img + kImgW1);
+    unsigned short* w3 = reinterpret_cast<unsigned short*>(img + kImgW1 + kImgW2);
     float* ep = reinterpret_cast<float*>(img + kImgW1 + kImgW2 + kImgW3);
     unsigned short* w2t = reinterpret_cast<unsigned short*>(img + kImgOffW2T);
+    unsigned short* s1 = reinterpret_cast<unsigned short*>(img + kImgOffS);
+    unsigned short* s2 = reinterpret_cast<unsigned short*>(img + kImgOffS + kImgW1S);
+    unsigned short* s3 = reinterpret_cast<unsigned short*>(img + kImgOffS + kImgW1S + kImgW2S);
     const int n1 = 128 * 32, n2 = 128 * 128, n3 = 16 * 128;
-    const int total = n1 + n2 + n3 + 3 * 128 + 4 + n2;
+    const int nt = n1 + n2 + n3 + 3 * 128 + 4 + n2;  // the training image
+    const int total = nt + n1 + 128 * kHK + 16 * kHK;
+    // a bias as the BF16 pair (hi, lo) of a folded column
+    auto hi = [](float b) { return bf16r(b); };
+    auto lo = [](float b) { return bf16r(b - bf16r(b)); };
+    auto put = [](unsigned short* p, float v) { *p = (unsigned short)(__float_as_uint(v) >> 16); };
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         if (t < n1) {
             const int j = t / 32, i = t % 32;  // hidden j (N), input i (K)
@@ -716,10 +736,25 @@ __global__ void prep_image_kernel(const float* __restrict__ w, unsigned char* __
             else if (q < 256) ep[q] = w[kOffB2 + q - 128];
             else if (q < 384) ep[q] = bf16r(w[kOffW3 + q - 256]);
             else ep[q] = (q == 384) ? w[kOffB3] : 0.f;
-        } else {
+        } else if (t < nt) {
             const int q = t - (n1 + n2 + n3 + 3 * 128 + 4), i = q / 128, j = q % 128;  // in i (N), out j (K)
             const float v = bf16r(w[kOffW2 + i * BM_MLP_H + j]);
             w2t[kmajor_off(i, j, 128) / 2] = (unsigned short)(__float_as_uint(v) >> 16);
+        } else if (t < nt + n1) {
+            const int q = t - nt, j = q / 32, i = q % 32;  // hidden j (N), input i (K)
+            const float b = w[kOffB1 + j];
+            const float v = i < BM_MLP_IN ? bf16r(w[i * BM_MLP_H + j]) : i == 24 ? hi(b) : i == 25 ? lo(b) : 0.f;
+            put(s1 + kmajor_off(j, i, 32) / 2, v);
+        } else if (t < nt + n1 + 128 * kHK) {
+            const int q = t - nt - n1, j = q / kHK, i = q % kHK;  // out j (N), in i (K)
+            const float b = w[kOffB2 + j];
+            const float v = i < 128 ? bf16r(w[kOffW2 + i * BM_MLP_H + j]) : i == 128 ? hi(b) : i == 129 ? lo(b) : 0.f;
+            put(s2 + kmajor_off(j, i, kHK) / 2, v);
+        } else {
+            const int q = t - nt - n1 - 128 * kHK, j = q / kHK, i = q % kHK;  // row j (N = 16), in i (K)
+            const float b = w[kOffB3];
+            const float v = j != 0 ? 0.f : i < 128 ? bf16r(w[kOffW3 + i]) : i == 128 ? hi(b) : i == 129 ? lo(b) : 0.f;
+            put(s3 + kmajor_off(j, i, kHK) / 2, v);
         }
     }
 }
@@ -741,22 +776,21 @@ struct TcArgs {
 };
 
 // Hidden-layer epilogue: this thread's accumulator row (128 FP32 columns at
-// taddr) plus bias, ReLU, BF16, stored as its row of the next A operand.
-__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* __restrict__ bias, unsigned char* sm,
-                                                int tid) {
+// taddr; the bias is already in it), ReLU, BF16, stored as its row of the
+// next A operand.
+__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, unsigned char* sm, int tid) {
 #pragma unroll 1
     for (int c = 0; c < 4; c++) {
         float d[32];
         tmem_ld32(taddr + 32u * c, d);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const float* bq = bias + 32 * c + 8 * q;
             uint4 o;
-            o.x = cvt_relu_bf16x2(d[8 * q + 0] + bq[0], d[8 * q + 1] + bq[1]);
-            o.y = cvt_relu_bf16x2(d[8 * q + 2] + bq[2], d[8 * q + 3] + bq[3]);
-            o.z = cvt_relu_bf16x2(d[8 * q + 4] + bq[4], d[8 * q + 5] + bq[5]);
-            o.w = cvt_relu_bf16x2(d[8 * q + 6] + bq[6], d[8 * q + 7] + bq[7]);
-            *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 32 * c + 8 * q, 128)) = o;
+            o.x = cvt_relu_bf16x2(d[8 * q + 0], d[8 * q + 1]);
+            o.y = cvt_relu_bf16x2(d[8 * q + 2], d[8 * q + 3]);
+            o.z = cvt_relu_bf16x2(d[8 * q + 4], d[8 * q + 5]);
+            o.w = cvt_relu_bf16x2(d[8 * q + 6], d[8 * q + 7]);
+            *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 32 * c + 8 * q, kHK)) = o;
         }
     }
 }
@@ -782,7 +816,7 @@ __device__ __forceinline__ void build_features(const TcArgs& a, const float* ta,
     }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        uint4 q = make_uint4(0u, 0u, 0u, 0u);
+        uint4 q = make_uint4(kBf16One2, 0u, 0u, 0u);  // columns 24, 25: the bias inputs
         if (c < 3) {
             q.x = cvt_bf16x2(x[8 * c + 0], x[8 * c + 1]);
             q.y = cvt_bf16x2(x[8 * c + 2], x[8 * c + 3]);
@@ -814,11 +848,12 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + tail + 24);
     const uint32_t bar1 = smem_u32(&bars[0]), bar2 = smem_u32(&bars[1]), bar3 = smem_u32(&bars[2]);
 
-    {  // weights into shared memory; epilogue vectors after the operand buffers
-        const uint4* src = reinterpret_cast<const uint4*>(a.img);
-        for (int i = tid; i < (kImgW1 + kImgW2 + kImgW3) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
-        for (int i = tid; i < kImgEp / 16; i += kTcThreads)
-            reinterpret_cast<uint4*>(sm + kSmEp)[i] = src[(kImgW1 + kImgW2 + kImgW3) / 16 + i];
+    {  // the scorer image into shared memory; this thread's constant H
+       // columns (128, 129: the bias inputs of layers 2 and 3)
+        const uint4* src = reinterpret_cast<const uint4*>(a.img + kImgOffS);
+        for (int i = tid; i < (kImgW1S + kImgW2S + kImgW3S) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
+        *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 128, kHK)) = make_uint4(kBf16One2, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 136, kHK)) = make_uint4(0u, 0u, 0u, 0u);
     }
     if (tid == 0) {
         mbar_init(bar1, 1);
@@ -837,7 +872,6 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
     const uint32_t tm_1 = tmem + lane_base;         // layer 1 (columns 0..127)
     const uint32_t tm_2 = tmem + 128u + lane_base;  // layer 2, then the output layer (columns 128..)
-    const float* ep = reinterpret_cast<const float*>(sm + kSmEp);
     const uint32_t sW1 = smem_u32(sm + kSmW1), sW2 = smem_u32(sm + kSmW2), sW3 = smem_u32(sm + kSmW3);
     const uint32_t sH = smem_u32(sm + kSmH), sX = smem_u32(sm + kSmX);
     uint32_t phase = 0;  // parity of the current tile's completions (each barrier completes once per tile)
@@ -886,13 +920,13 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
             // layer 1 done: its epilogue fills H with h1
             if (!__syncthreads_and(mbar_wait(bar1, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
-            hidden_epilogue(tm_1, ep, sm, tid);
+            hidden_epilogue(tm_1, sm, tid);
             tc_handoff();
-            if (tid == 0) {  // layer 2
+            if (tid == 0) {  // layer 2, K = 144 (b2 in columns 128, 129)
 #pragma unroll
-                for (int s = 0; s < 8; s++)
-                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, 2048u),
-                             smem_desc(sW2 + 256u * s, 128u, 2048u), kIdesc128, s > 0);
+                for (int s = 0; s < kHK / 16; s++)
+                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, kHK / 8 * 128u),
+                             smem_desc(sW2 + 256u * s, 128u, kHK / 8 * 128u), kIdesc128, s > 0);
                 mma_commit(bar2);
             }
             last_bar = bar2;
@@ -908,13 +942,13 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
             // layer 2 done: its epilogue writes h2 over h1
             if (!__syncthreads_and(mbar_wait(bar2, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
-            hidden_epilogue(tm_2, ep + 128, sm, tid);
+            hidden_epilogue(tm_2, sm, tid);
             tc_handoff();
-            if (tid == 0) {  // output layer, N = 16 (row 0 of B holds w3), into columns 128..143
+            if (tid == 0) {  // output layer, N = 16 (row 0 of B holds w3 and b3), into columns 128..143
 #pragma unroll
-                for (int s = 0; s < 8; s++)
-                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, 2048u),
-                             smem_desc(sW3 + 256u * s, 128u, 2048u), kIdesc16, s > 0);
+                for (int s = 0; s < kHK / 16; s++)
+                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, kHK / 8 * 128u),
+                             smem_desc(sW3 + 256u * s, 128u, kHK / 8 * 128u), kIdesc16, s > 0);
                 mma_commit(bar3);
             }
             last_bar = bar3;
@@ -922,7 +956,7 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
             if (!__syncthreads_and(mbar_wait(bar3, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
             const float o = tmem_ld1(tm_2);
-            if (v <= a.n) out_row[v - 1] = (v != u) ? o + ep[384] : -INFINITY;
+            if (v <= a.n) out_row[v - 1] = (v != u) ? o : -INFINITY;
             phase ^= 1u;
             tc_fence_before();
             __syncthreads();

@@ -627,3 +627,188 @@ extern "C" bm_status bm_select_independent(bm_ctx* ctx, const int32_t* pairs, co
     *nchosen = c;
     return BM_OK;
 }
+
+// ------------------------------------------------ similarity-filtered pass
+//
+// The single pass of optimize_mapping in the reference's graph-alignment
+// variant (src/graph-alignment.c:489-595): m1 and m2 run over the vertex list
+// nodes[] (the variant's order of first appearance); the swap (m1, m2) is
+// evaluated only when the similarity of the swapped images beats the current
+// one (:545-553), and a positive delta is applied at once.  The engine
+// evaluates K consecutive rows at a time under the current mapping (the row
+// kernel, whole rows), then one CTA per row finds the first position p (from
+// the row's start position on) whose vertex passes the filter with a positive
+// delta; rows before the first row with such a position are what the serial
+// pass scanned, that position is its next accept, and the rest is evaluated
+// again after the swap (as bm_sweep_parity).  The similarity is computed in
+// FP64 with the variant's operations in its order, each rounded on its own
+// (no fused multiply-add), so the decisions are the variant's.
+
+namespace {
+
+constexpr int kSimThreads = 256;
+
+// calculate_node_similarity (src/graph-alignment.c:274-284): -(0.7 x (5|d in|
+// + 5|d out| + |d avg in| + |d avg out|) + 0.3 x |d rank|); a, b: five
+// metrics (in, out, avg in, avg out, rank).
+__device__ __forceinline__ double node_similarity(const double* a, const double* b) {
+    double s = __dmul_rn(5.0, fabs(__dsub_rn(a[0], b[0])));
+    s = __dadd_rn(s, __dmul_rn(5.0, fabs(__dsub_rn(a[1], b[1]))));
+    s = __dadd_rn(s, fabs(__dsub_rn(a[2], b[2])));
+    s = __dadd_rn(s, fabs(__dsub_rn(a[3], b[3])));
+    const double o = fabs(__dsub_rn(a[4], b[4]));
+    return -__dadd_rn(__dmul_rn(0.7, s), __dmul_rn(0.3, o));
+}
+
+// Per row r (u = rows[r]): the first position p >= start[r] of nodes[] with
+// v = nodes[p] != u, delta(u, v) > 0 and the similarity filter passed; out_pos
+// gets p (or nnodes when none), out_delta its delta.
+__global__ void __launch_bounds__(kSimThreads) sim_first_kernel(const int64_t* __restrict__ full, int32_t n,
+                                                                const int32_t* __restrict__ rows,
+                                                                const int32_t* __restrict__ start,
+                                                                const int32_t* __restrict__ nodes, int32_t nnodes,
+                                                                const int32_t* __restrict__ pi,
+                                                                const double* __restrict__ ma,
+                                                                const double* __restrict__ mb, int32_t* out_pos,
+                                                                long long* out_delta) {
+    __shared__ int32_t s_best;
+    const int r = blockIdx.x;
+    const int32_t u = rows[r];
+    const int64_t* row = full + (size_t)r * ((size_t)n + 1);
+    const int32_t f1 = pi[u];
+    if (threadIdx.x == 0) s_best = nnodes;
+    __syncthreads();
+    // positions in blocks of the CTA's width, so the first hit ends the scan
+    for (int32_t p0 = start[r]; p0 < nnodes; p0 += kSimThreads) {
+        const int32_t p = p0 + (int32_t)threadIdx.x;
+        if (p < nnodes) {
+            const int32_t v = nodes[p];
+            if (v != u && row[v] > 0) {
+                const int32_t f2 = pi[v];
+                const double cur = __dadd_rn(node_similarity(ma + 5 * (size_t)u, mb + 5 * (size_t)f1),
+                                             node_similarity(ma + 5 * (size_t)v, mb + 5 * (size_t)f2));
+                const double swp = __dadd_rn(node_similarity(ma + 5 * (size_t)u, mb + 5 * (size_t)f2),
+                                             node_similarity(ma + 5 * (size_t)v, mb + 5 * (size_t)f1));
+                if (swp > cur) atomicMin(&s_best, p);
+            }
+        }
+        __syncthreads();
+        if (s_best < nnodes) break;
+    }
+    if (threadIdx.x == 0) {
+        const int32_t p = s_best;
+        out_pos[r] = p;
+        out_delta[r] = p < nnodes ? (long long)row[nodes[p]] : 0;
+    }
+}
+
+}  // namespace
+
+extern "C" bm_status bm_sweep_similarity(bm_ctx* ctx, const int32_t* nodes, int32_t nnodes, const double* metrics_a,
+                                         const double* metrics_b, int64_t max_accepts, double time_budget_s,
+                                         bm_progress* prog) {
+    bm_status s = bm_require_mapped(ctx);
+    if (s != BM_OK) return s;
+    if (!prog || !nodes || !metrics_a || !metrics_b || nnodes < 1)
+        return bm_fail(ctx, BM_INVALID_ARG, "vertex list, metrics and progress are required");
+    if ((s = bm_rows_smem_check(ctx)) != BM_OK) return s;
+    const int32_t n = ctx->n;
+    if (nnodes > n) return bm_fail(ctx, BM_INVALID_ARG, "%d listed vertices for n = %d", nnodes, n);
+    {
+        std::vector<char> seen((size_t)n + 1, 0);
+        for (int32_t i = 0; i < nnodes; i++) {
+            const int32_t v = nodes[i];
+            if (v < 1 || v > n || seen[(size_t)v]) return bm_fail(ctx, BM_INVALID_ARG, "nodes[%d] = %d: bad or repeated", i, v);
+            seen[(size_t)v] = 1;
+        }
+    }
+    const int32_t kmax = std::max(1, std::min(nnodes, ctx->num_sms));
+    // device copies: the list, both metric tables, whole rows and the per-row answers
+    const size_t nb = ((size_t)nnodes * 4 + 255) & ~(size_t)255;
+    const size_t mbytes = sizeof(double) * 5 * ((size_t)n + 1);
+    const size_t fb = sizeof(int64_t) * (size_t)kmax * ((size_t)n + 1);
+    const size_t small = 4 * (((size_t)kmax * 8 + 255) & ~(size_t)255);
+    void* dev = nullptr;
+    BM_CUDA(ctx, bm_cuda_malloc(&dev, nb + 2 * mbytes + fb + small));
+    struct Free {
+        void* p;
+        ~Free() { bm_cuda_free(p); }
+    } guard{dev};
+    char* d = static_cast<char*>(dev);
+    int32_t* d_nodes = reinterpret_cast<int32_t*>(d);
+    double* d_ma = reinterpret_cast<double*>(d + nb);
+    double* d_mb = reinterpret_cast<double*>(d + nb + mbytes);
+    int64_t* d_full = reinterpret_cast<int64_t*>(d + nb + 2 * mbytes);
+    char* sm = d + nb + 2 * mbytes + fb;
+    const size_t sstep = ((size_t)kmax * 8 + 255) & ~(size_t)255;
+    int32_t* d_rows = reinterpret_cast<int32_t*>(sm);
+    int32_t* d_start = reinterpret_cast<int32_t*>(sm + sstep);
+    int32_t* d_pos = reinterpret_cast<int32_t*>(sm + 2 * sstep);
+    long long* d_delta = reinterpret_cast<long long*>(sm + 3 * sstep);
+    BM_CUDA(ctx, cudaMemcpyAsync(d_nodes, nodes, sizeof(int32_t) * (size_t)nnodes, cudaMemcpyHostToDevice, ctx->stream));
+    BM_CUDA(ctx, cudaMemcpyAsync(d_ma, metrics_a, mbytes, cudaMemcpyHostToDevice, ctx->stream));
+    BM_CUDA(ctx, cudaMemcpyAsync(d_mb, metrics_b, mbytes, cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = bm_rows_refresh_work(ctx)) != BM_OK) return s;
+    std::vector<int32_t> h_rows((size_t)kmax), h_start((size_t)kmax), h_pos((size_t)kmax);
+    std::vector<long long> h_delta((size_t)kmax);
+    const auto t0 = clk::now();
+    int32_t pos = prog->next_row_pos, col = prog->next_col;  // row position; column position (0-based)
+    if (pos < 0 || pos >= nnodes) pos = 0;
+    if (col < 0 || col >= nnodes) col = 0;
+    int64_t accepts0 = prog->accepts;
+    int32_t K = 1;
+    prog->converged = 0;
+    bm_status ret = BM_OK;
+    while (pos < nnodes) {
+        if (max_accepts >= 0 && prog->accepts - accepts0 >= max_accepts) break;
+        if (time_budget_s > 0 && secs_since(t0) >= time_budget_s) { ret = BM_TIMEOUT; break; }
+        const int32_t k = std::min(K, nnodes - pos);
+        for (int32_t i = 0; i < k; i++) {
+            h_rows[(size_t)i] = nodes[pos + i];
+            h_start[(size_t)i] = (i == 0) ? col : 0;
+        }
+        BM_CUDA(ctx, cudaMemcpyAsync(d_rows, h_rows.data(), sizeof(int32_t) * (size_t)k, cudaMemcpyHostToDevice, ctx->stream));
+        BM_CUDA(ctx, cudaMemcpyAsync(d_start, h_start.data(), sizeof(int32_t) * (size_t)k, cudaMemcpyHostToDevice, ctx->stream));
+        if ((s = bm_launch_rows(ctx, d_rows, nullptr, k, d_full, nullptr, h_rows.data())) != BM_OK) return s;
+        sim_first_kernel<<<k, kSimThreads, 0, ctx->stream>>>(d_full, n, d_rows, d_start, d_nodes, nnodes, ctx->pi, d_ma,
+                                                             d_mb, d_pos, d_delta);
+        BM_LAUNCH_CHECK(ctx, "sim_first_kernel");
+        BM_CUDA(ctx, cudaMemcpyAsync(h_pos.data(), d_pos, sizeof(int32_t) * (size_t)k, cudaMemcpyDeviceToHost, ctx->stream));
+        BM_CUDA(ctx, cudaMemcpyAsync(h_delta.data(), d_delta, sizeof(long long) * (size_t)k, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+        BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        prog->launches++;
+        prog->evaluated += (int64_t)k * (n - 1);
+        int32_t hit = -1;
+        for (int32_t i = 0; i < k; i++)
+            if (h_pos[(size_t)i] < nnodes) { hit = i; break; }
+        if (hit >= 0) {
+            const int32_t u = h_rows[(size_t)hit], p = h_pos[(size_t)hit], v = nodes[p];
+            const int32_t pr[2] = {u, v};
+            BM_CUDA(ctx, cudaMemcpyAsync(d_rows, pr, sizeof pr, cudaMemcpyHostToDevice, ctx->stream));
+            if ((s = bm_launch_apply(ctx, d_rows, 1)) != BM_OK) return s;
+            BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            ctx->score += h_delta[(size_t)hit];
+            prog->accepts++;
+            prog->rows_done += hit;
+            pos += hit;
+            col = p + 1;
+            if (col >= nnodes) { pos++; col = 0; prog->rows_done++; }
+            K = std::max(1, K / 2);
+        } else {
+            prog->rows_done += k;
+            pos += k;
+            col = 0;
+            K = std::min(kmax, K * 2);
+        }
+    }
+    if (pos >= nnodes) { prog->sweeps++; pos = 0; col = 0; }
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    prog->next_row_pos = pos;
+    prog->next_col = col;
+    prog->seconds += secs_since(t0);
+    s = verify_score(ctx);
+    prog->score = ctx->score;
+    if (s != BM_OK) return s;
+    return ret;
+}

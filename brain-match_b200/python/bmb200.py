@@ -156,6 +156,7 @@ def cuda_lib() -> C.CDLL:
             "bm_search_sharded": (C.c_int, [vp, vp, vp, C.c_int32, C.c_int32, C.c_int64, C.c_double,
                                             C.POINTER(Progress)]),
             "bm_select_independent": (C.c_int, [vp, vp, vp, C.c_int32, vp, C.POINTER(C.c_int32)]),
+            "bm_sweep_similarity": (C.c_int, [vp, vp, C.c_int32, vp, vp, C.c_int64, C.c_double, C.POINTER(Progress)]),
             "bm_set_wait_limit": (C.c_int, [vp, C.c_int64]),
             "bm_probe_l2_bandwidth": (C.c_int, [vp, C.c_int64, C.c_int32, C.POINTER(C.c_double)]),
             "bm_device_memory": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
@@ -248,6 +249,8 @@ def host_lib() -> C.CDLL:
             "bm_ordering_by_weighted_degree": (None, [C.POINTER(Edges), vp]),
             "bm_rows_from_ordering": (None, [C.c_int32, vp, vp]),
             "bm_greedy_match": (C.c_int, [C.POINTER(Edges), C.POINTER(Edges), vp]),
+            "bm_first_appearance": (C.c_int, [C.POINTER(Edges), vp, C.POINTER(C.c_int32)]),
+            "bm_node_metrics": (C.c_int, [C.POINTER(Edges), vp, vp]),
             "bm_host_score": (C.c_int64, [C.POINTER(Edges), C.POINTER(Edges), vp]),
             "bm_check_bijection": (C.c_int32, [C.c_int32, vp]),
         }
@@ -372,6 +375,26 @@ def rows_from_ordering(order: np.ndarray) -> np.ndarray:
     rows = np.zeros(n, np.int32)
     host_lib().bm_rows_from_ordering(n, _ptr(order), _ptr(rows))
     return rows
+
+
+def first_appearance(g: Graph) -> np.ndarray:
+    """bm_first_appearance: vertices in order of first appearance in g's edges."""
+    out = np.zeros(max(1, g.n), np.int32)
+    cnt = C.c_int32()
+    e = g.edges_struct()
+    if host_lib().bm_first_appearance(C.byref(e), _ptr(out), C.byref(cnt)) != 0:
+        raise RuntimeError("bm_first_appearance failed")
+    return out[:cnt.value].copy()
+
+
+def node_metrics(g: Graph, rank=None) -> np.ndarray:
+    """bm_node_metrics: (n+1) x 5 doubles (in, out, avg in, avg out, rank)."""
+    out = np.zeros((g.n + 1) * 5, np.float64)
+    r = None if rank is None else _i32(rank)
+    e = g.edges_struct()
+    if host_lib().bm_node_metrics(C.byref(e), None if r is None else _ptr(r), _ptr(out)) != 0:
+        raise RuntimeError("bm_node_metrics failed")
+    return out.reshape(g.n + 1, 5)
 
 
 def greedy_match(A: Graph, B: Graph) -> np.ndarray:
@@ -516,6 +539,17 @@ class Engine:
         self._chk(self.L.bm_rows_best(self.h, _ptr(rows), None if cl is None else _ptr(cl), rows.shape[0], _ptr(out)),
                   "bm_rows_best")
         return out
+
+    def sweep_similarity(self, nodes, metrics_a, metrics_b, max_accepts=-1, time_budget=0.0, prog=None):
+        """bm_sweep_similarity: one similarity-filtered pass; returns (Progress, status)."""
+        prog = prog or Progress()
+        nd = _i32(nodes)
+        ma = np.ascontiguousarray(np.asarray(metrics_a, np.float64))
+        mb = np.ascontiguousarray(np.asarray(metrics_b, np.float64))
+        st = self.L.bm_sweep_similarity(self.h, _ptr(nd), nd.shape[0], _ptr(ma), _ptr(mb), max_accepts, time_budget,
+                                        C.byref(prog))
+        self._chk(st, "bm_sweep_similarity", ok=(BM_OK, BM_TIMEOUT))
+        return prog, st
 
     def select_independent(self, pairs, deltas) -> np.ndarray:
         """bm_select_independent: indices of the chosen candidates."""

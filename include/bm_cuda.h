@@ -183,6 +183,21 @@ bm_status bm_search_batched(bm_ctx* ctx, const int32_t* row_order, int32_t nrows
                             int32_t rows_per_batch, int64_t max_accepts, int32_t max_sweeps,
                             double time_budget_s, int64_t target_score, bm_progress* prog);
 
+/* The single pass of optimize_mapping in the reference's graph-alignment
+ * variant (src/graph-alignment.c:489-595), with its similarity filter
+ * (:545-553): m1 and then m2 run over nodes[0..nnodes) (the variant's vertex
+ * list, bm_first_appearance in bm_host.h); the swap is evaluated only when
+ * calculate_node_similarity (:274-284, FP64, the same operations in the same
+ * order) of the swapped images beats the current pair's, and a positive delta
+ * is applied at once.  metrics_a, metrics_b: five doubles per vertex id
+ * 0..n of each graph (bm_node_metrics).  One pass, resumable through
+ * prog->next_row_pos / next_col (positions in nodes[]); stops early after
+ * max_accepts (-1: none) or the time budget (BM_TIMEOUT).  The deltas follow
+ * bm_set_semantics: BM_SEMANTICS_REF_CPU reproduces the variant on graphs
+ * with self-loops too. */
+bm_status bm_sweep_similarity(bm_ctx* ctx, const int32_t* nodes, int32_t nnodes, const double* metrics_a,
+                              const double* metrics_b, int64_t max_accepts, double time_budget_s, bm_progress* prog);
+
 /* Deterministic independent-subset selection of candidate swaps (pairs[2i],
  * pairs[2i+1]) with deltas[i]: among delta > 0, in descending delta then
  * ascending index, a swap is taken when neither endpoint lies in the closed A

@@ -116,6 +116,19 @@ int32_t bm_check_bijection(int32_t n, const int32_t* pi);
 int bm_select_independent_host(const bm_edges* A, const int32_t* pairs, const int64_t* deltas, int32_t count,
                                int32_t* chosen, int32_t* nchosen);
 
+/* Inputs of the similarity-filtered pass (bm_sweep_similarity in
+ * bm_cuda.h), as the reference's graph-alignment variant builds them:
+ * bm_first_appearance writes the vertices in order of first appearance in
+ * the edge list, the source then the target of each edge (its g->nodes,
+ * add_node from add_edge, src/graph-alignment.c:159-200; nodes needs n
+ * entries); bm_node_metrics writes calculate_node_metrics (:235-272) for the
+ * listed vertices, five doubles per vertex id 0..n: in-degree, out-degree,
+ * the weight total of both directions over the in-degree and over the
+ * out-degree, and rank[v] (the ordering rank; NULL gives 0); unlisted
+ * vertices get zeros.  Both return 0, or -1 on a bad id or no memory. */
+int bm_first_appearance(const bm_edges* e, int32_t* nodes, int32_t* count);
+int bm_node_metrics(const bm_edges* e, const int32_t* rank, double* metrics);
+
 /* SplitMix64 step and a uniform double in [0,1) — the generator's RNG. */
 uint64_t bm_splitmix64(uint64_t* state);
 

@@ -105,3 +105,21 @@ def test_bijection_check():
     assert bm.check_bijection(np.array([0, 1, 2, 3], np.int32)) == 0
     assert bm.check_bijection(np.array([0, 1, 1, 3], np.int32)) == 2
     assert bm.check_bijection(np.array([0, 1, 2, 4], np.int32)) == 3
+
+
+def test_first_appearance_and_node_metrics():
+    """The graph-alignment variant's vertex list (add_node order) and its
+    calculate_node_metrics, against a direct computation."""
+    src = np.array([5, 2, 5, 7, 2, 9], np.int32)
+    dst = np.array([2, 7, 9, 5, 5, 9], np.int32)
+    w = np.array([3, 1, 4, 1, 5, 9], np.int32)
+    g = bm.Graph(10, src, dst, w)
+    np.testing.assert_array_equal(bm.first_appearance(g), [5, 2, 7, 9])
+    rank = np.arange(11, dtype=np.int32) * 10
+    m = bm.node_metrics(g, rank)
+    for v in range(11):
+        outd, ind = int((src == v).sum()), int((dst == v).sum())
+        tot = int(w[src == v].sum() + w[dst == v].sum())
+        listed = v in (5, 2, 7, 9)
+        exp = [ind, outd, tot / ind if ind else 0.0, tot / outd if outd else 0.0, rank[v]] if listed else [0] * 5
+        np.testing.assert_array_equal(m[v], np.array(exp, np.float64))
