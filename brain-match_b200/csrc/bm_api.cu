@@ -157,6 +157,9 @@ extern "C" void bm_ctx_destroy(bm_ctx* ctx) {
     if (ctx->hstage) bm_cuda_host_free(ctx->hstage);
     if (ctx->h_slots) bm_cuda_host_free(ctx->h_slots);
     if (ctx->slots_ev) cudaEventDestroy(ctx->slots_ev);
+    if (ctx->row_fork) cudaEventDestroy(ctx->row_fork);
+    if (ctx->row_join) cudaEventDestroy(ctx->row_join);
+    if (ctx->row_side) cudaStreamDestroy(ctx->row_side);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -553,6 +556,19 @@ extern "C" bm_status bm_set_row_split(bm_ctx* ctx, int32_t slots) {
 extern "C" bm_status bm_get_row_split(bm_ctx* ctx, int32_t* slots) {
     if (!ctx || !slots) return BM_INVALID_ARG;
     *slots = ctx->row_split;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_set_row_tiers(bm_ctx* ctx, int32_t heavy_rows) {
+    if (!ctx) return BM_INVALID_ARG;
+    if (heavy_rows < -1) return bm_fail(ctx, BM_INVALID_ARG, "heavy_rows must be -1 (off), 0 (automatic) or a row count");
+    ctx->row_tiers = heavy_rows;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_get_row_tiers(bm_ctx* ctx, int32_t* heavy_rows) {
+    if (!ctx || !heavy_rows) return BM_INVALID_ARG;
+    *heavy_rows = ctx->row_tiers;
     return BM_OK;
 }
 

@@ -107,6 +107,12 @@ struct bm_ctx {
     int32_t split_n = 0;
     int32_t split_slots_max = 0;
     int split_active[2 * 9] = {};   // resident clusters per (threads, cluster size); 0 = not queried
+    // tiered row launches: 0 = automatic, -1 = off, k > 0 = at most k rows in
+    // the wider tier; the second stream and its fork/join events
+    int32_t row_tiers = 0;
+    cudaStream_t row_side = nullptr;
+    cudaEvent_t row_fork = nullptr;
+    cudaEvent_t row_join = nullptr;
     // host copy of A's adjacency (independence tests of batched swaps)
     std::vector<int32_t> hA_optr, hA_iptr;
     std::vector<uint32_t> hA_oent, hA_ient;

@@ -109,6 +109,11 @@ struct RowArgs {
     unsigned* scnt;     // [nrows][kMaxCluster] slot arrivals per slice (self-resetting)
     unsigned* rcnt;     // [nrows] slice arrivals per row (self-resetting)
     Partial* rpart;     // [nrows][kMaxCluster] slice reductions
+    // tiered launches: slot s takes the row whose work estimate ranks
+    // rank_lo + s among the launch's rows (descending, ties by position);
+    // null = slot s takes row s
+    const int32_t* rank_work;
+    int32_t rank_lo;
 };
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -183,7 +188,27 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
 
     // plan[0..2]: row, part of the row, parts of the row.  Read back from
     // shared memory where needed (short register live ranges).
-    if (tid == 0) {
+    if (a.rank_work) {
+        // rank the launch's rows (at most kItemChunk) by their work estimate;
+        // it_len is free until the first item chunk is staged
+        int32_t* wr = it_len;
+        if (tid == 0) { plan[0] = -1; plan[1] = 0; plan[2] = 1; }
+        for (int32_t j = tid; j < a.nrows; j += THREADS) {
+            const int32_t uj = __ldg(a.rows + j);
+            wr[j] = (uj >= 1 && uj <= n) ? __ldg(a.rank_work + uj) : -1;
+        }
+        __syncthreads();
+        const int32_t want = a.rank_lo + slot;
+        for (int32_t j = tid; j < a.nrows; j += THREADS) {
+            const int32_t wj = wr[j];
+            int32_t rk = 0;
+            for (int32_t k = 0; k < a.nrows; k++) {
+                const int32_t wk = wr[k];
+                rk += (wk > wj || (wk == wj && k < j)) ? 1 : 0;
+            }
+            if (rk == want) plan[0] = j;
+        }
+    } else if (tid == 0) {
         if (a.slots) {
             const int4 d = __ldg(a.slots + slot);
             plan[0] = d.x; plan[1] = d.y; plan[2] = d.z;
@@ -683,7 +708,7 @@ __global__ void __launch_bounds__(kWorkThreads) row_work_kernel(RowArgs a, int32
 }
 
 template <int THREADS, bool REFCPU>
-bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem) {
+bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem, cudaStream_t stream) {
     static bool configured[64] = {false};
     auto kern = rows_kernel<THREADS, REFCPU>;
     if (!configured[ctx->device & 63]) {
@@ -694,7 +719,7 @@ bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem) {
     cfg.gridDim = dim3((unsigned)(args.nslots * cl), 1, 1);
     cfg.blockDim = dim3(THREADS, 1, 1);
     cfg.dynamicSmemBytes = smem;
-    cfg.stream = ctx->stream;
+    cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)cl;
@@ -822,6 +847,28 @@ int32_t host_split_plan(const bm_ctx* ctx, const int32_t* h_rows, int32_t nrows,
     return (int32_t)out.size();
 }
 
+// Rows of a launch of nrows rows in cl-CTA clusters that go to the 2 cl tier:
+// the most that keep both launches within kTierFill of the resident CTA
+// slots (measured at 57 rows in 4-CTA clusters: 6 rows in 8-CTA clusters
+// +8 %, 8 rows put clusters in a second wave), capped by the caller's
+// setting.
+constexpr double kTierFill = 0.85;
+
+int32_t tier_rows(bm_ctx* ctx, int32_t nrows, int cl, size_t smem, bm_status* st) {
+    *st = BM_OK;
+    int& cap = ctx->split_active[(ctx->row_threads == 256 ? 0 : 1) * (kMaxCluster + 1) + 1];
+    if (cap == 0) {
+        *st = (ctx->row_threads == 256) ? max_clusters_t<256>(ctx, 1, smem, &cap) : max_clusters_t<512>(ctx, 1, smem, &cap);
+        if (*st != BM_OK) return 0;
+        if (cap <= 0) cap = -1;
+    }
+    if (cap <= 0) return 0;
+    const int64_t budget = (int64_t)(kTierFill * cap) - (int64_t)nrows * cl;
+    int64_t h = budget > 0 ? std::min<int64_t>(nrows, budget / cl) : 0;
+    if (ctx->row_tiers > 0) h = std::min<int64_t>(h, ctx->row_tiers);
+    return (int32_t)h;
+}
+
 }  // namespace
 
 bm_status bm_rows_smem_check(bm_ctx* ctx) {
@@ -933,6 +980,48 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
             }
         }
     }
+    auto launch = [&](const RowArgs& x, int c, cudaStream_t strm) -> bm_status {
+        if (x.refcpu)
+            return (ctx->row_threads == 256) ? launch_rows_t<256, true>(ctx, x, c, smem, strm)
+                                             : launch_rows_t<512, true>(ctx, x, c, smem, strm);
+        return (ctx->row_threads == 256) ? launch_rows_t<256, false>(ctx, x, c, smem, strm)
+                                         : launch_rows_t<512, false>(ctx, x, c, smem, strm);
+    };
+    args.rank_work = nullptr;
+    args.rank_lo = 0;
+    // Tiers: when the launch leaves resident CTA slots free, the H rows with
+    // the largest work estimate (ranked on the device) get clusters of 2 cl
+    // in a launch on a second stream, concurrent with the cl-CTA launch of
+    // the others.  A launch waits on its heaviest row, and a row's scatter
+    // rate grows with its CTAs.  The two launches together stay within
+    // kTierFill of the resident CTA slots: mixed cluster sizes fragment the
+    // GPCs, and a cluster left for a second wave costs more than the tier
+    // saves.
+    const int32_t H = (args.slots || ctx->row_ctas != 0 || ctx->row_tiers < 0 || cl >= kMaxCluster || !ctx->rwork ||
+                       nrows > kItemChunk)
+                          ? 0 : tier_rows(ctx, nrows, cl, smem, &st);
+    if (st != BM_OK) return st;
+    if (H > 0) {
+        if (!ctx->row_side) {
+            BM_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->row_side, cudaStreamNonBlocking));
+            BM_CUDA(ctx, cudaEventCreateWithFlags(&ctx->row_fork, cudaEventDisableTiming));
+            BM_CUDA(ctx, cudaEventCreateWithFlags(&ctx->row_join, cudaEventDisableTiming));
+        }
+        RowArgs hv = args, lt = args;
+        hv.nrows = lt.nrows = nrows;
+        hv.rank_work = lt.rank_work = ctx->rwork;
+        hv.rank_lo = 0;
+        hv.nslots = H;
+        lt.rank_lo = H;
+        lt.nslots = nrows - H;
+        BM_CUDA(ctx, cudaEventRecord(ctx->row_fork, ctx->stream));
+        BM_CUDA(ctx, cudaStreamWaitEvent(ctx->row_side, ctx->row_fork, 0));
+        if ((st = launch(hv, 2 * cl, ctx->row_side)) != BM_OK) return st;
+        BM_CUDA(ctx, cudaEventRecord(ctx->row_join, ctx->row_side));
+        if (H < nrows && (st = launch(lt, cl, ctx->stream)) != BM_OK) return st;
+        BM_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->row_join, 0));
+        return BM_OK;
+    }
     // grid.x is limited to 2^31-1; chunk very long row lists
     const int32_t max_rows_per_launch = 1 << 20;
     for (int32_t r0 = 0; r0 < nrows; r0 += max_rows_per_launch) {
@@ -944,13 +1033,7 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
         ar.full = d_full ? d_full + (size_t)r0 * ((size_t)ctx->n + 1) : nullptr;
         ar.res = d_res ? d_res + r0 : nullptr;
         ar.colout = d_colout ? d_colout + (size_t)r0 * (size_t)ncols : nullptr;
-        if (ar.refcpu)
-            st = (ctx->row_threads == 256) ? launch_rows_t<256, true>(ctx, ar, cl, smem)
-                                           : launch_rows_t<512, true>(ctx, ar, cl, smem);
-        else
-            st = (ctx->row_threads == 256) ? launch_rows_t<256, false>(ctx, ar, cl, smem)
-                                           : launch_rows_t<512, false>(ctx, ar, cl, smem);
-        if (st != BM_OK) return st;
+        if ((st = launch(ar, cl, ctx->stream)) != BM_OK) return st;
     }
     return BM_OK;
 }

@@ -169,6 +169,8 @@ def cuda_lib() -> C.CDLL:
             "bm_rows_max_active_clusters": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
             "bm_set_row_tiling": (C.c_int, [vp, C.c_int32, C.c_int32]),
             "bm_set_row_split": (C.c_int, [vp, C.c_int32]),
+            "bm_set_row_tiers": (C.c_int, [vp, C.c_int32]),
+            "bm_get_row_tiers": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "bm_set_semantics": (C.c_int, [vp, C.c_int32]),
             "bm_get_semantics": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "bm_get_row_split": (C.c_int, [vp, C.POINTER(C.c_int32)]),
@@ -712,6 +714,15 @@ class Engine:
     def row_split(self) -> int:
         v = C.c_int32()
         self._chk(self.L.bm_get_row_split(self.h, C.byref(v)), "bm_get_row_split")
+        return v.value
+
+    def set_row_tiers(self, heavy_rows: int = 0) -> None:
+        """Rows of a launch run in twice-wider clusters: 0 automatic, -1 off, k > 0 at most k."""
+        self._chk(self.L.bm_set_row_tiers(self.h, heavy_rows), "bm_set_row_tiers")
+
+    def row_tiers(self) -> int:
+        v = C.c_int32()
+        self._chk(self.L.bm_get_row_tiers(self.h, C.byref(v)), "bm_get_row_tiers")
         return v.value
 
     SEMANTICS = {"exact": 0, "ref-cpu": 1}

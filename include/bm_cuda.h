@@ -634,6 +634,17 @@ bm_status bm_get_row_tiling(bm_ctx* ctx, int32_t* ctas_per_row, int32_t* threads
  * evaluates one pair per thread. */
 bm_status bm_set_row_split(bm_ctx* ctx, int32_t slots);
 bm_status bm_get_row_split(bm_ctx* ctx, int32_t* slots);
+/* Tiered row launches: a launch of few rows in c-CTA clusters that leaves
+ * resident CTA slots free runs its heaviest rows (by the same work estimate,
+ * ranked on the device, so the _dev entry points use it too) in 2c-CTA
+ * clusters, in a second launch on the context's second stream concurrent with
+ * the first; the calling stream waits for both.  Results are identical
+ * either way.  heavy_rows: 0 = automatic (default: as many rows as keep both
+ * launches within 85 % of the resident CTA slots), -1 = off, k > 0 = at most
+ * k rows.  Not used when the CTAs per row are set (bm_set_row_tiling) or a
+ * split plan is active.  No reference counterpart. */
+bm_status bm_set_row_tiers(bm_ctx* ctx, int32_t heavy_rows);
+bm_status bm_get_row_tiers(bm_ctx* ctx, int32_t* heavy_rows);
 /* How many row clusters of the given shape can be resident at once on the
  * device for the current n (cudaOccupancyMaxActiveClusters). */
 bm_status bm_rows_max_active_clusters(bm_ctx* ctx, int32_t ctas_per_row, int32_t threads, int32_t* out);

@@ -59,3 +59,5 @@ def test_null_context_is_rejected():
     assert L.bm_set_semantics(None, 1) == bm.BM_INVALID_ARG
     assert L.bm_get_semantics(None, C.byref(m)) == bm.BM_INVALID_ARG and m.value == -1
     assert L.bm_set_row_split(None, 0) == bm.BM_INVALID_ARG
+    assert L.bm_set_row_tiers(None, 0) == bm.BM_INVALID_ARG
+    assert L.bm_get_row_tiers(None, C.byref(m)) == bm.BM_INVALID_ARG
