@@ -65,12 +65,11 @@ constexpr int kImgOffW2T = kImgW1 + kImgW2 + kImgW3 + kImgEp;
 // 32; K = 128, 129 of a 144-wide hidden input), and the weights' matching
 // columns hold the bias as a pair of BF16 values, hi = bf16(b) and
 // lo = bf16(b - hi), so the FP32 accumulator receives b to about 2^-16.
-constexpr int kHK = 144;                   // hidden input width of the scorer's layers 2 and 3
+constexpr int kHK = 144;                   // hidden input width of the scorer's layer 2
 constexpr int kImgW1S = 128 * 32 * 2;      // N=128 hidden x K=32
 constexpr int kImgW2S = 128 * kHK * 2;     // N=128 out x K=144
-constexpr int kImgW3S = 16 * kHK * 2;      // N=16 x K=144: w3 and b3 in row 0
 constexpr int kImgOffS = kImgOffW2T + kImgW2T;
-constexpr int kImgBytes = kImgOffS + kImgW1S + kImgW2S + kImgW3S;
+constexpr int kImgBytes = kImgOffS + kImgW1S + kImgW2S;
 
 }  // namespace
 
@@ -563,13 +562,13 @@ __global__ void gather_batch_kernel(const uint16_t* __restrict__ rx, const float
 //      (K padded to 32) in the feature buffer X;
 //   2. one thread issues layer 1 (two K=16 MMAs, M=N=128) into TMEM columns
 //      0..127; the threads read their accumulator row back (tcgen05.ld
-//      32x32b), add the bias and convert with ReLU to BF16 (cvt.rn.relu.bf16x2)
-//      into the activation buffer H;
-//   3. eight K=16 MMAs accumulate layer 2 into TMEM columns 128..255; the same
-//      epilogue writes h2 over h1 in H;
-//   4. the output layer h2 . w3 runs as eight K=16 MMAs with N=16 (w3 in row 0
-//      of the B operand, zeros elsewhere) into columns 128..143, and each
-//      thread reads its column 128 and adds b3.
+//      32x32b; the bias is already in it) and convert with ReLU to BF16
+//      (cvt.rn.relu.bf16x2) into the activation buffer H;
+//   3. nine K=16 MMAs accumulate layer 2 into TMEM columns 128..255;
+//   4. each thread reads its layer-2 row back, rounds h2 = bf16(relu(.)) and
+//      forms the output b3 + h2 . w3 in FP32 on the CUDA cores (an N=16
+//      output MMA would re-read the 36 KB of H from shared memory, whose
+//      bandwidth the N=128 MMAs already use up, for one useful column).
 // Tiles overlap: while layer 2 of tile t runs on the tensor cores, the threads
 // build the features of tile t+1 into X and issue its layer 1 into columns
 // 0..127, which step 2 of tile t has already read back.  Every buffer is
@@ -578,18 +577,18 @@ __global__ void gather_batch_kernel(const uint16_t* __restrict__ rx, const float
 constexpr int kTcThreads = 128;
 constexpr uint32_t kSmW1 = 0;                       // the scorer image: W1 (bias columns 24, 25)
 constexpr uint32_t kSmW2 = kSmW1 + kImgW1S;         // 8192: W2, K = 144 (bias columns 128, 129)
-constexpr uint32_t kSmW3 = kSmW2 + kImgW2S;         // 45056: w3 and b3, K = 144
+constexpr uint32_t kSmW3 = kSmW2 + kImgW2S;         // 45056: w3 (BF16-rounded) and b3, FP32
 constexpr uint32_t kSmH = 49 * 1024;                // 50176: h1 / h2 operand, K = 144 (36 KB)
 constexpr uint32_t kSmX = kSmH + 128 * kHK * 2;     // 87040: features operand, K = 32 (8 KB)
 constexpr uint32_t kSmBits = kSmX + 128 * 32 * 2;   // 95232
 constexpr uint32_t kTcMinSmem = 100 * 1024;         // at most 2 CTAs (2 x 256 TMEM columns) per SM
-static_assert(kSmW3 + kImgW3S <= kSmH && kSmBits % 16 == 0 && kSmH % 1024 == 0 && kSmX % 1024 == 0,
+static_assert(kSmW3 + 4 * (BM_MLP_H + 1) <= kSmH && kSmBits % 16 == 0 && kSmH % 1024 == 0 && kSmX % 1024 == 0,
               "operand layout");
 constexpr uint32_t kBf16One2 = 0x3F803F80u;         // two BF16 ones, packed
 
 __host__ __device__ constexpr uint32_t bits_words(int32_t n) { return (uint32_t)(n + 32) / 32u; }
 __host__ __device__ constexpr uint32_t tc_tail(int32_t n) { return kSmBits + ((2u * bits_words(n) * 4u + 15u) & ~15u); }
-// two candidate bitmaps, then three mbarriers and the TMEM base slot
+// two candidate bitmaps, then the mbarriers and the TMEM base slot
 __host__ __device__ constexpr uint32_t tc_smem_bytes(int32_t n) { return tc_tail(n) + 32u; }
 
 // Byte offset of element (row r, k) in a K-major no-swizzle operand with
@@ -615,7 +614,6 @@ __host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
 }
 constexpr uint32_t kIdesc128 = idesc_bf16(128, 128);
-constexpr uint32_t kIdesc16 = idesc_bf16(128, 16);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -667,13 +665,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// One FP32 column of this thread's TMEM lane.
-__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
-    uint32_t r;
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    return __uint_as_float(r);
+// 32 consecutive 32-bit columns of this thread's TMEM lane, without waiting:
+// the registers are valid after tmem_wait_ld().
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
 }
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
@@ -709,10 +714,9 @@ __global__ void prep_image_kernel(const float* __restrict__ w, unsigned char* __
     unsigned short* w2t = reinterpret_cast<unsigned short*>(img + kImgOffW2T);
     unsigned short* s1 = reinterpret_cast<unsigned short*>(img + kImgOffS);
     unsigned short* s2 = reinterpret_cast<unsigned short*>(img + kImgOffS + kImgW1S);
-    unsigned short* s3 = reinterpret_cast<unsigned short*>(img + kImgOffS + kImgW1S + kImgW2S);
     const int n1 = 128 * 32, n2 = 128 * 128, n3 = 16 * 128;
     const int nt = n1 + n2 + n3 + 3 * 128 + 4 + n2;  // the training image
-    const int total = nt + n1 + 128 * kHK + 16 * kHK;
+    const int total = nt + n1 + 128 * kHK;
     // a bias as the BF16 pair (hi, lo) of a folded column
     auto hi = [](float b) { return bf16r(b); };
     auto lo = [](float b) { return bf16r(b - bf16r(b)); };
@@ -745,16 +749,11 @@ __global__ void prep_image_kernel(const float* __restrict__ w, unsigned char* __
             const float b = w[kOffB1 + j];
             const float v = i < BM_MLP_IN ? bf16r(w[i * BM_MLP_H + j]) : i == 24 ? hi(b) : i == 25 ? lo(b) : 0.f;
             put(s1 + kmajor_off(j, i, 32) / 2, v);
-        } else if (t < nt + n1 + 128 * kHK) {
+        } else {
             const int q = t - nt - n1, j = q / kHK, i = q % kHK;  // out j (N), in i (K)
             const float b = w[kOffB2 + j];
             const float v = i < 128 ? bf16r(w[kOffW2 + i * BM_MLP_H + j]) : i == 128 ? hi(b) : i == 129 ? lo(b) : 0.f;
             put(s2 + kmajor_off(j, i, kHK) / 2, v);
-        } else {
-            const int q = t - nt - n1 - 128 * kHK, j = q / kHK, i = q % kHK;  // row j (N = 16), in i (K)
-            const float b = w[kOffB3];
-            const float v = j != 0 ? 0.f : i < 128 ? bf16r(w[kOffW3 + i]) : i == 128 ? hi(b) : i == 129 ? lo(b) : 0.f;
-            put(s3 + kmajor_off(j, i, kHK) / 2, v);
         }
     }
 }
@@ -776,34 +775,47 @@ struct TcArgs {
 };
 
 // Hidden-layer epilogue: this thread's accumulator row (128 FP32 columns at
-// taddr; the bias is already in it), ReLU, BF16, stored as its row of the
-// next A operand.
+// taddr; the bias is already in it), read back with four loads and one wait,
+// ReLU, BF16, stored as its row of the next A operand.
 __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, unsigned char* sm, int tid) {
-#pragma unroll 1
-    for (int c = 0; c < 4; c++) {
-        float d[32];
-        tmem_ld32(taddr + 32u * c, d);
+    uint32_t d[128];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            uint4 o;
-            o.x = cvt_relu_bf16x2(d[8 * q + 0], d[8 * q + 1]);
-            o.y = cvt_relu_bf16x2(d[8 * q + 2], d[8 * q + 3]);
-            o.z = cvt_relu_bf16x2(d[8 * q + 4], d[8 * q + 5]);
-            o.w = cvt_relu_bf16x2(d[8 * q + 6], d[8 * q + 7]);
-            *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 32 * c + 8 * q, kHK)) = o;
-        }
+    for (int c = 0; c < 4; c++) tmem_ld32_async(taddr + 32u * c, d + 32 * c);
+    tmem_wait_ld();
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        uint4 o;
+        o.x = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 0]), __uint_as_float(d[8 * q + 1]));
+        o.y = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 2]), __uint_as_float(d[8 * q + 3]));
+        o.z = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 4]), __uint_as_float(d[8 * q + 5]));
+        o.w = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 6]), __uint_as_float(d[8 * q + 7]));
+        *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 8 * q, kHK)) = o;
     }
+}
+
+// Candidate v's vertex record (12 floats), loaded ahead of its features.
+struct CandRec {
+    float4 q[3];
+};
+__device__ __forceinline__ CandRec load_cand(const TcArgs& a, int32_t v) {
+    CandRec c;
+    if (v <= a.n) {
+        const float4* t4 = reinterpret_cast<const float4*>(a.tab + (size_t)v * BM_FT);
+        c.q[0] = t4[0]; c.q[1] = t4[1]; c.q[2] = t4[2];
+    } else {
+        c.q[0] = c.q[1] = c.q[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    return c;
 }
 
 // Features of this thread's candidate v of row u into its row of the X operand.
 __device__ __forceinline__ void build_features(const TcArgs& a, const float* ta, const uint32_t* bits_out,
-                                               const uint32_t* bits_in, int32_t u, int32_t v, unsigned char* sm,
-                                               int tid) {
+                                               const uint32_t* bits_in, int32_t u, int32_t v, const CandRec& cr,
+                                               unsigned char* sm, int tid) {
     float x[BM_MLP_IN];
     if (v <= a.n && v != u) {
         float tb[BM_FT];
-        const float4* t4 = reinterpret_cast<const float4*>(a.tab + (size_t)v * BM_FT);
-        const float4 q0 = t4[0], q1 = t4[1], q2 = t4[2];
+        const float4 q0 = cr.q[0], q1 = cr.q[1], q2 = cr.q[2];
         tb[0] = q0.x; tb[1] = q0.y; tb[2] = q0.z; tb[3] = q0.w;
         tb[4] = q1.x; tb[5] = q1.y; tb[6] = q1.z; tb[7] = q1.w;
         tb[8] = q2.x; tb[9] = q2.y; tb[10] = q2.z; tb[11] = q2.w;
@@ -846,19 +858,23 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     const uint32_t tail = tc_tail(a.n);
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + tail);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + tail + 24);
-    const uint32_t bar1 = smem_u32(&bars[0]), bar2 = smem_u32(&bars[1]), bar3 = smem_u32(&bars[2]);
+    const uint32_t bar1 = smem_u32(&bars[0]), bar2 = smem_u32(&bars[1]);
 
-    {  // the scorer image into shared memory; this thread's constant H
-       // columns (128, 129: the bias inputs of layers 2 and 3)
+    {  // the scorer image (W1, W2) into shared memory, w3 and b3 (FP32)
+       // from the training image's epilogue vectors; this thread's constant
+       // H columns (128, 129: the bias inputs of layer 2)
         const uint4* src = reinterpret_cast<const uint4*>(a.img + kImgOffS);
-        for (int i = tid; i < (kImgW1S + kImgW2S + kImgW3S) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
+        for (int i = tid; i < (kImgW1S + kImgW2S) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
+        const float* ep = reinterpret_cast<const float*>(a.img + kImgW1 + kImgW2 + kImgW3);
+        float* w3s = reinterpret_cast<float*>(sm + kSmW3);
+        w3s[tid] = ep[256 + tid];
+        if (tid == 0) w3s[128] = ep[384];
         *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 128, kHK)) = make_uint4(kBf16One2, 0u, 0u, 0u);
         *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 136, kHK)) = make_uint4(0u, 0u, 0u, 0u);
     }
     if (tid == 0) {
         mbar_init(bar1, 1);
         mbar_init(bar2, 1);
-        mbar_init(bar3, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -871,8 +887,9 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
     const uint32_t tm_1 = tmem + lane_base;         // layer 1 (columns 0..127)
-    const uint32_t tm_2 = tmem + 128u + lane_base;  // layer 2, then the output layer (columns 128..)
-    const uint32_t sW1 = smem_u32(sm + kSmW1), sW2 = smem_u32(sm + kSmW2), sW3 = smem_u32(sm + kSmW3);
+    const uint32_t tm_2 = tmem + 128u + lane_base;  // layer 2 (columns 128..255)
+    const uint32_t sW1 = smem_u32(sm + kSmW1), sW2 = smem_u32(sm + kSmW2);
+    const float4* w3v = reinterpret_cast<const float4*>(sm + kSmW3);
     const uint32_t sH = smem_u32(sm + kSmH), sX = smem_u32(sm + kSmX);
     uint32_t phase = 0;  // parity of the current tile's completions (each barrier completes once per tile)
     // the last commit and the parity it completes: it covers every earlier MMA
@@ -912,11 +929,14 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
         __syncthreads();
         float* out_row = a.scores + (size_t)r * a.n;
         // prologue: features and layer 1 of the row's first tile
-        build_features(a, ta, bits_out, bits_in, u, 1 + tid, sm, tid);
+        build_features(a, ta, bits_out, bits_in, u, 1 + tid, load_cand(a, 1 + tid), sm, tid);
         tc_handoff();
         issue_layer1(phase);
         for (int32_t v0 = 1; v0 <= a.n; v0 += 128) {
             const int32_t v = v0 + tid;
+            const bool more = v0 + 128 <= a.n;
+            // the next tile's candidate record, in flight during this epilogue
+            const CandRec next = load_cand(a, more ? v + 128 : a.n + 1);
             // layer 1 done: its epilogue fills H with h1
             if (!__syncthreads_and(mbar_wait(bar1, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
@@ -933,34 +953,37 @@ __global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
             last_par = phase;
             // next tile's features and layer 1 while layer 2 runs (X and columns
             // 0..127 are free: layer 1 of this tile completed and was read back)
-            const bool more = v0 + 128 <= a.n;
             if (more) {
-                build_features(a, ta, bits_out, bits_in, u, v + 128, sm, tid);
+                build_features(a, ta, bits_out, bits_in, u, v + 128, next, sm, tid);
                 tc_handoff();
                 issue_layer1(phase ^ 1u);
             }
-            // layer 2 done: its epilogue writes h2 over h1
+            // layer 2 done: the output o = b3 + h2 . w3 on the CUDA cores, in
+            // FP32 from this thread's accumulator row (h2 = bf16(relu(D2)))
             if (!__syncthreads_and(mbar_wait(bar2, phase, a.wait_limit))) { ok = false; break; }
             tc_fence_after();
-            hidden_epilogue(tm_2, sm, tid);
-            tc_handoff();
-            if (tid == 0) {  // output layer, N = 16 (row 0 of B holds w3 and b3), into columns 128..143
+            float o = reinterpret_cast<const float*>(w3v)[128];
+            {
+                uint32_t d[128];
 #pragma unroll
-                for (int s = 0; s < kHK / 16; s++)
-                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, kHK / 8 * 128u),
-                             smem_desc(sW3 + 256u * s, 128u, kHK / 8 * 128u), kIdesc16, s > 0);
-                mma_commit(bar3);
+                for (int c = 0; c < 4; c++) tmem_ld32_async(tm_2 + 32u * c, d + 32 * c);
+                tmem_wait_ld();
+#pragma unroll
+                for (int q = 0; q < 32; q++) {
+                    const float4 w4 = w3v[q];
+                    const uint32_t h01 = cvt_relu_bf16x2(__uint_as_float(d[4 * q + 0]), __uint_as_float(d[4 * q + 1]));
+                    const uint32_t h23 = cvt_relu_bf16x2(__uint_as_float(d[4 * q + 2]), __uint_as_float(d[4 * q + 3]));
+                    o = fmaf(__uint_as_float(h01 << 16), w4.x, o);
+                    o = fmaf(__uint_as_float(h01 & 0xFFFF0000u), w4.y, o);
+                    o = fmaf(__uint_as_float(h23 << 16), w4.z, o);
+                    o = fmaf(__uint_as_float(h23 & 0xFFFF0000u), w4.w, o);
+                }
             }
-            last_bar = bar3;
-            last_par = phase;
-            if (!__syncthreads_and(mbar_wait(bar3, phase, a.wait_limit))) { ok = false; break; }
-            tc_fence_after();
-            const float o = tmem_ld1(tm_2);
             if (v <= a.n) out_row[v - 1] = (v != u) ? o : -INFINITY;
+            // the next tile's layer-1 epilogue overwrites H only after its own
+            // wait, and its layer 2 (over these TMEM columns) is issued only
+            // after the barrier that follows that epilogue
             phase ^= 1u;
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
         }
     }
     if (!ok && tid == 0) atomicExch(a.flag, 1);
