@@ -556,40 +556,61 @@ __global__ void gather_batch_kernel(const uint16_t* __restrict__ rx, const float
 
 // --------------------------------------------- tensor-core row scoring kernel
 //
-// One CTA (128 threads) scores whole rows: for row u, candidates v = 1..n in
-// tiles of 128, one candidate per thread.  Per tile t:
-//   1. every thread builds its candidate's 24 features as the BF16 A operand
-//      (K padded to 32) in the feature buffer X;
-//   2. one thread issues layer 1 (two K=16 MMAs, M=N=128) into TMEM columns
-//      0..127; the threads read their accumulator row back (tcgen05.ld
-//      32x32b; the bias is already in it) and convert with ReLU to BF16
-//      (cvt.rn.relu.bf16x2) into the activation buffer H;
-//   3. nine K=16 MMAs accumulate layer 2 into TMEM columns 128..255;
-//   4. each thread reads its layer-2 row back, rounds h2 = bf16(relu(.)) and
-//      forms the output b3 + h2 . w3 in FP32 on the CUDA cores (an N=16
-//      output MMA would re-read the 36 KB of H from shared memory, whose
-//      bandwidth the N=128 MMAs already use up, for one useful column).
-// Tiles overlap: while layer 2 of tile t runs on the tensor cores, the threads
-// build the features of tile t+1 into X and issue its layer 1 into columns
-// 0..127, which step 2 of tile t has already read back.  Every buffer is
-// rewritten only after the MMA that reads it has signalled completion.
+// One CTA per SM (768 threads, all 512 TMEM columns) scores whole rows: for
+// row u, candidates v = 1..n in tiles of 128, one candidate per TMEM lane.
+// The tiles of the CTA's rows flow through a pipeline of three roles; each
+// role has two groups of four warps, group g taking the tiles t = g mod 2, so
+// that two tiles are in flight in every role.  Tile t holds TMEM slot
+// D[t & 3] (128 columns: layer 1's accumulators, then layer 2's over them,
+// then the output layer's operand and accumulator) and shared-memory slots
+// X[t & 1], H[t & 1].  A group ends each step with a named barrier over its
+// warps, after which its first thread issues the MMAs that consume what the
+// group wrote:
+//   F  (warps 0-7)    build tile t's BF16 features (K padded to 32, the bias
+//                     inputs in columns 24, 25) into X, then layer 1 (two K=16
+//                     MMAs, M=N=128) into D;
+//   E1 (warps 8-15)   read layer 1 back (tcgen05.ld 32x32b; the bias is
+//                     already in it), write bf16(relu(.)) (cvt.rn.relu.bf16x2)
+//                     into H, then layer 2 (nine K=16 MMAs over H, K=144 with
+//                     the bias inputs in columns 128, 129) into the same D;
+//   E2 (warps 16-23)  read layer 2 back, write bf16(relu(.)) as the output
+//                     layer's A operand into columns 0..63 of D (two BF16 per
+//                     column; each quarter is written after it was read), run
+//                     the output layer (eight K=16 MMAs, N=16, A in tensor
+//                     memory, w3 in row 0 of B) into columns 64..79, read the
+//                     output column back and add b3.  Neither h2 nor the
+//                     output layer touches shared memory, whose bandwidth the
+//                     N=128 MMAs already use up.
+// mbarriers, one per TMEM slot and kind: d1full, d2full, d3full (the commits
+// after each layer; d1full(t) also frees X for tile t+2, d2full(t) H for tile
+// t+2) and dfree (an E2 group's 128 threads: the slot is free for tile t+4).
+// Use k of a slot waits for phase k & 1; no barrier can run two phases ahead
+// of a waiter, since each completion needs the waiter's own earlier step.
+// Every wait is bounded (the context's wait limit); a wait that runs out
+// raises the CTA's abort flag, which every other wait checks, and each group
+// leaves its loop together (its waits are combined over its barrier); the
+// issuing threads then wait (default bound) for their last commits before
+// the columns are freed.
 
-constexpr int kTcThreads = 128;
-constexpr uint32_t kSmW1 = 0;                       // the scorer image: W1 (bias columns 24, 25)
-constexpr uint32_t kSmW2 = kSmW1 + kImgW1S;         // 8192: W2, K = 144 (bias columns 128, 129)
-constexpr uint32_t kSmW3 = kSmW2 + kImgW2S;         // 45056: w3 (BF16-rounded) and b3, FP32
-constexpr uint32_t kSmH = 49 * 1024;                // 50176: h1 / h2 operand, K = 144 (36 KB)
-constexpr uint32_t kSmX = kSmH + 128 * kHK * 2;     // 87040: features operand, K = 32 (8 KB)
-constexpr uint32_t kSmBits = kSmX + 128 * 32 * 2;   // 95232
-constexpr uint32_t kTcMinSmem = 100 * 1024;         // at most 2 CTAs (2 x 256 TMEM columns) per SM
-static_assert(kSmW3 + 4 * (BM_MLP_H + 1) <= kSmH && kSmBits % 16 == 0 && kSmH % 1024 == 0 && kSmX % 1024 == 0,
+constexpr int kTcThreads = 768;                        // F 0-7, E1 8-15, E2 16-23 (two groups each)
+constexpr uint32_t kSmW1 = 0;                          // W1 (bias columns 24, 25), 8 KB
+constexpr uint32_t kSmW2 = kSmW1 + kImgW1S;            // 8192: W2, K = 144 (bias columns 128, 129), 36 KB
+constexpr uint32_t kSmW3 = kSmW2 + kImgW2S;            // 45056: the output layer's B (N=16, K=128), then b3 (FP32)
+constexpr uint32_t kSmH = 50 * 1024;                   // H[2]: h1 operands, K = 144, 36 KB each
+constexpr uint32_t kSmHBytes = 128 * kHK * 2;
+constexpr uint32_t kSmX = kSmH + 2 * kSmHBytes;        // 122880: X[2]: feature operands, K = 32, 8 KB each
+constexpr uint32_t kSmXBytes = 128 * 32 * 2;
+constexpr uint32_t kSmBits = kSmX + 2 * kSmXBytes;     // 141312: each F group's two candidate bitmaps
+static_assert(kSmW3 + kImgW3 + 16 <= kSmH && kSmH % 1024 == 0 && kSmX % 1024 == 0 && kSmBits % 16 == 0,
               "operand layout");
 constexpr uint32_t kBf16One2 = 0x3F803F80u;         // two BF16 ones, packed
 
 __host__ __device__ constexpr uint32_t bits_words(int32_t n) { return (uint32_t)(n + 32) / 32u; }
-__host__ __device__ constexpr uint32_t tc_tail(int32_t n) { return kSmBits + ((2u * bits_words(n) * 4u + 15u) & ~15u); }
-// two candidate bitmaps, then the mbarriers and the TMEM base slot
-__host__ __device__ constexpr uint32_t tc_smem_bytes(int32_t n) { return tc_tail(n) + 32u; }
+__host__ __device__ constexpr uint32_t tc_bits_bytes(int32_t n) { return (2u * bits_words(n) * 4u + 15u) & ~15u; }
+__host__ __device__ constexpr uint32_t tc_tail(int32_t n) { return kSmBits + 2u * tc_bits_bytes(n); }
+// two F groups' candidate bitmaps, then 16 mbarriers, the TMEM base slot and
+// the abort flag (at least 138 KB in all: one CTA per SM)
+__host__ __device__ constexpr uint32_t tc_smem_bytes(int32_t n) { return tc_tail(n) + 144u; }
 
 // Byte offset of element (row r, k) in a K-major no-swizzle operand with
 // kcols columns: 8-row x 8-element core matrices of 128 contiguous bytes,
@@ -614,6 +635,7 @@ __host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
 }
 constexpr uint32_t kIdesc128 = idesc_bf16(128, 128);
+constexpr uint32_t kIdesc16 = idesc_bf16(128, 16);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -625,6 +647,19 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
         :
         : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// The same with the A operand in tensor memory (M rows in lanes 0..127, K
+// along the columns, two 16-bit elements per column, lower K in the low half).
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 
@@ -679,6 +714,27 @@ __device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t* r) {
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 16 consecutive 32-bit columns of this thread's TMEM lane from registers;
+// complete after tmem_wait_st().
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        :
+        : "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+          "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// One 32-bit column of this thread's TMEM lane.
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    return r;
+}
 
 __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
@@ -774,26 +830,7 @@ struct TcArgs {
     long long wait_limit;  // bound of each MMA-completion wait, SM cycles
 };
 
-// Hidden-layer epilogue: this thread's accumulator row (128 FP32 columns at
-// taddr; the bias is already in it), read back with four loads and one wait,
-// ReLU, BF16, stored as its row of the next A operand.
-__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, unsigned char* sm, int tid) {
-    uint32_t d[128];
-#pragma unroll
-    for (int c = 0; c < 4; c++) tmem_ld32_async(taddr + 32u * c, d + 32 * c);
-    tmem_wait_ld();
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-        uint4 o;
-        o.x = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 0]), __uint_as_float(d[8 * q + 1]));
-        o.y = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 2]), __uint_as_float(d[8 * q + 3]));
-        o.z = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 4]), __uint_as_float(d[8 * q + 5]));
-        o.w = cvt_relu_bf16x2(__uint_as_float(d[8 * q + 6]), __uint_as_float(d[8 * q + 7]));
-        *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 8 * q, kHK)) = o;
-    }
-}
-
-// Candidate v's vertex record (12 floats), loaded ahead of its features.
+// Candidate v's vertex record (12 floats).
 struct CandRec {
     float4 q[3];
 };
@@ -808,10 +845,10 @@ __device__ __forceinline__ CandRec load_cand(const TcArgs& a, int32_t v) {
     return c;
 }
 
-// Features of this thread's candidate v of row u into its row of the X operand.
+// Features of candidate v of row u into row `row` of the X operand at xs.
 __device__ __forceinline__ void build_features(const TcArgs& a, const float* ta, const uint32_t* bits_out,
                                                const uint32_t* bits_in, int32_t u, int32_t v, const CandRec& cr,
-                                               unsigned char* sm, int tid) {
+                                               unsigned char* xs, int row) {
     float x[BM_MLP_IN];
     if (v <= a.n && v != u) {
         float tb[BM_FT];
@@ -835,7 +872,265 @@ __device__ __forceinline__ void build_features(const TcArgs& a, const float* ta,
             q.z = cvt_bf16x2(x[8 * c + 4], x[8 * c + 5]);
             q.w = cvt_bf16x2(x[8 * c + 6], x[8 * c + 7]);
         }
-        *reinterpret_cast<uint4*>(sm + kSmX + kmajor_off(tid, 8 * c, 32)) = q;
+        *reinterpret_cast<uint4*>(xs + kmajor_off(row, 8 * c, 32)) = q;
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+// Bounded wait of one role: gives up when the wait limit passes or another
+// role raised the abort flag (both checked before every try).
+__device__ __forceinline__ bool role_wait(uint32_t mbar, uint32_t parity, long long limit, volatile int* abort) {
+    const long long t0 = clock64();
+    for (;;) {
+        if (*abort || clock64() - t0 >= limit) return false;
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+}
+
+// Named barrier `id` over one role's four warps (128 threads), AND of v.
+__device__ __forceinline__ bool role_bar_and(uint32_t id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %2, 0;\n\t"
+        "bar.red.and.pred p, %1, 128, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r)
+        : "r"(id), "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void role_bar(uint32_t id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+__global__ void __launch_bounds__(kTcThreads, 1) mlp_rows_tc_kernel(TcArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int role = warp >> 3;                 // 0 F, 1 E1, 2 E2
+    const int grp = (warp >> 2) & 1;            // the tiles t = grp mod 2
+    const int gtid = tid & 127;                 // thread in the group = TMEM lane / tile row
+    const bool leader = gtid == 0;
+    const uint32_t gbar = 1u + 2u * (uint32_t)role + (uint32_t)grp;  // the group's named barrier
+    const uint32_t nw = bits_words(a.n);
+    const uint32_t tail = tc_tail(a.n);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + tail);  // four of each kind below, one per TMEM slot
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + tail + 128);
+    volatile int* abort = reinterpret_cast<volatile int*>(sm + tail + 132);
+    auto bar = [&](int k, int q) { return smem_u32(&bars[4 * k + q]); };
+    constexpr int D1FULL = 0, D2FULL = 1, D3FULL = 2, DFREE = 3;
+    auto par = [](int32_t t) { return (uint32_t)(t >> 2) & 1u; };  // phase of tile t on its slot's barrier
+
+    {  // the scorer image (W1, W2); the training image's output-layer B (w3 in
+       // row 0) and b3 (FP32, from its epilogue vectors); the constant columns
+       // of both H (128, 129: the bias inputs of layer 2; 130..143 zero)
+        const uint4* src = reinterpret_cast<const uint4*>(a.img + kImgOffS);
+        for (int i = tid; i < (kImgW1S + kImgW2S) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
+        const uint4* w3src = reinterpret_cast<const uint4*>(a.img + kImgW1 + kImgW2);
+        if (tid < kImgW3 / 16) reinterpret_cast<uint4*>(sm + kSmW3)[tid] = w3src[tid];
+        const float* ep = reinterpret_cast<const float*>(a.img + kImgW1 + kImgW2 + kImgW3);
+        if (tid == 0) *reinterpret_cast<float*>(sm + kSmW3 + kImgW3) = ep[384];
+        if (tid < 256) {
+            unsigned char* h = sm + kSmH + (tid >> 7) * kSmHBytes;
+            const int row = tid & 127;
+            *reinterpret_cast<uint4*>(h + kmajor_off(row, 128, kHK)) = make_uint4(kBf16One2, 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(h + kmajor_off(row, 136, kHK)) = make_uint4(0u, 0u, 0u, 0u);
+        }
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 4; k++)
+            for (int q = 0; q < 4; q++) mbar_init(bar(k, q), k == DFREE ? 128u : 1u);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    // the CTA's tiles: rows blockIdx.x, blockIdx.x + gridDim.x, ...; tiles of 128 candidates
+    const int32_t tpr = (a.n + 127) / 128;
+    const int32_t my_rows = a.nrows > (int32_t)blockIdx.x ? (a.nrows - 1 - (int32_t)blockIdx.x) / (int32_t)gridDim.x + 1 : 0;
+    const int32_t T = my_rows * tpr;
+    auto tile_row = [&](int32_t t, int32_t& r, int32_t& v0) {
+        const int32_t ri = t / tpr;
+        r = (int32_t)blockIdx.x + ri * (int32_t)gridDim.x;
+        v0 = 1 + (t - ri * tpr) * 128;
+    };
+    const long long lim = a.wait_limit;
+    bool ok = true;
+    uint32_t last_bar = 0, last_par = 0;  // this thread's last commit (the issuing threads)
+    const uint32_t lb = (uint32_t)((warp & 3) * 32) << 16;  // the warp's TMEM lanes
+
+    if (role == 0) {
+        // ---- F: features, then layer 1
+        uint32_t* bits_out = reinterpret_cast<uint32_t*>(sm + kSmBits + grp * tc_bits_bytes(a.n));
+        uint32_t* bits_in = bits_out + nw;
+        const uint32_t sW1 = smem_u32(sm + kSmW1);
+        const uint32_t sX = smem_u32(sm + kSmX + grp * kSmXBytes);
+        float ta[BM_FT];
+        int32_t u = 0, cur_r = -1;
+        for (int32_t t = grp; t < T; t += 2) {
+            const int q = t & 3;
+            int32_t r, v0;
+            tile_row(t, r, v0);
+            bool w = true;
+            if (t >= 2) w = role_wait(bar(D1FULL, (t - 2) & 3), par(t - 2), lim, abort);  // X free
+            if (w && t >= 4) w = role_wait(bar(DFREE, q), par(t - 4), lim, abort);        // slot free
+            if (!role_bar_and(gbar, w)) { ok = false; break; }
+            if (r != cur_r) {
+                // a new row: its bitmaps of the v with B(pi u, pi v) > 0
+                // (B'-out of u) and B(pi v, pi u) > 0 (B'-in of u), and its record
+                cur_r = r;
+                u = a.rows[r];
+                for (uint32_t i = gtid; i < 2 * nw; i += 128) bits_out[i] = 0u;
+                role_bar(gbar);
+                const int32_t fu = a.pi[u];
+                for (int32_t j = a.b_optr[fu] + gtid; j < a.b_optr[fu + 1]; j += 128) {
+                    const uint32_t e = a.b_oent[j];
+                    if (e) atomicOr(&bits_out[bm_eid(e) >> 5], 1u << (bm_eid(e) & 31));
+                }
+                for (int32_t j = a.b_iptr[fu] + gtid; j < a.b_iptr[fu + 1]; j += 128) {
+                    const uint32_t e = a.b_ient[j];
+                    if (e) atomicOr(&bits_in[bm_eid(e) >> 5], 1u << (bm_eid(e) & 31));
+                }
+#pragma unroll
+                for (int i = 0; i < BM_FT; i++) ta[i] = a.tab[(size_t)u * BM_FT + i];
+                role_bar(gbar);
+            }
+            build_features(a, ta, bits_out, bits_in, u, v0 + gtid, load_cand(a, v0 + gtid), sm + kSmX + grp * kSmXBytes, gtid);
+            proxy_fence();
+            role_bar(gbar);
+            if (leader) {
+                tc_fence_after();
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+                    mma_bf16(tmem + 128u * q, smem_desc(sX + 256u * k, 128u, 512u), smem_desc(sW1 + 256u * k, 128u, 512u),
+                             kIdesc128, k > 0);
+                mma_commit(bar(D1FULL, q));
+                last_bar = bar(D1FULL, q);
+                last_par = par(t);
+            }
+        }
+    } else if (role == 1) {
+        // ---- E1: layer-1 epilogue into H, then layer 2
+        unsigned char* h = sm + kSmH + grp * kSmHBytes;
+        const uint32_t sH = smem_u32(h), sW2 = smem_u32(sm + kSmW2);
+        for (int32_t t = grp; t < T; t += 2) {
+            const int q = t & 3;
+            bool w = role_wait(bar(D1FULL, q), par(t), lim, abort);
+            if (w && t >= 2) w = role_wait(bar(D2FULL, (t - 2) & 3), par(t - 2), lim, abort);  // H free
+            if (!role_bar_and(gbar, w)) { ok = false; break; }
+            tc_fence_after();
+#pragma unroll
+            for (int c4 = 0; c4 < 4; c4++) {
+                uint32_t d[32];
+                tmem_ld32_async(tmem + 128u * q + 32u * c4 + lb, d);
+                tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    uint4 o;
+                    o.x = cvt_relu_bf16x2(__uint_as_float(d[8 * c + 0]), __uint_as_float(d[8 * c + 1]));
+                    o.y = cvt_relu_bf16x2(__uint_as_float(d[8 * c + 2]), __uint_as_float(d[8 * c + 3]));
+                    o.z = cvt_relu_bf16x2(__uint_as_float(d[8 * c + 4]), __uint_as_float(d[8 * c + 5]));
+                    o.w = cvt_relu_bf16x2(__uint_as_float(d[8 * c + 6]), __uint_as_float(d[8 * c + 7]));
+                    *reinterpret_cast<uint4*>(h + kmajor_off(gtid, 32 * c4 + 8 * c, kHK)) = o;
+                }
+            }
+            proxy_fence();
+            tc_fence_before();
+            role_bar(gbar);
+            if (leader) {
+                tc_fence_after();
+#pragma unroll
+                for (int k = 0; k < kHK / 16; k++)
+                    mma_bf16(tmem + 128u * q, smem_desc(sH + 256u * k, 128u, kHK / 8 * 128u),
+                             smem_desc(sW2 + 256u * k, 128u, kHK / 8 * 128u), kIdesc128, k > 0);
+                mma_commit(bar(D2FULL, q));
+                last_bar = bar(D2FULL, q);
+                last_par = par(t);
+            }
+        }
+    } else {
+        // ---- E2: h2 = bf16(relu(D2)) into columns 0..63 of the tile's slot,
+        // the output layer, its column back + b3
+        const uint32_t sW3 = smem_u32(sm + kSmW3);
+        const float b3 = *reinterpret_cast<const float*>(sm + kSmW3 + kImgW3);
+        int32_t cur_r = -1, u = 0;
+        for (int32_t t = grp; t < T; t += 2) {
+            const int q = t & 3;
+            int32_t r, v0;
+            tile_row(t, r, v0);
+            if (r != cur_r) { cur_r = r; u = a.rows[r]; }
+            bool w = role_wait(bar(D2FULL, q), par(t), lim, abort);
+            if (!role_bar_and(gbar, w)) { ok = false; break; }
+            tc_fence_after();
+            const uint32_t d2 = tmem + 128u * q + lb;
+#pragma unroll
+            for (int c4 = 0; c4 < 4; c4++) {
+                // columns 32 c4 .. 32 c4 + 31 in, packed into 16 c4 .. 16 c4 + 15
+                // (columns already read)
+                uint32_t d[32], hh[16];
+                tmem_ld32_async(d2 + 32u * c4, d);
+                tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 16; c++) hh[c] = cvt_relu_bf16x2(__uint_as_float(d[2 * c]), __uint_as_float(d[2 * c + 1]));
+                tmem_st16(d2 + 16u * c4, hh);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            role_bar(gbar);
+            if (leader) {
+                tc_fence_after();
+                const uint32_t dq = tmem + 128u * q;
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    mma_bf16_ts(dq + 64u, dq + 8u * k, smem_desc(sW3 + 256u * k, 128u, 2048u), kIdesc16, k > 0);
+                mma_commit(bar(D3FULL, q));
+                last_bar = bar(D3FULL, q);
+                last_par = par(t);
+            }
+            w = role_wait(bar(D3FULL, q), par(t), lim, abort);
+            if (!role_bar_and(gbar, w)) { ok = false; break; }
+            tc_fence_after();
+            const float o = __uint_as_float(tmem_ld1(d2 + 64u)) + b3;
+            tc_fence_before();
+            mbar_arrive(bar(DFREE, q));  // the slot is free for tile t + 4
+            const int32_t v = v0 + gtid;
+            if (v <= a.n) a.scores[(size_t)r * a.n + (v - 1)] = (v != u) ? o : -INFINITY;
+        }
+    }
+    if (!ok) {
+        *abort = 1;
+        atomicExch(a.flag, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    // after an abort the issuing threads let their MMAs in flight finish
+    // before the columns are freed (the default bound, whatever bound the
+    // waits above were given); otherwise every commit has been waited on
+    if (*abort && last_bar) mbar_wait(last_bar, last_par);
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
     }
 }
 
@@ -846,156 +1141,6 @@ __device__ __forceinline__ void tc_handoff() {
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-}
-
-__global__ void __launch_bounds__(kTcThreads) mlp_rows_tc_kernel(TcArgs a) {
-    extern __shared__ __align__(1024) unsigned char sm[];
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5;
-    const uint32_t nw = bits_words(a.n);
-    uint32_t* bits_out = reinterpret_cast<uint32_t*>(sm + kSmBits);
-    uint32_t* bits_in = bits_out + nw;
-    const uint32_t tail = tc_tail(a.n);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + tail);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + tail + 24);
-    const uint32_t bar1 = smem_u32(&bars[0]), bar2 = smem_u32(&bars[1]);
-
-    {  // the scorer image (W1, W2) into shared memory, w3 and b3 (FP32)
-       // from the training image's epilogue vectors; this thread's constant
-       // H columns (128, 129: the bias inputs of layer 2)
-        const uint4* src = reinterpret_cast<const uint4*>(a.img + kImgOffS);
-        for (int i = tid; i < (kImgW1S + kImgW2S) / 16; i += kTcThreads) reinterpret_cast<uint4*>(sm)[i] = src[i];
-        const float* ep = reinterpret_cast<const float*>(a.img + kImgW1 + kImgW2 + kImgW3);
-        float* w3s = reinterpret_cast<float*>(sm + kSmW3);
-        w3s[tid] = ep[256 + tid];
-        if (tid == 0) w3s[128] = ep[384];
-        *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 128, kHK)) = make_uint4(kBf16One2, 0u, 0u, 0u);
-        *reinterpret_cast<uint4*>(sm + kSmH + kmajor_off(tid, 136, kHK)) = make_uint4(0u, 0u, 0u, 0u);
-    }
-    if (tid == 0) {
-        mbar_init(bar1, 1);
-        mbar_init(bar2, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(256u)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    tc_handoff();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    const uint32_t tm_1 = tmem + lane_base;         // layer 1 (columns 0..127)
-    const uint32_t tm_2 = tmem + 128u + lane_base;  // layer 2 (columns 128..255)
-    const uint32_t sW1 = smem_u32(sm + kSmW1), sW2 = smem_u32(sm + kSmW2);
-    const float4* w3v = reinterpret_cast<const float4*>(sm + kSmW3);
-    const uint32_t sH = smem_u32(sm + kSmH), sX = smem_u32(sm + kSmX);
-    uint32_t phase = 0;  // parity of the current tile's completions (each barrier completes once per tile)
-    // the last commit and the parity it completes: it covers every earlier MMA
-    // of the issuing thread, so the error path waits on it alone
-    uint32_t last_bar = 0, last_par = 0;
-    bool ok = true;
-
-    auto issue_layer1 = [&](uint32_t par) {
-        if (tid == 0) {
-#pragma unroll
-            for (int s = 0; s < 2; s++)
-                mma_bf16(tmem, smem_desc(sX + 256u * s, 128u, 512u), smem_desc(sW1 + 256u * s, 128u, 512u),
-                         kIdesc128, s > 0);
-            mma_commit(bar1);
-        }
-        last_bar = bar1;
-        last_par = par;
-    };
-
-    for (int32_t r = blockIdx.x; r < a.nrows && ok; r += gridDim.x) {
-        const int32_t u = a.rows[r];
-        // bitmaps of the v with B(pi u, pi v) > 0 (B'-out of u) and B(pi v, pi u) > 0 (B'-in of u)
-        for (uint32_t i = tid; i < 2 * nw; i += kTcThreads) bits_out[i] = 0u;
-        __syncthreads();
-        const int32_t fu = a.pi[u];
-        for (int32_t j = a.b_optr[fu] + tid; j < a.b_optr[fu + 1]; j += kTcThreads) {
-            const uint32_t e = a.b_oent[j];
-            if (e) atomicOr(&bits_out[bm_eid(e) >> 5], 1u << (bm_eid(e) & 31));
-        }
-        for (int32_t j = a.b_iptr[fu] + tid; j < a.b_iptr[fu + 1]; j += kTcThreads) {
-            const uint32_t e = a.b_ient[j];
-            if (e) atomicOr(&bits_in[bm_eid(e) >> 5], 1u << (bm_eid(e) & 31));
-        }
-        float ta[BM_FT];
-#pragma unroll
-        for (int i = 0; i < BM_FT; i++) ta[i] = a.tab[(size_t)u * BM_FT + i];
-        __syncthreads();
-        float* out_row = a.scores + (size_t)r * a.n;
-        // prologue: features and layer 1 of the row's first tile
-        build_features(a, ta, bits_out, bits_in, u, 1 + tid, load_cand(a, 1 + tid), sm, tid);
-        tc_handoff();
-        issue_layer1(phase);
-        for (int32_t v0 = 1; v0 <= a.n; v0 += 128) {
-            const int32_t v = v0 + tid;
-            const bool more = v0 + 128 <= a.n;
-            // the next tile's candidate record, in flight during this epilogue
-            const CandRec next = load_cand(a, more ? v + 128 : a.n + 1);
-            // layer 1 done: its epilogue fills H with h1
-            if (!__syncthreads_and(mbar_wait(bar1, phase, a.wait_limit))) { ok = false; break; }
-            tc_fence_after();
-            hidden_epilogue(tm_1, sm, tid);
-            tc_handoff();
-            if (tid == 0) {  // layer 2, K = 144 (b2 in columns 128, 129)
-#pragma unroll
-                for (int s = 0; s < kHK / 16; s++)
-                    mma_bf16(tmem + 128u, smem_desc(sH + 256u * s, 128u, kHK / 8 * 128u),
-                             smem_desc(sW2 + 256u * s, 128u, kHK / 8 * 128u), kIdesc128, s > 0);
-                mma_commit(bar2);
-            }
-            last_bar = bar2;
-            last_par = phase;
-            // next tile's features and layer 1 while layer 2 runs (X and columns
-            // 0..127 are free: layer 1 of this tile completed and was read back)
-            if (more) {
-                build_features(a, ta, bits_out, bits_in, u, v + 128, next, sm, tid);
-                tc_handoff();
-                issue_layer1(phase ^ 1u);
-            }
-            // layer 2 done: the output o = b3 + h2 . w3 on the CUDA cores, in
-            // FP32 from this thread's accumulator row (h2 = bf16(relu(D2)))
-            if (!__syncthreads_and(mbar_wait(bar2, phase, a.wait_limit))) { ok = false; break; }
-            tc_fence_after();
-            float o = reinterpret_cast<const float*>(w3v)[128];
-            {
-                uint32_t d[128];
-#pragma unroll
-                for (int c = 0; c < 4; c++) tmem_ld32_async(tm_2 + 32u * c, d + 32 * c);
-                tmem_wait_ld();
-#pragma unroll
-                for (int q = 0; q < 32; q++) {
-                    const float4 w4 = w3v[q];
-                    const uint32_t h01 = cvt_relu_bf16x2(__uint_as_float(d[4 * q + 0]), __uint_as_float(d[4 * q + 1]));
-                    const uint32_t h23 = cvt_relu_bf16x2(__uint_as_float(d[4 * q + 2]), __uint_as_float(d[4 * q + 3]));
-                    o = fmaf(__uint_as_float(h01 << 16), w4.x, o);
-                    o = fmaf(__uint_as_float(h01 & 0xFFFF0000u), w4.y, o);
-                    o = fmaf(__uint_as_float(h23 << 16), w4.z, o);
-                    o = fmaf(__uint_as_float(h23 & 0xFFFF0000u), w4.w, o);
-                }
-            }
-            if (v <= a.n) out_row[v - 1] = (v != u) ? o : -INFINITY;
-            // the next tile's layer-1 epilogue overwrites H only after its own
-            // wait, and its layer 2 (over these TMEM columns) is issued only
-            // after the barrier that follows that epilogue
-            phase ^= 1u;
-        }
-    }
-    if (!ok && tid == 0) atomicExch(a.flag, 1);
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) {
-        // let the MMAs in flight finish before the columns are freed (the
-        // default bound, whatever bound the waits above were given)
-        if (!ok) mbar_wait(last_bar, last_par);
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
-    }
 }
 
 // ------------------------------------------- tensor-core training kernel
@@ -1484,7 +1629,6 @@ int simt_grid(bm_ctx* ctx, int64_t k, int per_sm) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)ctx->num_sms * per_sm));
 }
 
-uint32_t tc_launch_smem(int32_t n) { return std::max(tc_smem_bytes(n), kTcMinSmem); }
 
 bm_status set_attrs(bm_mlp* M) {
     bm_ctx* ctx = M->ctx;
@@ -1492,7 +1636,7 @@ bm_status set_attrs(bm_mlp* M) {
                                       (int)sizeof(MlpSmem)));
     BM_CUDA(ctx, cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(GradSmem)));
-    const uint32_t tcs = tc_launch_smem(M->n);
+    const uint32_t tcs = tc_smem_bytes(M->n);
     if (tcs > ctx->smem_optin)
         return bm_fail(ctx, BM_UNSUPPORTED, "tensor-core scoring needs %u bytes of shared memory", tcs);
     BM_CUDA(ctx, cudaFuncSetAttribute(mlp_rows_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcs));
@@ -1614,8 +1758,8 @@ bm_status launch_row_scores(bm_mlp* M, const int32_t* d_rows, int32_t nrows) {
     const DevGraph& B = ctx->g[1];
     TcArgs a{M->d_img, M->d_tab, d_rows, nrows, M->n, B.out_ptr, B.out_ent, B.in_ptr, B.in_ent, ctx->pi, M->d_sc,
              M->d_flag, ctx->wait_limit > 0 ? (long long)ctx->wait_limit : kWaitLimit};
-    const int grid = std::min(nrows, 2 * ctx->num_sms);
-    mlp_rows_tc_kernel<<<grid, kTcThreads, tc_launch_smem(M->n), ctx->stream>>>(a);
+    const int grid = std::min(nrows, ctx->num_sms);
+    mlp_rows_tc_kernel<<<grid, kTcThreads, tc_smem_bytes(M->n), ctx->stream>>>(a);
     BM_LAUNCH_CHECK(ctx, "mlp_rows_tc_kernel");
     return BM_OK;
 }
