@@ -160,6 +160,7 @@ extern "C" void bm_ctx_destroy(bm_ctx* ctx) {
     if (ctx->row_fork) cudaEventDestroy(ctx->row_fork);
     if (ctx->row_join) cudaEventDestroy(ctx->row_join);
     if (ctx->row_side) cudaStreamDestroy(ctx->row_side);
+    if (ctx->row_graph.exec) cudaGraphExecDestroy(ctx->row_graph.exec);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

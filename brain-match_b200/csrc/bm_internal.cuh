@@ -113,6 +113,15 @@ struct bm_ctx {
     cudaStream_t row_side = nullptr;
     cudaEvent_t row_fork = nullptr;
     cudaEvent_t row_join = nullptr;
+    // bm_rows_best's copy-in, row launches and copy-out as one CUDA graph,
+    // for one row count, valid while every buffer and setting it captured is
+    // unchanged (bm_rows.cu)
+    struct RowGraph {
+        cudaGraphExec_t exec = nullptr;
+        int32_t nrows = -1, n = -1, semantics = -1, row_tiers = 0, row_ctas = -1, row_threads = -1;
+        const void *stage = nullptr, *hstage = nullptr, *pi = nullptr, *ov = nullptr, *a = nullptr, *b = nullptr;
+        int64_t launches = 0;  // kernels per replay
+    } row_graph;
     // host copy of A's adjacency (independence tests of batched swaps)
     std::vector<int32_t> hA_optr, hA_iptr;
     std::vector<uint32_t> hA_oent, hA_ient;

@@ -45,6 +45,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <vector>
 
 #include "bm_internal.cuh"
@@ -1078,6 +1079,104 @@ extern "C" bm_status bm_delta_rows(bm_ctx* ctx, const int32_t* rows, int32_t nro
     return BM_OK;
 }
 
+namespace {
+
+// Whether a host-row launch of nrows rows would take a split plan (then the
+// plan, made per call from the rows, keeps it off the graph path).  An
+// unqueried occupancy counts as yes: the plain path queries it.
+bool split_would_apply(const bm_ctx* ctx, int32_t nrows) {
+    if (ctx->row_split < 0 || !ctx->slots || nrows >= ctx->split_slots_max || ctx->h_rwork.size() != (size_t)ctx->n + 1)
+        return false;
+    if (ctx->row_split > 0) return true;
+    int cl = ctx->row_ctas;
+    if (cl == 0) {
+        cl = 1;
+        while (cl < kMaxCluster && (int64_t)nrows * cl * 2 <= (int64_t)ctx->num_sms * 2) cl *= 2;
+    }
+    const int cached = ctx->split_active[(ctx->row_threads == 256 ? 0 : 1) * (kMaxCluster + 1) + cl];
+    return cached == 0 || cached >= 4 * nrows;
+}
+
+constexpr int32_t kRowGraphMaxRows = 4096;
+
+// bm_rows_best without column bounds as a replayed CUDA graph: the rows are
+// copied (CPU) into pinned staging, the graph copies them in, runs the row
+// launches (tiers included) and copies the results out to pinned staging,
+// from which they are copied (CPU) to the caller.  The first call of a row
+// count runs plainly and then captures the graph; a change of row count,
+// staging buffers, graphs, semantics or row settings captures it again.
+bm_status rows_best_graph(bm_ctx* ctx, const int32_t* rows, int32_t nrows, bm_row_result* out) {
+    const size_t rb = (sizeof(int32_t) * (size_t)nrows + 255) & ~(size_t)255;
+    const size_t ob = sizeof(bm_row_result) * (size_t)nrows;
+    bm_status s = bm_stage(ctx, rb + ob);
+    if (s != BM_OK) return s;
+    if ((s = bm_hstage(ctx, rb + ob)) != BM_OK) return s;
+    bm_ctx::RowGraph& G = ctx->row_graph;
+    const bool hit = G.exec && G.nrows == nrows && G.n == ctx->n && G.semantics == ctx->semantics &&
+                     G.row_tiers == ctx->row_tiers && G.row_ctas == ctx->row_ctas && G.row_threads == ctx->row_threads &&
+                     G.stage == ctx->stage && G.hstage == ctx->hstage && G.pi == ctx->pi && G.ov == ctx->ov &&
+                     G.a == ctx->g[0].out_ptr && G.b == ctx->g[1].out_ptr;
+    int32_t* d_rows = (int32_t*)ctx->stage;
+    bm_row_result* d_out = (bm_row_result*)((char*)ctx->stage + rb);
+    int32_t* h_in = (int32_t*)ctx->hstage;
+    bm_row_result* h_out = (bm_row_result*)((char*)ctx->hstage + rb);
+    if (hit) {
+        std::memcpy(h_in, rows, sizeof(int32_t) * (size_t)nrows);
+        BM_CUDA(ctx, cudaGraphLaunch(G.exec, ctx->stream));
+        BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        ctx->launches += G.launches;
+        std::memcpy(out, h_out, ob);
+        return BM_OK;
+    }
+    if (G.exec) {
+        cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+    }
+    // this call runs plainly (it also sets the kernel attributes and the
+    // occupancy figures the launches read), then the graph is captured
+    BM_CUDA(ctx, cudaMemcpyAsync(d_rows, rows, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = bm_launch_rows(ctx, d_rows, nullptr, nrows, nullptr, d_out, nullptr)) != BM_OK) return s;
+    BM_CUDA(ctx, cudaMemcpyAsync(out, d_out, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const int64_t l0 = ctx->launches;
+    cudaGraph_t graph = nullptr;
+    BM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t c1 = cudaMemcpyAsync(d_rows, h_in, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream);
+    const bm_status ls = c1 == cudaSuccess ? bm_launch_rows(ctx, d_rows, nullptr, nrows, nullptr, d_out, nullptr) : BM_OK;
+    const cudaError_t c2 = cudaMemcpyAsync(h_out, d_out, ob, cudaMemcpyDeviceToHost, ctx->stream);
+    const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    const int64_t captured = ctx->launches - l0;
+    ctx->launches = l0;
+    if (ls != BM_OK || c1 != cudaSuccess || c2 != cudaSuccess || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (ls != BM_OK) return ls;
+        return bm_cuda_fail(ctx, c1 != cudaSuccess ? c1 : c2 != cudaSuccess ? c2 : ce, "row graph capture");
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        G.exec = nullptr;
+        return bm_cuda_fail(ctx, ie, "row graph instantiation");
+    }
+    G.launches = captured;
+    G.nrows = nrows;
+    G.n = ctx->n;
+    G.semantics = ctx->semantics;
+    G.row_tiers = ctx->row_tiers;
+    G.row_ctas = ctx->row_ctas;
+    G.row_threads = ctx->row_threads;
+    G.stage = ctx->stage;
+    G.hstage = ctx->hstage;
+    G.pi = ctx->pi;
+    G.ov = ctx->ov;
+    G.a = ctx->g[0].out_ptr;
+    G.b = ctx->g[1].out_ptr;
+    return BM_OK;
+}
+
+}  // namespace
+
 extern "C" bm_status bm_rows_best(bm_ctx* ctx, const int32_t* rows, const int32_t* col_lo, int32_t nrows,
                                   bm_row_result* out) {
     bm_status s = bm_require_mapped(ctx);
@@ -1085,6 +1184,7 @@ extern "C" bm_status bm_rows_best(bm_ctx* ctx, const int32_t* rows, const int32_
     if (nrows < 0 || (nrows > 0 && (!rows || !out))) return bm_fail(ctx, BM_INVALID_ARG, "bad row buffers");
     if (nrows == 0) return BM_OK;
     if ((s = check_rows(ctx, rows, nrows)) != BM_OK) return s;
+    if (!col_lo && nrows <= kRowGraphMaxRows && !split_would_apply(ctx, nrows)) return rows_best_graph(ctx, rows, nrows, out);
     const size_t rb = (sizeof(int32_t) * (size_t)nrows + 255) & ~(size_t)255;
     const size_t ob = sizeof(bm_row_result) * (size_t)nrows;
     if ((s = bm_stage(ctx, 2 * rb + ob)) != BM_OK) return s;

@@ -153,3 +153,38 @@ def test_tier_setting_validation(cfg1):
     e.set_row_tiers(5)
     assert e.row_tiers() == 5
     e.set_row_tiers(0)
+
+
+def test_host_rows_graph_replays(cfg1):
+    """bm_rows_best without column bounds runs as a captured CUDA graph per row
+    count: replays with new rows, a new row count, changed settings and a
+    changed mapping all give the device-rows path's results, and each replay
+    counts its kernels."""
+    n, A, B, e = cfg1
+    e.set_row_tiers(0)
+    for k, seed in ((57, 1), (57, 2), (57, 3), (40, 4), (57, 5), (100, 6), (100, 7)):
+        rows = _rows(n, A, k, seed=200 + seed)
+        c0 = e.launch_count()
+        got = e.rows_best(rows)
+        launches = e.launch_count() - c0
+        exp, dev_launches = _dev_best(e, rows)
+        np.testing.assert_array_equal(got, exp)
+        assert launches == dev_launches
+    rows = _rows(n, A, 57, seed=300)
+    for tiers in (-1, 2, 0):
+        e.set_row_tiers(tiers)
+        np.testing.assert_array_equal(e.rows_best(rows), _dev_best(e, rows)[0])
+        np.testing.assert_array_equal(e.rows_best(rows), _dev_best(e, rows)[0])
+    # a changed mapping: the graph reads the current one
+    pi0 = e.get_mapping()
+    best = e.rows_best(rows)
+    i = int(np.argmax(best["best_delta"]))
+    assert best["best_delta"][i] > 0
+    e.apply_swaps(np.array([[best["row"][i], best["best"][i]]], np.int32), np.array([best["best_delta"][i]], np.int64))
+    try:
+        got = e.rows_best(rows)
+        np.testing.assert_array_equal(got, _dev_best(e, rows)[0])
+        assert not np.array_equal(got, best)
+    finally:
+        e.set_mapping(pi0)
+    np.testing.assert_array_equal(e.rows_best(rows), best)
