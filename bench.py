@@ -372,8 +372,9 @@ def run_ours(args, ws, rank, local, dist):
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak,
                         "traffic": traffic, "peak_source": peak_kind,
-                        "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of "
-                                           f"{traffic_rec['launches']} timed launches of this command, kernel "
+                        "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of the row launches, "
+                                           f"summed per step (a step's rows may run as two launches), mean of "
+                                           f"{traffic_rec['steps']} timed steps of this command, kernel "
                                            f"source digest {traffic_rec['kernel_digest']}") if traffic_rec else
                                           "no ncu record of this kernel source and command",
                         "l2_peak": l2, "l2_frac": (achieved / l2) if l2 else None,
@@ -429,16 +430,17 @@ def rows_kernel_digest() -> str:
 
 
 def recorded_traffic(steps: int, warmup: int, rows_per_step: int):
-    """DRAM bytes (read + write) per rows_kernel launch from an ncu capture of
-    this bench's own launches (the record names the capture and the digest of
-    the kernel's sources it was taken on); None unless the record is of the
-    current kernel source and of this run's steps, warm-up and batch size."""
+    """DRAM bytes (read + write) of the row kernel per step (the step's
+    launches summed) from an ncu capture of this bench's own launches (the
+    record names the capture and the digest of the kernel's sources it was
+    taken on); None unless the record is of the current kernel source and of
+    this run's steps, warm-up and batch size."""
     try:
         with open(TRAFFIC_RECORD) as f:
             rec = json.load(f)
         if (rec["kernel_digest"] == rows_kernel_digest() and rec["steps"] == steps and rec["warmup"] == warmup
                 and rec["rows_per_step"] == rows_per_step):
-            return float(rec["dram_bytes_per_launch"]), rec
+            return float(rec["dram_bytes_per_step"]), rec
     except (OSError, ValueError, KeyError):
         pass
     return None, None
