@@ -158,6 +158,42 @@ def test_row_scores_match_fp64_oracle(golden_cfg1, backend):
     e.close()
 
 
+def test_row_scores_several_rows_per_cta(golden_cfg1):
+    """More rows than SMs: the scorer's CTAs take several rows each (the
+    feature groups rebuild their candidate bitmaps at every row change, the
+    output groups switch rows mid-pipeline).  Rows that are a CTA's second or
+    third are checked against the FP64 oracle, all rows against the SIMT
+    scorer, and a repeated row gives identical scores wherever it lands."""
+    n, A, B = golden_graphs(golden_cfg1)
+    e = make_engine(n, A, B, golden_cfg1["pi_init"])
+    m = bm.Mlp(e, seed=5)
+    rng = np.random.default_rng(11)
+    R = 333  # 2 or 3 rows per CTA on a 148-SM B200 (one CTA per SM)
+    rows = rng.integers(1, n + 1, R).astype(np.int32)
+    rows[-1] = rows[0]
+    m.set_backend(0)
+    sc = m.score_rows(rows)
+    m.set_backend(1)
+    ref = m.score_rows(rows)
+    m.set_backend(0)
+    np.testing.assert_array_equal(sc[-1], sc[0])
+    for r, u in enumerate(rows):
+        assert sc[r, u - 1] == -np.inf
+    fin = np.isfinite(ref)
+    err = np.abs(sc[fin] - ref[fin]) / (1.0 + np.abs(ref[fin]))
+    assert np.quantile(err, 0.99) < 2e-3, np.quantile(err, 0.99)
+    pick = np.array([R - 40, R - 20, R - 2], np.int64)
+    v = np.arange(1, n + 1, dtype=np.int32)
+    pairs = np.stack([np.repeat(rows[pick], n), np.tile(v, len(pick))], 1).astype(np.int32)
+    keep = pairs[:, 0] != pairs[:, 1]
+    o = mlp_oracle(m.params(), m.pair_features(pairs[keep]), rounding=True)[0]
+    got = sc[pick].reshape(-1)[keep].astype(np.float64)
+    err = np.abs(got - o) / (1.0 + np.abs(o))
+    assert np.quantile(err, 0.99) < 2e-3, np.quantile(err, 0.99)
+    assert err.max() < 3e-2, err.max()
+    e.close()
+
+
 def test_simt_rows_equal_simt_pairs(golden_cfg1):
     n, A, B = golden_graphs(golden_cfg1)
     e = make_engine(n, A, B, golden_cfg1["pi_init"])
