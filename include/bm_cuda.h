@@ -460,7 +460,10 @@ bm_status bm_greedy_match_dev(bm_ctx* ctx, int32_t n, int64_t mA, const int32_t*
  * BF16 inputs, weights and activations, FP32 accumulation and FP32 master
  * weights.  Parameters are packed as W1[24][128] b1[128] W2[128][128] b2[128]
  * w3[128] b3 (W[i][j]: input i, output j), bm_mlp_num_params() floats.
- * A model is bound to the context (and the graphs) it was created on. */
+ * A model is bound to the context (and the graphs) it was created on.
+ * bm_mlp_create returns BM_UNSUPPORTED when the tensor-core row scorer's
+ * shared memory (about 141 KB + n / 2 bytes of candidate bitmaps) exceeds the
+ * device's per-block limit: n above about 180,000 vertices on a B200. */
 typedef struct bm_mlp bm_mlp;
 
 bm_status bm_mlp_create(bm_ctx* ctx, uint64_t seed, bm_mlp** out);
