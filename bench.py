@@ -403,6 +403,8 @@ def run_ours(args, ws, rank, local, dist):
     eng.close()
     if rank == 0 and ws == 1 and args.learned_seconds > 0 and out.get("search", {}).get("converged"):
         out["learned_vs_plain"] = learned_compare(local, A, B, init, rows, out["search"], args.learned_seconds)
+    if rank == 0 and ws == 1 and args.learned_seconds > 0:
+        out["learned_vs_uniform"] = learned_vs_uniform(local, A, B, init, rows)
     if rank == 0 and ws == 1 and not args.no_extras:
         out["initial_matching"] = initial_matching(local, A, B, init)
         out["higher_order"] = higher_order(local, A, B, init, not args.no_reference_gpu)
@@ -633,6 +635,49 @@ def learned_compare(device, A, B, init, rows, plain, seconds):
     return out
 
 
+def learned_vs_uniform(device, A, B, init, rows, uniform_seconds=8.0):
+    """Proposal searches with exact checks from the greedy matching: uniform
+    random partners (64 per row, 4,736 rows per batch: the fastest of the
+    uniform settings measured) for uniform_seconds, then the model's top 32 of
+    1,024 sampled partners per row (2,368 rows per batch, feature table
+    refreshed every 4 batches) until it reaches the uniform search's score,
+    with record harvest and training inside its clock.  Same seed and start."""
+    def engine():
+        e = bm.Engine(device)
+        e.set_graphs(A, B)
+        e.set_mapping(init)
+        return e
+
+    e = engine()
+    m = bm.Mlp(e, seed=1)
+    t0 = time.perf_counter()
+    _, p, s = m.search(rows, topk=64, uniform=True, exact_fallback=False, time_budget=uniform_seconds, seed=7,
+                       rows_per_batch=4736)
+    t_u = time.perf_counter() - t0
+    out = {"uniform": {"seconds": t_u, "score": int(p.score), "proposals": int(s.proposals), "sweeps": int(p.sweeps),
+                       "hit_rate": s.hits / max(1, s.proposals), "topk": 64, "rows_per_batch": 4736}}
+    e.close()
+    e = engine()
+    t0 = time.perf_counter()
+    m = bm.Mlp(e, seed=1)
+    m.reserve_records(5_000_000)
+    nrec = m.collect_rows(rows, per_row=256, seed=3)
+    m.fit(1500, batch=8192, lr=2e-3)
+    e.sync()
+    t_train = time.perf_counter() - t0
+    st, p2, s2 = m.search(rows, topk=32, sample=1024, exact_fallback=False, target_score=out["uniform"]["score"],
+                          time_budget=2 * uniform_seconds, seed=7, rows_per_batch=2368, refresh_batches=4)
+    t_l = time.perf_counter() - t0
+    reached = p2.score >= out["uniform"]["score"]
+    out["learned"] = {"seconds": t_l, "reached": bool(reached), "score": int(p2.score), "harvest_train_s": t_train,
+                      "records": int(nrec), "proposals": int(s2.proposals), "sweeps": int(p2.sweeps),
+                      "hit_rate": s2.hits / max(1, s2.proposals), "t_propose": s2.t_propose, "t_exact": s2.t_exact,
+                      "topk": 32, "sample": 1024, "rows_per_batch": 2368}
+    out["time_ratio"] = (t_l / t_u) if reached else None
+    e.close()
+    return out
+
+
 def higher_order(device, A, B, init, reference_kernels=True):
     """Exact k-set permutation deltas on the full-scale pair: 4,096 random
     8-subsets (8! = 40,320 permutations each) and 65,536 3-vertex sets along
@@ -808,6 +853,8 @@ def run_section(args):
             out = delta_table(0, A, B, init, {})
         elif args.only == "mlp_scorer":
             out = scorer_throughput(0, A, B, init, rows)
+        elif args.only == "learned_vs_uniform":
+            out = learned_vs_uniform(0, A, B, init, rows)
         else:
             out = subset_assignment(0, A, B, init, "initial matching")
     print(json.dumps({"section": args.only, "result": out}), flush=True)
@@ -834,7 +881,7 @@ def main():
     ap.add_argument("--sa-candidates", type=int, default=0, help="starting proposals per iteration (0: autotuned)")
     ap.add_argument("--only", default=None,
                     choices=["initial_matching", "higher_order", "delta_table", "subset_assignment", "sa_chains",
-                             "mlp_scorer"],
+                             "mlp_scorer", "learned_vs_uniform"],
                     help="run one side section alone and print its result (a profiling target, not a bench line)")
     args = ap.parse_args()
     if args.write_workload:

@@ -313,7 +313,8 @@ struct PairSrc {
     const uint16_t* xbf;
     const int32_t* pairs;
     const int32_t* rows;
-    int32_t n;
+    int32_t n;             // partners per row: all vertices, or cands' row length
+    const int32_t* cands;  // [rows][n] partner lists; null = partners 1..n
 };
 
 __device__ __forceinline__ bool load_pair(const FeatSrc& F, const PairSrc& P, int64_t q, float* x) {
@@ -331,7 +332,7 @@ __device__ __forceinline__ bool load_pair(const FeatSrc& F, const PairSrc& P, in
         v = P.pairs[2 * q + 1];
     } else {
         u = P.rows[q / P.n];
-        v = (int32_t)(q % P.n) + 1;
+        v = P.cands ? P.cands[q] : (int32_t)(q % P.n) + 1;
     }
     if (u == v) {
         for (int i = 0; i < BM_MLP_IN; i++) x[i] = 0.f;
@@ -825,9 +826,11 @@ struct TcArgs {
     const int32_t* b_iptr;
     const uint32_t* b_ient;
     const int32_t* pi;
-    float* scores;  // [nrows x n], row r at r * n, partner v at v - 1
+    float* scores;  // [nrows x span], row r at r * span: partner v at v - 1, or list entry i at i
     int32_t* flag;
     long long wait_limit;  // bound of each MMA-completion wait, SM cycles
+    const int32_t* cands;  // [nrows x span] partner lists (never u itself); null = partners 1..n
+    int32_t span;          // n, or the lists' length
 };
 
 // Candidate v's vertex record (12 floats).
@@ -966,7 +969,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) mlp_rows_tc_kernel(TcArgs a) {
     const uint32_t tmem = *tmem_slot;
 
     // the CTA's tiles: rows blockIdx.x, blockIdx.x + gridDim.x, ...; tiles of 128 candidates
-    const int32_t tpr = (a.n + 127) / 128;
+    const int32_t tpr = (a.span + 127) / 128;
     const int32_t my_rows = a.nrows > (int32_t)blockIdx.x ? (a.nrows - 1 - (int32_t)blockIdx.x) / (int32_t)gridDim.x + 1 : 0;
     const int32_t T = my_rows * tpr;
     auto tile_row = [&](int32_t t, int32_t& r, int32_t& v0) {
@@ -1015,7 +1018,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) mlp_rows_tc_kernel(TcArgs a) {
                 for (int i = 0; i < BM_FT; i++) ta[i] = a.tab[(size_t)u * BM_FT + i];
                 role_bar(gbar);
             }
-            build_features(a, ta, bits_out, bits_in, u, v0 + gtid, load_cand(a, v0 + gtid), sm + kSmX + grp * kSmXBytes, gtid);
+            // candidate: partner v0 + gtid, or list entry v0 - 1 + gtid (past the list: none)
+            const int32_t ci = v0 - 1 + gtid;
+            const int32_t v = a.cands ? (ci < a.span ? __ldg(a.cands + (size_t)r * a.span + ci) : a.n + 1) : v0 + gtid;
+            build_features(a, ta, bits_out, bits_in, u, v, load_cand(a, v), sm + kSmX + grp * kSmXBytes, gtid);
             proxy_fence();
             role_bar(gbar);
             if (leader) {
@@ -1113,8 +1119,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) mlp_rows_tc_kernel(TcArgs a) {
             const float o = __uint_as_float(tmem_ld1(d2 + 64u)) + b3;
             tc_fence_before();
             mbar_arrive(bar(DFREE, q));  // the slot is free for tile t + 4
-            const int32_t v = v0 + gtid;
-            if (v <= a.n) a.scores[(size_t)r * a.n + (v - 1)] = (v != u) ? o : -INFINITY;
+            const int32_t ci = v0 - 1 + gtid;
+            if (ci < a.span) a.scores[(size_t)r * a.span + ci] = (a.cands || ci + 1 != u) ? o : -INFINITY;
         }
     }
     if (!ok) {
@@ -1595,12 +1601,49 @@ __global__ void __launch_bounds__(kTopThreads) topk_kernel(const float* __restri
     }
 }
 
+// S distinct partners other than u for every row: u's other n - 1 ids taken
+// along an arithmetic progression modulo n - 1 with a random start and a
+// random step coprime to n - 1 (Philox, counter = row id, call), so each
+// listed partner is uniform and no two repeat.  One warp per row; S <= n - 1.
+__global__ void sample_cands_kernel(const int32_t* __restrict__ rows, int32_t nrows, int32_t S, int32_t n, uint64_t seed,
+                                    uint64_t call, int32_t* __restrict__ cands) {
+    const int32_t warps = (int32_t)(gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t m = (uint32_t)(n - 1);
+    for (int32_t i = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < nrows; i += warps) {
+        const int32_t u = rows[i];
+        uint32_t start = 0, step = 1;
+        if (lane == 0 && m > 1) {
+            const uint32_t c[4] = {(uint32_t)i, (uint32_t)u, (uint32_t)call, 0x53414D50u};
+            const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+            uint32_t o[4];
+            bm_philox4x32_10(c, key, o);
+            start = o[0] % m;
+            step = 1u + o[1] % (m - 1u);
+            auto gcd = [](uint32_t x, uint32_t y) {
+                while (y) { const uint32_t t = x % y; x = y; y = t; }
+                return x;
+            };
+            while (gcd(step, m) != 1u) step = step + 1u < m ? step + 1u : 1u;
+        }
+        start = __shfl_sync(0xffffffffu, start, 0);
+        step = __shfl_sync(0xffffffffu, step, 0);
+        for (int32_t j = lane; j < S; j += 32) {
+            const uint32_t idx = (uint32_t)(((uint64_t)start + (uint64_t)j * step) % m);
+            int32_t v = 1 + (int32_t)idx;
+            if (v >= u) v++;
+            cands[(size_t)i * S + j] = v;
+        }
+    }
+}
+
 // pairs (u, partner) of every row's K proposals; an empty slot gives (u, u).
-// With `uniform` set, partners are uniform random ids other than u instead
-// (Philox, counter = row id, slot, call).
+// topv holds partner ids, or, with cands, positions + 1 in the rows' S-long
+// partner lists.  With `uniform` set, partners are uniform random ids other
+// than u instead (Philox, counter = row id, slot, call).
 __global__ void proposal_pairs_kernel(const int32_t* __restrict__ rows, const int32_t* __restrict__ topv, int32_t nrows,
                                       int32_t K, int32_t n, int32_t uniform, uint64_t seed, uint64_t call,
-                                      int32_t* __restrict__ pairs) {
+                                      int32_t* __restrict__ pairs, const int32_t* __restrict__ cands, int32_t S) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows * K; i += gridDim.x * blockDim.x) {
         const int32_t u = rows[i / K];
         int32_t v;
@@ -1614,6 +1657,8 @@ __global__ void proposal_pairs_kernel(const int32_t* __restrict__ rows, const in
                 v = 1 + (int32_t)(o[0] % (uint32_t)(n - 1));
                 if (v >= u) v++;
             }
+        } else if (cands) {
+            v = topv[i] > 0 ? cands[(size_t)(i / K) * S + (topv[i] - 1)] : u;
         } else {
             v = topv[i] > 0 ? topv[i] : u;
         }
@@ -1733,9 +1778,13 @@ bm_status launch_adamw(bm_mlp* M, float lr, float wd) {
 }
 
 // Scores of rows x all partners into M->d_sc (row r at r * n).
-bm_status launch_row_scores(bm_mlp* M, const int32_t* d_rows, int32_t nrows) {
+// Scores of rows x all partners into M->d_sc (row r at r * n), or, with
+// d_cands, of rows x their S listed partners (row r at r * S).
+bm_status launch_row_scores(bm_mlp* M, const int32_t* d_rows, int32_t nrows, const int32_t* d_cands = nullptr,
+                            int32_t S = 0) {
     bm_ctx* ctx = M->ctx;
-    const size_t need = (size_t)nrows * (size_t)M->n;
+    const int32_t span = d_cands ? S : M->n;
+    const size_t need = (size_t)nrows * (size_t)span;
     if (need > M->sc_cap) {
         bm_cuda_free(M->d_sc);
         M->d_sc = nullptr;
@@ -1747,8 +1796,8 @@ bm_status launch_row_scores(bm_mlp* M, const int32_t* d_rows, int32_t nrows) {
         M->sc_cap = need;
     }
     if (M->backend == 1) {
-        PairSrc P{nullptr, nullptr, nullptr, d_rows, M->n};
-        return launch_score_simt(M, P, (int64_t)nrows * M->n, M->d_sc);
+        PairSrc P{nullptr, nullptr, nullptr, d_rows, span, d_cands};
+        return launch_score_simt(M, P, (int64_t)nrows * span, M->d_sc);
     }
     if (M->img_dirty) {
         prep_image_kernel<<<64, 256, 0, ctx->stream>>>(M->d_w, M->d_img);
@@ -1757,16 +1806,16 @@ bm_status launch_row_scores(bm_mlp* M, const int32_t* d_rows, int32_t nrows) {
     }
     const DevGraph& B = ctx->g[1];
     TcArgs a{M->d_img, M->d_tab, d_rows, nrows, M->n, B.out_ptr, B.out_ent, B.in_ptr, B.in_ent, ctx->pi, M->d_sc,
-             M->d_flag, ctx->wait_limit > 0 ? (long long)ctx->wait_limit : kWaitLimit};
+             M->d_flag, ctx->wait_limit > 0 ? (long long)ctx->wait_limit : kWaitLimit, d_cands, span};
     const int grid = std::min(nrows, ctx->num_sms);
     mlp_rows_tc_kernel<<<grid, kTcThreads, tc_smem_bytes(M->n), ctx->stream>>>(a);
     BM_LAUNCH_CHECK(ctx, "mlp_rows_tc_kernel");
     return BM_OK;
 }
 
-bm_status launch_topk(bm_mlp* M, int32_t nrows, int32_t K, int32_t* d_v, float* d_s) {
+bm_status launch_topk(bm_mlp* M, int32_t nrows, int32_t K, int32_t* d_v, float* d_s, int32_t span = 0) {
     bm_ctx* ctx = M->ctx;
-    topk_kernel<<<nrows, kTopThreads, 0, ctx->stream>>>(M->d_sc, M->n, K, d_v, d_s);
+    topk_kernel<<<nrows, kTopThreads, 0, ctx->stream>>>(M->d_sc, span > 0 ? span : M->n, K, d_v, d_s);
     BM_LAUNCH_CHECK(ctx, "topk_kernel");
     return BM_OK;
 }
@@ -2082,6 +2131,33 @@ extern "C" bm_status bm_mlp_score_rows_dev(bm_mlp* M, const int32_t* d_rows, int
     return BM_OK;
 }
 
+extern "C" bm_status bm_mlp_score_candidates(bm_mlp* M, const int32_t* rows, int32_t nrows, const int32_t* cands,
+                                             int32_t S, float* scores) {
+    bm_status s = mlp_check(M);
+    if (s != BM_OK) return s;
+    bm_ctx* ctx = M->ctx;
+    if (nrows < 0 || S < 1 || (nrows > 0 && (!rows || !cands || !scores)))
+        return bm_fail(ctx, BM_INVALID_ARG, "bad buffers or S < 1");
+    if (nrows == 0) return BM_OK;
+    if ((s = check_ids(ctx, rows, nrows, "rows")) != BM_OK) return s;
+    for (int64_t i = 0; i < (int64_t)nrows * S; i++) {
+        const int32_t v = cands[i];
+        if (v < 1 || v > ctx->n || v == rows[i / S])
+            return bm_fail(ctx, BM_INVALID_ARG, "candidate %lld = %d is outside 1..%d or its row's vertex", (long long)i,
+                           v, ctx->n);
+    }
+    const size_t rb = al256(sizeof(int32_t) * (size_t)nrows);
+    if ((s = scratch(M, rb + sizeof(int32_t) * (size_t)nrows * (size_t)S)) != BM_OK) return s;
+    int32_t* d_r = (int32_t*)M->d_scr;
+    int32_t* d_c = (int32_t*)((char*)M->d_scr + rb);
+    BM_CUDA(ctx, cudaMemcpyAsync(d_r, rows, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream));
+    BM_CUDA(ctx, cudaMemcpyAsync(d_c, cands, sizeof(int32_t) * (size_t)nrows * S, cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = launch_row_scores(M, d_r, nrows, d_c, S)) != BM_OK) return s;
+    BM_CUDA(ctx, cudaMemcpyAsync(scores, M->d_sc, sizeof(float) * (size_t)nrows * S, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    return check_flag(M);
+}
+
 extern "C" bm_status bm_mlp_status(bm_mlp* M) {
     if (!M || !M->ctx) return BM_INVALID_ARG;
     return check_flag(M);
@@ -2234,12 +2310,17 @@ extern "C" bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* M, const int32_t* ro
     }
     const int32_t nr = (int32_t)order.size();
     const int32_t R = std::min(nr, p->rows_per_batch > 0 ? p->rows_per_batch : 2 * ctx->num_sms);
+    if (p->sample < 0) return bm_fail(ctx, BM_INVALID_ARG, "sample must be 0 (all partners) or a partner count");
+    // sampled scoring: the model scores S random partners per row (distinct,
+    // never u) and proposes the top K of them; S >= n - 1 scores every partner
+    const int32_t S = (!p->uniform && p->sample > 0 && p->sample < n - 1) ? std::max(p->sample, K) : 0;
     const int64_t RK = (int64_t)R * K;
     const size_t rb = al256(sizeof(int32_t) * (size_t)R);
     const size_t vb = al256(sizeof(int32_t) * (size_t)RK);
     const size_t pb = al256(sizeof(int32_t) * 2 * (size_t)RK);
     const size_t db = al256(sizeof(long long) * (size_t)RK);
-    if ((s = scratch(M, rb + 2 * vb + pb + db + pb)) != BM_OK) return s;
+    const size_t cb = al256(sizeof(int32_t) * (size_t)R * (size_t)S);
+    if ((s = scratch(M, rb + 2 * vb + pb + db + pb + cb)) != BM_OK) return s;
     char* base = (char*)M->d_scr;
     int32_t* d_r = (int32_t*)base;
     int32_t* d_tv = (int32_t*)(base + rb);
@@ -2247,6 +2328,7 @@ extern "C" bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* M, const int32_t* ro
     int32_t* d_p = (int32_t*)(base + rb + 2 * vb);
     long long* d_d = (long long*)(base + rb + 2 * vb + pb);
     int32_t* d_ap = (int32_t*)(base + rb + 2 * vb + pb + db);
+    int32_t* d_c = S ? (int32_t*)(base + rb + 2 * vb + pb + db + pb) : nullptr;
     std::vector<int32_t> h_p((size_t)2 * RK), h_ap((size_t)2 * R);
     std::vector<long long> h_d((size_t)RK);
     std::vector<int32_t> cand;
@@ -2271,12 +2353,18 @@ extern "C" bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* M, const int32_t* ro
         }
         BM_CUDA(ctx, cudaMemcpyAsync(d_r, order.data() + pos, sizeof(int32_t) * (size_t)k, cudaMemcpyHostToDevice,
                                      ctx->stream));
-        if (!p->uniform) {
+        if (!p->uniform && S) {
+            sample_cands_kernel<<<(int)std::min<int64_t>(((int64_t)k * 32 + 255) / 256, 4096), 256, 0, ctx->stream>>>(
+                d_r, k, S, n, p->seed, (uint64_t)batch, d_c);
+            BM_LAUNCH_CHECK(ctx, "sample_cands_kernel");
+            if ((s = launch_row_scores(M, d_r, k, d_c, S)) != BM_OK) return s;
+            if ((s = launch_topk(M, k, K, d_tv, d_ts, S)) != BM_OK) return s;
+        } else if (!p->uniform) {
             if ((s = launch_row_scores(M, d_r, k)) != BM_OK) return s;
             if ((s = launch_topk(M, k, K, d_tv, d_ts)) != BM_OK) return s;
         }
         proposal_pairs_kernel<<<(int)std::min<int64_t>((k * (int64_t)K + 255) / 256, 4096), 256, 0, ctx->stream>>>(
-            d_r, d_tv, k, K, n, p->uniform, p->seed, (uint64_t)batch, d_p);
+            d_r, d_tv, k, K, n, p->uniform, p->seed, (uint64_t)batch, d_p, d_c, S);
         BM_LAUNCH_CHECK(ctx, "proposal_pairs_kernel");
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         st->t_propose += secs_since(ta);

@@ -74,7 +74,7 @@ class LearnedParams(C.Structure):
                 ("train_every", C.c_int32),
                 ("train_batch", C.c_int32), ("lr", C.c_float), ("weight_decay", C.c_float), ("seed", C.c_uint64),
                 ("max_accepts", C.c_int64), ("max_sweeps", C.c_int32), ("time_budget_s", C.c_double),
-                ("target_score", C.c_int64)]
+                ("target_score", C.c_int64), ("sample", C.c_int32)]
 
 
 class LearnedStats(C.Structure):
@@ -213,6 +213,7 @@ def cuda_lib() -> C.CDLL:
             "bm_mlp_score_rows": (C.c_int, [vp, vp, C.c_int32, vp]),
             "bm_mlp_rows_topk": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp]),
             "bm_mlp_score_rows_dev": (C.c_int, [vp, vp, C.c_int32, vp]),
+            "bm_mlp_score_candidates": (C.c_int, [vp, vp, C.c_int32, vp, C.c_int32, vp]),
             "bm_mlp_status": (C.c_int, [vp]),
             "bm_mlp_gradients": (C.c_int, [vp, vp, vp, C.c_int64, vp, C.POINTER(C.c_float)]),
             "bm_mlp_adamw_step": (C.c_int, [vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.POINTER(C.c_float)]),
@@ -989,6 +990,15 @@ class Mlp:
         self._chk(self.L.bm_mlp_score_rows(self.h, _ptr(r), r.shape[0], _ptr(out)), "bm_mlp_score_rows")
         return out
 
+    def score_candidates(self, rows, cands) -> np.ndarray:
+        """bm_mlp_score_candidates: scores (nrows x S) of the listed partners."""
+        r = _i32(rows).reshape(-1)
+        c = _i32(cands).reshape(r.shape[0], -1)
+        out = np.zeros(c.shape, np.float32)
+        self._chk(self.L.bm_mlp_score_candidates(self.h, _ptr(r), r.shape[0], _ptr(c), c.shape[1], _ptr(out)),
+                  "bm_mlp_score_candidates")
+        return out
+
     def score_rows_dev(self, d_rows: int, nrows: int, d_scores: int) -> None:
         self._chk(self.L.bm_mlp_score_rows_dev(self.h, d_rows, nrows, d_scores), "bm_mlp_score_rows_dev")
 
@@ -1039,11 +1049,11 @@ class Mlp:
 
     def search(self, rows=None, topk=64, rows_per_batch=0, refresh_batches=1, uniform=False, exact_fallback=True,
                fallback_accepts=0, train_every=0, train_batch=4096, lr=1e-3, weight_decay=0.0, seed=1,
-               max_accepts=-1, max_sweeps=-1, time_budget=0.0, target_score=0, prog=None, stats=None):
+               max_accepts=-1, max_sweeps=-1, time_budget=0.0, target_score=0, prog=None, stats=None, sample=0):
         """bm_search_learned; returns (status, Progress, LearnedStats)."""
         prm = LearnedParams(topk, rows_per_batch, refresh_batches, int(bool(uniform)), int(bool(exact_fallback)),
                             fallback_accepts, train_every, train_batch, lr, weight_decay, seed, max_accepts,
-                            max_sweeps, time_budget, target_score)
+                            max_sweeps, time_budget, target_score, sample)
         prog = prog or Progress()
         stats = stats or LearnedStats()
         r = None if rows is None else _i32(rows)

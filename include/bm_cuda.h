@@ -491,6 +491,11 @@ bm_status bm_mlp_score_rows(bm_mlp* m, const int32_t* rows, int32_t nrows, float
  * produced in the model's own buffer and copied to d_scores).  A tensor-core
  * wait that ran out is reported by the next bm_mlp_status or host-side call. */
 bm_status bm_mlp_score_rows_dev(bm_mlp* m, const int32_t* d_rows, int32_t nrows, float* d_scores);
+/* Scores of listed partners: scores[r * S + i] for partner cands[r * S + i]
+ * of row rows[r] (1..n, not the row's own vertex), on the same kernels as
+ * bm_mlp_score_rows and equal to its scores at those partners. */
+bm_status bm_mlp_score_candidates(bm_mlp* m, const int32_t* rows, int32_t nrows, const int32_t* cands, int32_t S,
+                                  float* scores);
 /* Synchronise and report (then clear) the tensor-core kernel's error flag:
  * BM_TIMEOUT if an MMA completion wait ran out, else BM_OK. */
 bm_status bm_mlp_status(bm_mlp* m);
@@ -537,6 +542,9 @@ typedef struct bm_learned_params {
     int32_t max_sweeps;       /* < 0: unlimited */
     double time_budget_s;     /* <= 0: none */
     int64_t target_score;     /* > 0: stop once the score reaches it */
+    int32_t sample;           /* 0: the model scores every partner of a row; S > 0: it scores S distinct
+                                 random partners per row (Philox, fresh per batch) and proposes the top-K
+                                 of those (S below K counts as K; S of n - 1 or more means every partner) */
 } bm_learned_params;
 
 typedef struct bm_learned_stats {
@@ -547,10 +555,11 @@ typedef struct bm_learned_stats {
     double t_propose, t_exact, t_train;  /* seconds in features + scoring + top-K, exact checks + applies, training */
 } bm_learned_stats;
 
-/* Search that proposes the top-K partners of each row (model or uniform),
- * checks them with the exact delta, and applies the best improving proposal
- * of each row when it is independent of those already taken (descending
- * delta).  Stats accumulate into *stats. */
+/* Search that proposes the top-K partners of each row (model, over all
+ * partners or over a random sample of them, or uniform), checks them with the
+ * exact delta, and applies the best improving proposal of each row when it is
+ * independent of those already taken (descending delta).  Stats accumulate
+ * into *stats. */
 bm_status bm_search_learned(bm_ctx* ctx, bm_mlp* m, const int32_t* row_order, int32_t nrows,
                             const bm_learned_params* params, bm_progress* prog, bm_learned_stats* stats);
 
