@@ -754,7 +754,7 @@ def sa_chains(device, steps, candidates=0):
     dt = time.perf_counter() - t0
     out = {"chains": 64, "pairs": 16, "n_range": [min(ns), max(ns)], "steps_per_chain": steps,
            "proposals_per_s": 64 * steps / dt, "seconds": dt, "candidates_per_iteration": int(st.candidates),
-           "ctas_per_chain": int(st.ctas_per_chain),
+           "ctas_per_chain": int(st.ctas_per_chain), "threads_per_cta": int(st.threads_per_cta),
            "launches": int(st.launches), "accepts_mean": float(np.mean(acc)), "generation_s": t_gen,
            "timing": "host call: graph replay, transfers and final scores included"}
     batch.close()

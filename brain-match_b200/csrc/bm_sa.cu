@@ -80,19 +80,23 @@ struct SaArgs {
     double log_ratio;
 };
 
-constexpr int kSaThreads = 512;
+constexpr int kSaThreads = 512;     // threads per CTA of the allocation-free entry point (bm_sa_run tunes 256 or 512)
 constexpr int kSaMaxK = 64;         // proposals per iteration, adaptive up to this
 constexpr int kSaMaxInitialK = 16;  // largest settable starting K
 constexpr int kSaItem = 128;        // list entries per work item (four per lane)
 constexpr int kSaRowCap = 512;      // B row entries a warp stages in shared memory (longer rows: hash)
 constexpr int kSaUnitTable = 4096;  // items per iteration with an item -> list table (else binary search)
 
-// Dynamic shared memory of the chain kernel: the warps' B-row buffers, then
-// the chain's mapping when it fits.
-constexpr size_t kSaRowBytes = sizeof(uint32_t) * kSaRowCap * 2 * (kSaThreads / 32);  // two buffers per warp
-static_assert(kSaRowBytes >= sizeof(uint32_t) * 4 * 4096, "the swap apply stages four rows in the row buffers");
-
 constexpr int kSaApplyRowCap = 4096;  // entries per staged row in the swap apply (4 rows)
+
+// Dynamic shared memory of the chain kernel: the warps' B-row buffers (two
+// per warp), which the swap apply reuses for its four staged rows (at least
+// 64 KB), then the chain's mapping when it fits.
+__host__ __device__ constexpr size_t sa_dyn_base(int threads) {
+    return sizeof(uint32_t) * kSaRowCap * 2 * (size_t)(threads / 32) > sizeof(uint32_t) * 4 * kSaApplyRowCap
+               ? sizeof(uint32_t) * kSaRowCap * 2 * (size_t)(threads / 32)
+               : sizeof(uint32_t) * 4 * kSaApplyRowCap;
+}
 
 // Apply the swap pi(a) <-> pi(b) of one chain with the whole CTA: S updates of
 // every A entry incident to a or b (as apply_kernel in bm_apply.cu), then pi.
@@ -199,7 +203,7 @@ __device__ void chain_apply_block(const PairDev& P, int32_t* pi, int32_t* gpi, i
 // to the acceptance rate: it doubles (up to kSaMaxK) after an iteration with
 // no acceptance and drops to max(a.K, 2 (j + 1)) after the j-th proposal is
 // accepted; a function of the chain's own history, so replays are exact.
-template <int CL>
+template <int CL, int THREADS>
 __device__ __forceinline__ void sa_chain_body(const SaArgs& a) {
     extern __shared__ __align__(16) uint32_t s_dyn[];
     // CL CTAs (a cluster) run one chain: they draw the same proposals, split
@@ -209,7 +213,7 @@ __device__ __forceinline__ void sa_chain_body(const SaArgs& a) {
     const int crank = CL > 1 ? (int)cg::this_cluster().block_rank() : 0;
     if (c >= a.nchains) return;
     constexpr int kSeg = 4 * kSaMaxK;
-    constexpr int kW = kSaThreads / 32;
+    constexpr int kW = THREADS / 32;
     __shared__ bm_proposal s_prop[kSaMaxK];
     __shared__ int32_t s_sum[kSaMaxK];
     __shared__ long long s_d[kSaMaxK];
@@ -226,7 +230,7 @@ __device__ __forceinline__ void sa_chain_body(const SaArgs& a) {
     int32_t* pi = gpi;
     uint32_t* rowbuf = s_dyn + (size_t)warp * 2 * kSaRowCap;  // this warp's two B-row buffers
     if (a.pi_smem) {
-        int32_t* s_pi = reinterpret_cast<int32_t*>(s_dyn + (size_t)kSaRowCap * 2 * kW);
+        int32_t* s_pi = reinterpret_cast<int32_t*>(s_dyn + sa_dyn_base(THREADS) / sizeof(uint32_t));
         for (int32_t i = tid; i <= P.n; i += blockDim.x) s_pi[i] = gpi[i];
         pi = s_pi;
     }
@@ -440,12 +444,14 @@ __device__ __forceinline__ void sa_chain_body(const SaArgs& a) {
     }
 }
 
-__global__ void __launch_bounds__(kSaThreads, 1) sa_chain_kernel(SaArgs a) { sa_chain_body<1>(a); }
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) sa_chain_kernel(SaArgs a) { sa_chain_body<1, THREADS>(a); }
 
 // One chain per pair of CTAs (a cluster of two on two SMs), for batches with
 // fewer chains than half the SMs.
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSaThreads, 1) sa_chain_kernel_pair(SaArgs a) {
-    sa_chain_body<2>(a);
+template <int THREADS>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1) sa_chain_kernel_pair(SaArgs a) {
+    sa_chain_body<2, THREADS>(a);
 }
 
 // Initial S(v) and score of every chain: a warp per (chain, A vertex).
@@ -613,25 +619,39 @@ namespace {
 // chain's mapping when it fits (the largest n + 1 ints of the launch), else
 // the mapping stays in global memory.  Sets the kernel's dynamic
 // shared-memory limit; called before any stream capture.
-bm_status chain_smem(bm_ctx* ctx, SaArgs& args, int32_t n_max, size_t* smem) {
+bm_status chain_smem(bm_ctx* ctx, SaArgs& args, int32_t n_max, int32_t threads, size_t* smem) {
     const size_t need = sizeof(int32_t) * ((size_t)n_max + 1);
-    *smem = kSaRowBytes;
+    const size_t base = sa_dyn_base(threads);
+    *smem = base;
     args.pi_smem = 0;
-    if (kSaRowBytes + need + 16384 <= ctx->smem_optin) {
+    if (base + need + 16384 <= ctx->smem_optin) {
         args.pi_smem = 1;
         *smem += need;
     }
-    BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
-    BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+    if (threads == 256) {
+        BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+        BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel_pair<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+    } else {
+        BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+        BM_CUDA(ctx, cudaFuncSetAttribute(sa_chain_kernel_pair<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+    }
     return BM_OK;
 }
 
-// One launch of the chains: a CTA per chain, or a pair of CTAs per chain.
-void launch_chains(const SaArgs& args, int32_t ctas_per_chain, size_t smem, cudaStream_t stream) {
-    if (ctas_per_chain == 2)
-        sa_chain_kernel_pair<<<args.nchains * 2, kSaThreads, smem, stream>>>(args);
-    else
-        sa_chain_kernel<<<args.nchains, kSaThreads, smem, stream>>>(args);
+// One launch of the chains: a CTA per chain, or a pair of CTAs per chain, of
+// 256 or 512 threads.
+void launch_chains(const SaArgs& args, int32_t ctas_per_chain, int32_t threads, size_t smem, cudaStream_t stream) {
+    if (threads == 256) {
+        if (ctas_per_chain == 2)
+            sa_chain_kernel_pair<256><<<args.nchains * 2, 256, smem, stream>>>(args);
+        else
+            sa_chain_kernel<256><<<args.nchains, 256, smem, stream>>>(args);
+    } else {
+        if (ctas_per_chain == 2)
+            sa_chain_kernel_pair<512><<<args.nchains * 2, 512, smem, stream>>>(args);
+        else
+            sa_chain_kernel<512><<<args.nchains, 512, smem, stream>>>(args);
+    }
 }
 
 }  // namespace
@@ -645,6 +665,8 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
         return bm_fail(ctx, BM_INVALID_ARG, "need steps >= 0 and positive temperatures");
     if (prm->candidates < 0 || prm->candidates > 16)
         return bm_fail(ctx, BM_INVALID_ARG, "candidates must be 0 (tuned) or 1..16");
+    if (prm->threads_per_cta != 0 && prm->threads_per_cta != 256 && prm->threads_per_cta != 512)
+        return bm_fail(ctx, BM_INVALID_ARG, "threads_per_cta must be 0, 256 or 512");
     BM_CUDA(ctx, cudaSetDevice(ctx->device));
     const int32_t np = (int32_t)b->pairs.size();
     // chain layout and validation
@@ -714,14 +736,10 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
     if (K > kmax) return bm_fail(ctx, BM_INVALID_ARG, "candidates %d above this build's limit %d", K, kmax);
     int32_t n_max = 0;
     for (int32_t c = 0; c < nchains; c++) n_max = std::max(n_max, b->pairs[(size_t)chain_pair[c]].n);
-    size_t smem = 0;
-    {
-        bm_status st = chain_smem(ctx, args, n_max, &smem);
-        if (st != BM_OK) return st;
-    }
     // CTAs per chain: a pair when the chains fill at most half the SMs (the
-    // tuner may keep one); a fixed K keeps the pair rule
+    // tuner may keep one); a fixed K keeps the pair rule and 512 threads
     int32_t CLc = (2 * nchains <= ctx->num_sms) ? 2 : 1;
+    int32_t TH = prm->threads_per_cta ? prm->threads_per_cta : 512;
     if (K == 0) {
         int64_t ntot = 0;
         for (int32_t c = 0; c < nchains; c++) ntot += b->pairs[(size_t)chain_pair[c]].n;
@@ -731,26 +749,33 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
         int32_t tuned = 0;
         if (tune_lookup(key, &tuned)) {
             K = tuned & 0xFF;
-            CLc = (tuned >> 8) == 2 ? 2 : 1;
+            CLc = ((tuned >> 8) & 0xF) == 2 ? 2 : 1;
+            TH = ((tuned >> 12) & 1) ? 256 : 512;
             if (CLc == 2 && 2 * nchains > ctx->num_sms) CLc = 1;
             if (K < 1 || K > kmax) K = 8;
         } else {
             // time a short prefix of the real run for each (K, CTAs per
-            // chain) and keep the fastest; the chain depends on neither, so
-            // the prefix is simply replayed by the real run below
+            // chain, threads per CTA) and keep the fastest; the chain depends
+            // on none of them, so the prefix is simply replayed by the real
+            // run below
             float best_ms = 1e30f;
-            int32_t best_k = 8, best_cl = 1;
+            int32_t best_k = 8, best_cl = 1, best_th = 512;
             std::vector<ChainDev> snap = hc;
             const int32_t max_cl = (2 * nchains <= ctx->num_sms) ? 2 : 1;
-            for (int32_t trial = 0; trial < 5 * max_cl; trial++) {
-                const int32_t cand = 1 << (trial % 5), cl = 1 + trial / 5;
+            for (int32_t trial = 0; trial < 10 * max_cl; trial++) {
+                const int32_t cand = 1 << (trial % 5), cl = 1 + trial / 10, th = ((trial / 5) & 1) ? 256 : 512;
                 if (cand > kmax) continue;
+                SaArgs t = args;
+                size_t tsmem = 0;
+                {
+                    bm_status st = chain_smem(ctx, t, n_max, th, &tsmem);
+                    if (st != BM_OK) return st;
+                }
                 BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
                 BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
                 BM_CUDA(ctx, cudaMemcpyAsync(d_ch, snap.data(), sizeof(ChainDev) * (size_t)nchains, cudaMemcpyHostToDevice, ctx->stream));
                 sa_init_kernel<<<dim3(64, (unsigned)nchains), 256, 0, ctx->stream>>>(b->d_pairs, d_ch, nchains);
                 BM_LAUNCH_CHECK(ctx, "sa_init_kernel");
-                SaArgs t = args;
                 t.K = cand;
                 t.chunk = std::min<uint64_t>(4096, args.steps > 0 ? args.steps : 1);
                 struct Events {
@@ -760,17 +785,18 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
                 BM_CUDA(ctx, cudaEventCreate(&ev.a));
                 BM_CUDA(ctx, cudaEventCreate(&ev.b));
                 BM_CUDA(ctx, cudaEventRecord(ev.a, ctx->stream));
-                launch_chains(t, cl, smem, ctx->stream);
+                launch_chains(t, cl, th, tsmem, ctx->stream);
                 BM_LAUNCH_CHECK(ctx, "sa_chain_kernel(tune)");
                 BM_CUDA(ctx, cudaEventRecord(ev.b, ctx->stream));
                 BM_CUDA(ctx, cudaEventSynchronize(ev.b));
                 float ms = 0;
                 cudaEventElapsedTime(&ms, ev.a, ev.b);
-                if (ms < best_ms) { best_ms = ms; best_k = cand; best_cl = cl; }
+                if (ms < best_ms) { best_ms = ms; best_k = cand; best_cl = cl; best_th = th; }
             }
             K = best_k;
             CLc = best_cl;
-            tune_store(key, K | (CLc << 8));
+            TH = best_th;
+            tune_store(key, K | (CLc << 8) | ((TH == 256 ? 1 : 0) << 12));
             // restart from the initial state
             BM_CUDA(ctx, cudaMemcpyAsync(d_pi, init_pi, sizeof(int32_t) * (size_t)tot, cudaMemcpyHostToDevice, ctx->stream));
             BM_CUDA(ctx, cudaMemsetAsync(d_ov, 0, sizeof(int32_t) * (size_t)tot, ctx->stream));
@@ -778,6 +804,11 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
             sa_init_kernel<<<dim3(64, (unsigned)nchains), 256, 0, ctx->stream>>>(b->d_pairs, d_ch, nchains);
             BM_LAUNCH_CHECK(ctx, "sa_init_kernel");
         }
+    }
+    size_t smem = 0;
+    {
+        bm_status st = chain_smem(ctx, args, n_max, TH, &smem);
+        if (st != BM_OK) return st;
     }
     // capture one chunk launch in a graph and replay it
     const uint64_t launches = args.steps == 0 ? 0 : (args.steps + args.chunk - 1) / args.chunk;
@@ -787,7 +818,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
         cudaGraphExec_t exec = nullptr;
         args.K = K;
         BM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        launch_chains(args, CLc, smem, ctx->stream);
+        launch_chains(args, CLc, TH, smem, ctx->stream);
         cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
         if (ce != cudaSuccess) return bm_cuda_fail(ctx, ce, "cudaStreamEndCapture");
         ce = cudaGraphInstantiate(&exec, graph, 0);
@@ -813,6 +844,7 @@ extern "C" bm_status bm_sa_run(bm_batch* b, int32_t nchains, const int32_t* chai
     if (stats) {
         stats->candidates = K;
         stats->ctas_per_chain = CLc;
+        stats->threads_per_cta = TH;
         stats->launches = (int64_t)launches;
         stats->seconds = secs;
     }
@@ -878,8 +910,8 @@ bm_status bm_noalloc_setup(bm_ctx* ctx) {
     // entry point's two kernels here, so its first call loads nothing
     cudaFuncAttributes fa;
     BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_init_kernel));
-    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel));
-    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel_pair));  // its smem limit is set by every chain call
+    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel<kSaThreads>));
+    BM_CUDA(ctx, cudaFuncGetAttributes(&fa, sa_chain_kernel_pair<kSaThreads>));  // its smem limit is set by every chain call
     return BM_OK;
 }
 
@@ -975,10 +1007,10 @@ extern "C" bm_status bm_sa_run_noalloc(bm_batch* b, int32_t nchains, const int32
     args.chunk = prm->chunk > 0 ? (uint64_t)prm->chunk : (uint64_t)65536;
     args.K = K;
     size_t smem = 0;
-    if ((st = chain_smem(ctx, args, n_max, &smem)) != BM_OK) return st;
+    if ((st = chain_smem(ctx, args, n_max, kSaThreads, &smem)) != BM_OK) return st;
     const uint64_t launches = args.steps == 0 ? 0 : (args.steps + args.chunk - 1) / args.chunk;
     for (uint64_t l = 0; l < launches; l++) {
-        sa_chain_kernel<<<nchains, kSaThreads, smem, ctx->stream>>>(args);
+        sa_chain_kernel<kSaThreads><<<nchains, kSaThreads, smem, ctx->stream>>>(args);
         BM_LAUNCH_CHECK(ctx, "sa_chain_kernel");
     }
     if (final_pi)

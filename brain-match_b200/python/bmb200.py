@@ -60,12 +60,12 @@ class Progress(C.Structure):
 
 class SaParams(C.Structure):
     _fields_ = [("steps", C.c_int64), ("t0", C.c_double), ("t_end", C.c_double), ("candidates", C.c_int32),
-                ("chunk", C.c_int64)]
+                ("chunk", C.c_int64), ("threads_per_cta", C.c_int32)]
 
 
 class SaStats(C.Structure):
     _fields_ = [("candidates", C.c_int32), ("ctas_per_chain", C.c_int32), ("launches", C.c_int64),
-                ("seconds", C.c_double)]
+                ("seconds", C.c_double), ("threads_per_cta", C.c_int32)]
 
 
 class LearnedParams(C.Structure):
@@ -892,7 +892,7 @@ class Batch:
         self.ns.append(n)
         return idx.value
 
-    def sa_run(self, chain_pair, keys, init_pis, steps, t0=5.0, t_end=0.01, candidates=0, chunk=0):
+    def sa_run(self, chain_pair, keys, init_pis, steps, t0=5.0, t_end=0.01, candidates=0, chunk=0, threads=0):
         """Run chains; init_pis is a list of n+1 arrays.  Returns (final_pis,
         scores, accepts, stats)."""
         cp = _i32(chain_pair)
@@ -902,7 +902,7 @@ class Batch:
         nch = cp.shape[0]
         scores = np.zeros(nch, np.int64)
         acc = np.zeros(nch, np.int64)
-        prm = SaParams(steps, t0, t_end, candidates, chunk)
+        prm = SaParams(steps, t0, t_end, candidates, chunk, threads)
         st = SaStats()
         self.eng._chk(self.L.bm_sa_run(self.h, nch, _ptr(cp), _ptr(k), _ptr(flat), C.byref(prm), _ptr(out),
                                        _ptr(scores), _ptr(acc), C.byref(st)), "bm_sa_run")

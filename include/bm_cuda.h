@@ -284,6 +284,8 @@ typedef struct bm_sa_params {
                           * to 64) to its own acceptances: doubled after an iteration with none,
                           * 2 (j + 1) after the j-th is accepted. */
     int64_t chunk;       /* proposals per chain per kernel launch (0 = 65536) */
+    int32_t threads_per_cta; /* 256 or 512 with a set candidates value; 0 = 512 there, and with
+                              * candidates = 0 the tuner chooses it as well (256 or 512) */
 } bm_sa_params;
 
 typedef struct bm_sa_stats {
@@ -291,6 +293,7 @@ typedef struct bm_sa_stats {
     int32_t ctas_per_chain;  /* 1, or 2: a pair of CTAs (a cluster) per chain */
     int64_t launches;        /* graph replays */
     double seconds;      /* wall time of the chain launches */
+    int32_t threads_per_cta; /* 256 or 512 */
 } bm_sa_stats;
 
 /* Simulated annealing, the loop of simulated_annealing in

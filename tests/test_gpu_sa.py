@@ -20,8 +20,8 @@ def pairs():
     return out
 
 
-@pytest.mark.parametrize("candidates", [1, 4, 16])
-def test_chains_replay_on_cpu(pairs, candidates):
+@pytest.mark.parametrize("candidates,threads", [(1, 0), (4, 0), (16, 0), (1, 256), (4, 256), (16, 256)])
+def test_chains_replay_on_cpu(pairs, candidates, threads):
     eng = bm.Engine(0)
     batch = bm.Batch(eng)
     for A, B, _ in pairs:
@@ -31,9 +31,10 @@ def test_chains_replay_on_cpu(pairs, candidates):
     inits = [pairs[p][2] for p in chain_pair]
     steps = 6000
     pis, scores, acc, st = batch.sa_run(chain_pair, keys, inits, steps, t0=5.0, t_end=0.01,
-                                        candidates=candidates, chunk=1000)
+                                        candidates=candidates, chunk=1000, threads=threads)
     assert st.candidates == candidates and st.launches == 6
     assert st.ctas_per_chain == 2  # 5 chains fill at most half the SMs: a pair of CTAs per chain
+    assert st.threads_per_cta == (threads or 512)
     for c, p in enumerate(chain_pair):
         A, B, init = pairs[p]
         orc = Oracle(A.n, (A.src, A.dst, A.w), (B.src, B.dst, B.w))
