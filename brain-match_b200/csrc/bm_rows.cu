@@ -1100,8 +1100,9 @@ bool split_would_apply(const bm_ctx* ctx, int32_t nrows) {
 constexpr int32_t kRowGraphMaxRows = 4096;
 
 // bm_rows_best without column bounds as a replayed CUDA graph: the rows are
-// copied (CPU) into pinned staging, the graph copies them in, runs the row
-// launches (tiers included) and copies the results out to pinned staging,
+// copied (CPU) into pinned staging, the graph copies them in and runs the row
+// launches (tiers included), which write the row results straight into pinned
+// staging (zero copy: 32 bytes a row over the host link, no copy-out step),
 // from which they are copied (CPU) to the caller.  The first call of a row
 // count runs plainly and then captures the graph; a change of row count,
 // staging buffers, graphs, semantics or row settings captures it again.
@@ -1142,16 +1143,15 @@ bm_status rows_best_graph(bm_ctx* ctx, const int32_t* rows, int32_t nrows, bm_ro
     cudaGraph_t graph = nullptr;
     BM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     const cudaError_t c1 = cudaMemcpyAsync(d_rows, h_in, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream);
-    const bm_status ls = c1 == cudaSuccess ? bm_launch_rows(ctx, d_rows, nullptr, nrows, nullptr, d_out, nullptr) : BM_OK;
-    const cudaError_t c2 = cudaMemcpyAsync(h_out, d_out, ob, cudaMemcpyDeviceToHost, ctx->stream);
+    const bm_status ls = c1 == cudaSuccess ? bm_launch_rows(ctx, d_rows, nullptr, nrows, nullptr, h_out, nullptr) : BM_OK;
     const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
     const int64_t captured = ctx->launches - l0;
     ctx->launches = l0;
-    if (ls != BM_OK || c1 != cudaSuccess || c2 != cudaSuccess || ce != cudaSuccess) {
+    if (ls != BM_OK || c1 != cudaSuccess || ce != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
         if (ls != BM_OK) return ls;
-        return bm_cuda_fail(ctx, c1 != cudaSuccess ? c1 : c2 != cudaSuccess ? c2 : ce, "row graph capture");
+        return bm_cuda_fail(ctx, c1 != cudaSuccess ? c1 : ce, "row graph capture");
     }
     const cudaError_t ie = cudaGraphInstantiate(&G.exec, graph, 0);
     cudaGraphDestroy(graph);
