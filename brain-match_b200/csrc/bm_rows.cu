@@ -721,13 +721,18 @@ bm_status launch_rows_t(bm_ctx* ctx, const RowArgs& args, int cl, size_t smem, c
     cfg.blockDim = dim3(THREADS, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
+    // clusters placed for load balance rather than spread: with the two
+    // cluster sizes of a tiered launch resident together, spreading left
+    // clusters for a second wave well below the resident-cluster count
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)cl;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeClusterSchedulingPolicyPreference;
+    attr[1].val.clusterSchedulingPolicyPreference = cudaClusterSchedulingPolicyLoadBalancing;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     BM_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, args));
     BM_LAUNCH_CHECK(ctx, "rows_kernel");
     return BM_OK;
@@ -848,26 +853,35 @@ int32_t host_split_plan(const bm_ctx* ctx, const int32_t* h_rows, int32_t nrows,
     return (int32_t)out.size();
 }
 
-// Rows of a launch of nrows rows in cl-CTA clusters that go to the 2 cl tier:
-// the most that keep both launches within kTierFill of the resident CTA
-// slots (measured at 57 rows in 4-CTA clusters: 6 rows in 8-CTA clusters
-// +8 %, 8 rows put clusters in a second wave), capped by the caller's
-// setting.
-constexpr double kTierFill = 0.85;
-
-int32_t tier_rows(bm_ctx* ctx, int32_t nrows, int cl, size_t smem, bm_status* st) {
-    *st = BM_OK;
-    int& cap = ctx->split_active[(ctx->row_threads == 256 ? 0 : 1) * (kMaxCluster + 1) + 1];
-    if (cap == 0) {
-        *st = (ctx->row_threads == 256) ? max_clusters_t<256>(ctx, 1, smem, &cap) : max_clusters_t<512>(ctx, 1, smem, &cap);
-        if (*st != BM_OK) return 0;
-        if (cap <= 0) cap = -1;
+// Resident clusters of cl CTAs for the current n (occupancy query, cached
+// per thread count and cluster size).
+bm_status resident_clusters(bm_ctx* ctx, int cl, size_t smem, int* out) {
+    int& v = ctx->split_active[(ctx->row_threads == 256 ? 0 : 1) * (kMaxCluster + 1) + cl];
+    if (v == 0) {
+        const bm_status st = (ctx->row_threads == 256) ? max_clusters_t<256>(ctx, cl, smem, &v)
+                                                      : max_clusters_t<512>(ctx, cl, smem, &v);
+        if (st != BM_OK) return st;
+        if (v <= 0) v = -1;
     }
-    if (cap <= 0) return 0;
-    const int64_t budget = (int64_t)(kTierFill * cap) - (int64_t)nrows * cl;
-    int64_t h = budget > 0 ? std::min<int64_t>(nrows, budget / cl) : 0;
+    *out = v;
+    return BM_OK;
+}
+
+// Rows of a launch of nrows rows in cl-CTA clusters that go to the 2 cl tier.
+// A 2 cl cluster takes the room of two cl clusters in a GPC, so the H rows
+// and the other nrows - H fit at once while nrows + H stays below the
+// resident cl clusters (one cluster of margin) and H within the resident
+// 2 cl clusters; capped by the caller's setting.  Measured at 57 rows in 4-CTA
+// clusters (71 resident, so H = 13): H = 6 +8 %, H = 13-15 +12 % over one
+// launch; H = 17 puts clusters in a second wave.
+int32_t tier_rows(bm_ctx* ctx, int32_t nrows, int cl, size_t smem, bm_status* st) {
+    int m1 = 0, m2 = 0;
+    if ((*st = resident_clusters(ctx, cl, smem, &m1)) != BM_OK) return 0;
+    if ((*st = resident_clusters(ctx, 2 * cl, smem, &m2)) != BM_OK) return 0;
+    if (m1 <= 0 || m2 <= 0) return 0;
+    int64_t h = std::min<int64_t>({(int64_t)nrows, (int64_t)m1 - nrows - 1, (int64_t)m2});
     if (ctx->row_tiers > 0) h = std::min<int64_t>(h, ctx->row_tiers);
-    return (int32_t)h;
+    return (int32_t)std::max<int64_t>(h, 0);
 }
 
 }  // namespace
@@ -994,10 +1008,9 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
     // the largest work estimate (ranked on the device) get clusters of 2 cl
     // in a launch on a second stream, concurrent with the cl-CTA launch of
     // the others.  A launch waits on its heaviest row, and a row's scatter
-    // rate grows with its CTAs.  The two launches together stay within
-    // kTierFill of the resident CTA slots: mixed cluster sizes fragment the
-    // GPCs, and a cluster left for a second wave costs more than the tier
-    // saves.
+    // rate grows with its CTAs.  The two launches together must stay
+    // resident (tier_rows): a cluster left for a second wave costs more than
+    // the tier saves.
     const int32_t H = (args.slots || ctx->row_ctas != 0 || ctx->row_tiers < 0 || cl >= kMaxCluster || !ctx->rwork ||
                        nrows > kItemChunk)
                           ? 0 : tier_rows(ctx, nrows, cl, smem, &st);

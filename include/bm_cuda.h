@@ -655,8 +655,8 @@ bm_status bm_get_row_split(bm_ctx* ctx, int32_t* slots);
  * clusters, in a second launch on the context's second stream concurrent with
  * the first; the calling stream waits for both.  Results are identical
  * either way.  heavy_rows: 0 = automatic (default: as many rows as keep both
- * launches within 85 % of the resident CTA slots), -1 = off, k > 0 = at most
- * k rows.  Not used when the CTAs per row are set (bm_set_row_tiling) or a
+ * launches resident together, by the device's resident-cluster counts for
+ * the two cluster sizes), -1 = off, k > 0 = at most k rows.  Not used when the CTAs per row are set (bm_set_row_tiling) or a
  * split plan is active.  No reference counterpart. */
 bm_status bm_set_row_tiers(bm_ctx* ctx, int32_t heavy_rows);
 bm_status bm_get_row_tiers(bm_ctx* ctx, int32_t* heavy_rows);

@@ -13,9 +13,9 @@ from oracle_bind import Oracle
 
 pytestmark = pytest.mark.gpu
 
-# batch sizes: 1 and 20 (8-CTA clusters, no wider tier), 40 and 57 (4-CTA
-# clusters with 8-CTA tiers), 70 (4-CTA clusters filling the slots: no tier),
-# 100 (2-CTA clusters with 4-CTA tiers), 140 (no tier)
+# batch sizes: 1 and 20 (8-CTA clusters, no wider tier), 40, 57 and 70
+# (4-CTA clusters, 8-CTA tiers while the resident clusters allow), 100 and 140
+# (2-CTA clusters with 4-CTA tiers)
 SIZES = (1, 20, 40, 57, 70, 100, 140)
 
 
@@ -41,6 +41,26 @@ def _rows(n, A, k, seed):
     if k > 2:
         rows[-1] = rows[0]
     return rows
+
+
+def _tier_rows(e, k):
+    """Rows in the wider tier for a launch of k rows, by the library's rule:
+    the cluster size c is the largest power of two up to 8 with k c <= SMs;
+    below 8, H = min(k, resident c clusters - k - 1, resident 2c clusters)."""
+    import ctypes as C
+    v = C.c_int32()
+    e.L.bm_rows_max_active_clusters(e.h, 1, 512, C.byref(v))
+    sms = v.value // 2  # two CTAs per SM
+    c = 1
+    while c < 8 and k * c <= sms:
+        c *= 2
+    if c >= 8:
+        return 0
+    e.L.bm_rows_max_active_clusters(e.h, c, 512, C.byref(v))
+    m1 = v.value
+    e.L.bm_rows_max_active_clusters(e.h, 2 * c, 512, C.byref(v))
+    m2 = v.value
+    return max(0, min(k, m1 - k - 1, m2))
 
 
 def _dev_best(e, rows):
@@ -80,11 +100,7 @@ def test_tiers_equal_single_launch_and_oracle(golden_cfg1, cfg1, k):
             np.testing.assert_array_equal(e.rows_best(rows, col), base_col)
             got, launches = _dev_best(e, rows)
             np.testing.assert_array_equal(got, base_best)
-            assert launches in (1, 2)
-            if k in (40, 57, 100):
-                assert launches == 2, (k, tiers)
-            if k in (1, 20, 70, 140):
-                assert launches == 1, (k, tiers)
+            assert launches == (2 if _tier_rows(e, k) > 0 else 1), (k, tiers)
     finally:
         e.set_row_tiers(0)
 
