@@ -253,8 +253,18 @@ extern "C" bm_status bm_set_graph(bm_ctx* ctx, int side, int32_t n, int64_t m, c
     G.m_real = H.m_real;
     BM_TRY(upload(ctx, &G.out_ptr, H.optr.data(), H.optr.size()));
     BM_TRY(upload(ctx, &G.in_ptr, H.iptr.data(), H.iptr.size()));
-    BM_TRY(upload(ctx, &G.out_ent, H.oent.data(), H.oent.size()));
-    BM_TRY(upload(ctx, &G.in_ent, H.ient.data(), H.ient.size()));
+    if (side == BM_SIDE_A) {
+        // A's device lists in bank-spread order (the row kernel's scatter);
+        // the host copy below keeps them sorted by neighbour id
+        std::vector<uint32_t> oe = H.oent, ie = H.ient;
+        bm_bank_spread_lists(H.optr, oe);
+        bm_bank_spread_lists(H.iptr, ie);
+        BM_TRY(upload(ctx, &G.out_ent, oe.data(), oe.size()));
+        BM_TRY(upload(ctx, &G.in_ent, ie.data(), ie.size()));
+    } else {
+        BM_TRY(upload(ctx, &G.out_ent, H.oent.data(), H.oent.size()));
+        BM_TRY(upload(ctx, &G.in_ent, H.ient.data(), H.ient.size()));
+    }
     BM_TRY(upload(ctx, &G.self_w, H.self.data(), H.self.size()));
     if (side == BM_SIDE_B) {
         BM_TRY(upload(ctx, &G.out_twin, H.otw.data(), H.otw.size()));

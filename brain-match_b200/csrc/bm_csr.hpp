@@ -202,3 +202,32 @@ inline int bm_build_host_csr(bool side_b, int32_t n, int64_t m, const int32_t* s
     }
     return 0;
 }
+
+// Reorders the real entries of every list (the padding stays at the end) so
+// that the row kernel's shared-memory scatter meets fewer bank conflicts.  A
+// warp's lanes take consecutive 4-entry quads of a list, and its c-th atomic
+// instruction adds at entry c of each lane's quad, at accumulator word id
+// (bank id mod 32).  Position p of a list is given, where the list has one,
+// an entry of bank ((p >> 2) + 8 (p & 3)) mod 32, else the next bank up that
+// still has entries: entry c of 32 consecutive quads then lands in 32
+// different banks when the list's banks are balanced.  Sums over the lists do
+// not depend on the order; nothing may rely on these lists being sorted.
+inline void bm_bank_spread_lists(const std::vector<int32_t>& ptr, std::vector<uint32_t>& ent) {
+    std::vector<uint32_t> bucket[32];
+    for (size_t v = 0; v + 1 < ptr.size(); v++) {
+        const int32_t lo = ptr[v], hi = ptr[v + 1];
+        int32_t cnt = 0;
+        for (int b = 0; b < 32; b++) bucket[b].clear();
+        for (int32_t j = lo; j < hi; j++) {
+            const uint32_t e = ent[(size_t)j];
+            if (e) { bucket[bm_eid(e) & 31].push_back(e); cnt++; }
+        }
+        if (cnt < 2) continue;
+        size_t head[32] = {0};
+        for (int32_t p = 0; p < cnt; p++) {
+            int b = ((p >> 2) + 8 * (p & 3)) & 31;
+            while (head[b] >= bucket[b].size()) b = (b + 1) & 31;
+            ent[(size_t)lo + p] = bucket[b][head[b]++];
+        }
+    }
+}

@@ -8,6 +8,10 @@
 //                               null entries (0), so every list is 16-byte aligned
 //   self_w[n+1]                 self-loop weight (0 if none); self-loops are kept
 //                               out of the lists and scored separately
+// Graph A's device lists hold their entries in bank-spread order
+// (bm_bank_spread_lists: fewer shared-memory bank conflicts in the row
+// kernel's scatter), not sorted; every kernel only sums over them.  The host
+// copy of A (ctx->hA_*) keeps them sorted by neighbour id.
 // Graph B additionally holds
 //   out_twin, in_twin           index of the same edge in the other direction
 //   out_ent0, in_ent0           the entries with B ids (immutable)

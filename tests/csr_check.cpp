@@ -34,6 +34,8 @@ static int32_t hash_get(const HostCsr& G, int32_t g, int32_t h) {
     return 0;
 }
 
+static void check_bank_spread(const HostCsr& G);
+
 static void check_graph(bool side_b, int32_t n, const std::vector<int32_t>& s, const std::vector<int32_t>& d,
                         const std::vector<int32_t>& w) {
     HostCsr G;
@@ -106,6 +108,7 @@ static void check_graph(bool side_b, int32_t n, const std::vector<int32_t>& s, c
         if (side_b) CHECK(hash_get(G, kv.first.first, kv.first.second) == kv.second[0]);
     }
     CHECK(got_o.size() == exp.size() && got_i.size() == exp.size());
+    check_bank_spread(G);
     for (int v = 1; v <= n; v++) CHECK(G.self[v] == self[v]);
     if (side_b)
         for (int t = 0; t < 2000; t++) {
@@ -116,7 +119,49 @@ static void check_graph(bool side_b, int32_t n, const std::vector<int32_t>& s, c
         }
 }
 
+// bm_bank_spread_lists permutes the real entries inside each list and keeps
+// the padding last; on a list with balanced banks, entry c of any 32
+// consecutive quads falls in 32 different banks.
+static void check_bank_spread(const HostCsr& G) {
+    std::vector<uint32_t> oe = G.oent, ie = G.ient;
+    bm_bank_spread_lists(G.optr, oe);
+    bm_bank_spread_lists(G.iptr, ie);
+    for (int pass = 0; pass < 2; pass++) {
+        const std::vector<int32_t>& ptr = pass ? G.iptr : G.optr;
+        const std::vector<uint32_t>& before = pass ? G.ient : G.oent;
+        const std::vector<uint32_t>& after = pass ? ie : oe;
+        CHECK(after.size() == before.size());
+        for (size_t v = 0; v + 1 < ptr.size(); v++) {
+            std::vector<uint32_t> a(before.begin() + ptr[v], before.begin() + ptr[v + 1]);
+            std::vector<uint32_t> b(after.begin() + ptr[v], after.begin() + ptr[v + 1]);
+            bool pad = false;
+            for (uint32_t e : b) {
+                if (e == 0) pad = true;
+                else CHECK(!pad);
+            }
+            std::sort(a.begin(), a.end());
+            std::sort(b.begin(), b.end());
+            CHECK(a == b);
+        }
+    }
+}
+
+static void check_bank_spread_balanced() {
+    // one list of 256 entries, eight per bank, given in id order
+    std::vector<int32_t> ptr = {0, 0, 256};
+    std::vector<uint32_t> ent;
+    for (uint32_t i = 1; i <= 256; i++) ent.push_back(bm_pack(i, 1));
+    bm_bank_spread_lists(ptr, ent);
+    for (int q0 = 0; q0 + 32 <= 64; q0++)
+        for (int c = 0; c < 4; c++) {
+            unsigned seen = 0;
+            for (int k = 0; k < 32; k++) seen |= 1u << (bm_eid(ent[(size_t)(4 * (q0 + k) + c)]) & 31);
+            CHECK(seen == 0xFFFFFFFFu);
+        }
+}
+
 int main() {
+    check_bank_spread_balanced();
     std::mt19937 rng(12345);
     for (int trial = 0; trial < 300; trial++) {
         const int n = 1 + (int)(rng() % 60) + (trial % 10 == 0 ? 2000 : 0);
