@@ -95,6 +95,8 @@ static void free_graph(DevGraph& g) {
     bm_cuda_free(g.self_w);
     bm_cuda_free(g.out_twin); bm_cuda_free(g.in_twin);
     bm_cuda_free(g.out_ent0); bm_cuda_free(g.in_ent0);
+    bm_cuda_free(g.out_twin0); bm_cuda_free(g.in_twin0);
+    bm_cuda_free(g.out_pos); bm_cuda_free(g.in_pos);
     bm_cuda_free(g.hash);
     g = DevGraph();
 }
@@ -269,6 +271,10 @@ extern "C" bm_status bm_set_graph(bm_ctx* ctx, int side, int32_t n, int64_t m, c
     if (side == BM_SIDE_B) {
         BM_TRY(upload(ctx, &G.out_twin, H.otw.data(), H.otw.size()));
         BM_TRY(upload(ctx, &G.in_twin, H.itw.data(), H.itw.size()));
+        BM_TRY(upload(ctx, &G.out_twin0, H.otw.data(), H.otw.size()));
+        BM_TRY(upload(ctx, &G.in_twin0, H.itw.data(), H.itw.size()));
+        BM_TRY(upload(ctx, &G.out_pos, H.otw.data(), H.otw.size()));  // sized here, written with the mapping
+        BM_TRY(upload(ctx, &G.in_pos, H.itw.data(), H.itw.size()));
         BM_TRY(upload(ctx, &G.out_ent0, H.oent.data(), H.oent.size()));
         BM_TRY(upload(ctx, &G.in_ent0, H.ient.data(), H.ient.size()));
         BM_TRY(upload(ctx, &G.hash, H.htab.data(), H.htab.size()));

@@ -13,11 +13,16 @@
 // kernel's scatter), not sorted; every kernel only sums over them.  The host
 // copy of A (ctx->hA_*) keeps them sorted by neighbour id.
 // Graph B additionally holds
-//   out_twin, in_twin           index of the same edge in the other direction
-//   out_ent0, in_ent0           the entries with B ids (immutable)
+//   out_ent0, in_ent0           the entries with B ids, sorted by id (immutable)
+//   out_twin0, in_twin0         index of the same edge in the other direction,
+//                               in the sorted lists (immutable)
 //   hash[2^k]                   open-addressing table (g*(n+1)+h) -> w of B edges
 // and its live out_ent/in_ent carry neighbour ids relabelled into A space
 // (id = pi^-1(B id)), so B'-out(x) = B-out(pi x) lists A vertices directly.
+// When the mapping is set the live lists are rebuilt from the sorted ones in
+// bank-spread order of their A ids (spread_relabel_kernel), with their own
+// twins out_twin/in_twin and the position maps out_pos/in_pos; swaps relabel
+// live entries in place through the live twins.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -40,10 +45,14 @@ struct DevGraph {
     uint32_t* in_ent = nullptr;
     int32_t* self_w = nullptr;
     // B only
-    int32_t* out_twin = nullptr;
+    int32_t* out_twin = nullptr;   // twins of the live lists (rebuilt with them)
     int32_t* in_twin = nullptr;
     uint32_t* out_ent0 = nullptr;
     uint32_t* in_ent0 = nullptr;
+    int32_t* out_twin0 = nullptr;  // twins of the id-sorted lists (immutable)
+    int32_t* in_twin0 = nullptr;
+    int32_t* out_pos = nullptr;    // id-sorted position -> live position
+    int32_t* in_pos = nullptr;
     unsigned long long* hash = nullptr;
     int32_t hash_log2 = 0;
     // statistics

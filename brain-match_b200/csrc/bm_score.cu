@@ -1,5 +1,6 @@
 // bm_score.cu — full overlap score and per-vertex overlap, and the
-// relabelling of B's lists into A space.
+// relabelling of B's lists into A space (with their bank-spread order and
+// twins).
 //
 // score(pi) = sum over A entries (x->y, w) of min(w, w_B(pi x, pi y)), the sum
 // of calculate_alignment_score (src/graph-alignment-optimized.c:292-307).
@@ -48,11 +49,47 @@ score_kernel(GView A, HashView hb, const int32_t* __restrict__ selfB, const int3
     }
 }
 
-__global__ void relabel_kernel(const uint32_t* __restrict__ ent0, uint32_t* __restrict__ ent,
-                               const int32_t* __restrict__ pinv, int64_t m) {
+// One thread per B list g: the list's entries relabelled into A space
+// (id = pi^-1(B id)) and written in bank-spread order of their A ids, the rule
+// of bm_bank_spread_lists (position p takes, where it can, an entry of bank
+// ((p >> 2) + 8 (p & 3)) mod 32, else the next bank up that still has
+// entries), so the row kernel's scatter over these lists meets fewer
+// shared-memory bank conflicts.  pos[j] = the live position of the entry at
+// position j of the id-sorted list; padding stays last and in place.  tmp
+// (one int32 per entry) holds each bank's entries while they are placed.
+__global__ void spread_relabel_kernel(const int32_t* __restrict__ ptr, const uint32_t* __restrict__ ent0,
+                                      const int32_t* __restrict__ pinv, int32_t n, uint32_t* __restrict__ ent,
+                                      int32_t* __restrict__ pos, int32_t* __restrict__ tmp) {
+    for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g <= n; g += gridDim.x * blockDim.x) {
+        const int32_t lo = __ldg(ptr + g), hi = __ldg(ptr + g + 1);
+        int32_t cnt = hi - lo;
+        while (cnt > 0 && __ldg(ent0 + lo + cnt - 1) == 0u) cnt--;  // padding is last
+        int32_t num[32], head[32], end[32];
+        for (int b = 0; b < 32; b++) num[b] = 0;
+        for (int32_t i = lo; i < lo + cnt; i++) num[__ldg(pinv + bm_eid(__ldg(ent0 + i))) & 31]++;
+        int32_t s = lo;
+        for (int b = 0; b < 32; b++) { head[b] = s; s += num[b]; end[b] = s; }
+        for (int32_t i = lo; i < lo + cnt; i++) tmp[head[__ldg(pinv + bm_eid(__ldg(ent0 + i))) & 31]++] = i;
+        for (int b = 0; b < 32; b++) head[b] = end[b] - num[b];
+        for (int32_t p = 0; p < cnt; p++) {
+            int b = ((p >> 2) + 8 * (p & 3)) & 31;
+            while (head[b] == end[b]) b = (b + 1) & 31;
+            const int32_t i = tmp[head[b]++];
+            const uint32_t e = __ldg(ent0 + i);
+            ent[lo + p] = bm_pack((uint32_t)__ldg(pinv + bm_eid(e)), (uint32_t)bm_ew(e));
+            pos[i] = lo + p;
+        }
+        for (int32_t j = lo + cnt; j < hi; j++) { ent[j] = 0u; pos[j] = j; }
+    }
+}
+
+// The twins of the live lists: the entry at live position pos_self[j] has its
+// reverse-direction twin at live position pos_other[twin0[j]] (-1: padding).
+__global__ void live_twins_kernel(const int32_t* __restrict__ twin0, const int32_t* __restrict__ pos_self,
+                                  const int32_t* __restrict__ pos_other, int32_t* __restrict__ twin, int64_t m) {
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t e = __ldg(ent0 + j);
-        ent[j] = bm_pack((uint32_t)__ldg(pinv + bm_eid(e)), (uint32_t)bm_ew(e));
+        const int32_t t0 = __ldg(twin0 + j);
+        twin[__ldg(pos_self + j)] = t0 < 0 ? -1 : __ldg(pos_other + t0);
     }
 }
 
@@ -95,14 +132,23 @@ bm_status bm_check_score(bm_ctx* ctx) {
 
 bm_status bm_launch_relabel(bm_ctx* ctx) {
     const DevGraph& B = ctx->g[1];
-    int blocks = ctx->num_sms * 4;
+    if (B.m_out + B.m_in == 0) return BM_OK;
+    const int blocks = (ctx->n + 1 + 127) / 128;
+    // the live twin arrays serve as the placement scratch, then are rebuilt
+    spread_relabel_kernel<<<blocks, 128, 0, ctx->stream>>>(B.out_ptr, B.out_ent0, ctx->pinv, ctx->n, B.out_ent,
+                                                           B.out_pos, B.out_twin);
+    BM_LAUNCH_CHECK(ctx, "spread_relabel_kernel(out)");
+    spread_relabel_kernel<<<blocks, 128, 0, ctx->stream>>>(B.in_ptr, B.in_ent0, ctx->pinv, ctx->n, B.in_ent,
+                                                           B.in_pos, B.in_twin);
+    BM_LAUNCH_CHECK(ctx, "spread_relabel_kernel(in)");
+    const int tb = ctx->num_sms * 4;
     if (B.m_out > 0) {
-        relabel_kernel<<<blocks, 256, 0, ctx->stream>>>(B.out_ent0, B.out_ent, ctx->pinv, B.m_out);
-        BM_LAUNCH_CHECK(ctx, "relabel_kernel(out)");
+        live_twins_kernel<<<tb, 256, 0, ctx->stream>>>(B.out_twin0, B.out_pos, B.in_pos, B.out_twin, B.m_out);
+        BM_LAUNCH_CHECK(ctx, "live_twins_kernel(out)");
     }
     if (B.m_in > 0) {
-        relabel_kernel<<<blocks, 256, 0, ctx->stream>>>(B.in_ent0, B.in_ent, ctx->pinv, B.m_in);
-        BM_LAUNCH_CHECK(ctx, "relabel_kernel(in)");
+        live_twins_kernel<<<tb, 256, 0, ctx->stream>>>(B.in_twin0, B.in_pos, B.out_pos, B.in_twin, B.m_in);
+        BM_LAUNCH_CHECK(ctx, "live_twins_kernel(in)");
     }
     return BM_OK;
 }
