@@ -135,6 +135,9 @@ struct bm_ctx {
         const void *stage = nullptr, *hstage = nullptr, *pi = nullptr, *ov = nullptr, *a = nullptr, *b = nullptr;
         int64_t launches = 0;  // kernels per replay
     } row_graph;
+    // set while the row graph is captured: its launches write each row
+    // result's row id last, after a system-scope fence (the host polls it)
+    bool row_host_res = false;
     // host copy of A's adjacency (independence tests of batched swaps)
     std::vector<int32_t> hA_optr, hA_iptr;
     std::vector<uint32_t> hA_oent, hA_ient;

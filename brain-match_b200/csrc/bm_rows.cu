@@ -115,6 +115,9 @@ struct RowArgs {
     // null = slot s takes row s
     const int32_t* rank_work;
     int32_t rank_lo;
+    // results in host memory polled by the caller: each row id is written
+    // last, after a system-scope fence, as the row's completion flag
+    int32_t host_res;
 };
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -677,7 +680,19 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             better_best(t.best_v, t.best_d, parts[q].best_v, parts[q].best_d);
             t.npos += parts[q].npos;
         }
-        a.res[r] = row_result(u, t);
+        const bm_row_result o = row_result(u, t);
+        if (a.host_res) {
+            bm_row_result* d = a.res + r;
+            d->first_pos = o.first_pos;
+            d->first_delta = o.first_delta;
+            d->best = o.best;
+            d->best_delta = o.best_delta;
+            d->npos = o.npos;
+            __threadfence_system();
+            *reinterpret_cast<volatile int32_t*>(&d->row) = o.row;
+        } else {
+            a.res[r] = o;
+        }
     }
 }
 
@@ -1002,6 +1017,7 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
         return (ctx->row_threads == 256) ? launch_rows_t<256, false>(ctx, x, c, smem, strm)
                                          : launch_rows_t<512, false>(ctx, x, c, smem, strm);
     };
+    args.host_res = ctx->row_host_res ? 1 : 0;
     args.rank_work = nullptr;
     args.rank_lo = 0;
     // Tiers: when the launch leaves resident CTA slots free, the H rows with
@@ -1111,12 +1127,19 @@ bool split_would_apply(const bm_ctx* ctx, int32_t nrows) {
 }
 
 constexpr int32_t kRowGraphMaxRows = 4096;
+constexpr int64_t kRowPollMax = 20000000;  // result polls before waiting on the stream (about a second)
 
 // bm_rows_best without column bounds as a replayed CUDA graph: the rows are
 // copied (CPU) into pinned staging, the graph copies them in and runs the row
 // launches (tiers included), which write the row results straight into pinned
 // staging (zero copy: 32 bytes a row over the host link, no copy-out step),
-// from which they are copied (CPU) to the caller.  The first call of a row
+// from which they are copied (CPU) to the caller.  Each result's row id
+// (1..n, every row having been checked) is written last, after a
+// system-scope fence, so the call polls the ids (reset to 0 before the
+// launch) and returns once all have arrived, without waiting for the stream
+// to drain; the graph's last steps complete in stream order before any later
+// work of the context.  The polling is bounded, then the stream is waited
+// for (a failed launch reports its error there).  The first call of a row
 // count runs plainly and then captures the graph; a change of row count,
 // staging buffers, graphs, semantics or row settings captures it again.
 bm_status rows_best_graph(bm_ctx* ctx, const int32_t* rows, int32_t nrows, bm_row_result* out) {
@@ -1136,8 +1159,26 @@ bm_status rows_best_graph(bm_ctx* ctx, const int32_t* rows, int32_t nrows, bm_ro
     bm_row_result* h_out = (bm_row_result*)((char*)ctx->hstage + rb);
     if (hit) {
         std::memcpy(h_in, rows, sizeof(int32_t) * (size_t)nrows);
+        for (int32_t r = 0; r < nrows; r++) h_out[r].row = 0;
         BM_CUDA(ctx, cudaGraphLaunch(G.exec, ctx->stream));
-        BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        auto arrived = [&]() {
+            for (int32_t r = 0; r < nrows; r++)
+                if (*reinterpret_cast<volatile int32_t*>(&h_out[r].row) == 0) return false;
+            return true;
+        };
+        bool done = false;
+        for (int64_t it = 0; !done; it++) {
+            done = arrived();
+            // every 1024 polls: stop polling once the stream has finished or
+            // failed, or after about a second
+            if (!done && (it & 1023) == 1023 &&
+                (cudaStreamQuery(ctx->stream) != cudaErrorNotReady || it > (int64_t)kRowPollMax))
+                break;
+        }
+        if (!done) {
+            BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            if (!arrived()) return bm_fail(ctx, BM_CUDA_ERROR, "row results missing after the row graph finished");
+        }
         ctx->launches += G.launches;
         std::memcpy(out, h_out, ob);
         return BM_OK;
@@ -1156,7 +1197,9 @@ bm_status rows_best_graph(bm_ctx* ctx, const int32_t* rows, int32_t nrows, bm_ro
     cudaGraph_t graph = nullptr;
     BM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     const cudaError_t c1 = cudaMemcpyAsync(d_rows, h_in, sizeof(int32_t) * (size_t)nrows, cudaMemcpyHostToDevice, ctx->stream);
+    ctx->row_host_res = true;
     const bm_status ls = c1 == cudaSuccess ? bm_launch_rows(ctx, d_rows, nullptr, nrows, nullptr, h_out, nullptr) : BM_OK;
+    ctx->row_host_res = false;
     const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
     const int64_t captured = ctx->launches - l0;
     ctx->launches = l0;

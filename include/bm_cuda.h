@@ -133,7 +133,11 @@ typedef struct bm_row_result {
 } bm_row_result;
 
 /* col_lo may be NULL (all columns); otherwise col_lo[r] is the first column
- * considered for row r.  Host buffers. */
+ * considered for row r.  Host buffers.  Without col_lo (and up to 4,096 rows,
+ * no split plan) the call replays a CUDA graph whose kernels write the
+ * results into pinned memory and returns as soon as every row's result has
+ * arrived; the graph's last steps finish in the context's stream order
+ * before any later work of the context. */
 bm_status bm_rows_best(bm_ctx* ctx, const int32_t* rows, const int32_t* col_lo,
                        int32_t nrows, bm_row_result* out);
 bm_status bm_rows_best_dev(bm_ctx* ctx, const int32_t* d_rows, const int32_t* d_col_lo,
