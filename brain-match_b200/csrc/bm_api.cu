@@ -150,7 +150,7 @@ extern "C" void bm_ctx_destroy(bm_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     free_graph(ctx->g[0]);
     free_graph(ctx->g[1]);
-    bm_cuda_free(ctx->pi); bm_cuda_free(ctx->pinv); bm_cuda_free(ctx->ov);
+    bm_cuda_free(ctx->pi); bm_cuda_free(ctx->pinv); bm_cuda_free(ctx->ov); bm_cuda_free(ctx->ximg);
     bm_cuda_free(ctx->d_score);
     bm_cuda_free(ctx->stage);
     bm_cuda_free(ctx->flush_buf);
@@ -326,14 +326,17 @@ extern "C" bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* pi) {
         BM_CUDA(ctx, bm_cuda_malloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
         BM_CUDA(ctx, bm_cuda_malloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
         BM_CUDA(ctx, bm_cuda_malloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->ximg, sizeof(int4) * ((size_t)n + 1)));
     } else {
         // sizes may have changed with a new graph
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        bm_cuda_free(ctx->pi); bm_cuda_free(ctx->pinv); bm_cuda_free(ctx->ov);
+        bm_cuda_free(ctx->pi); bm_cuda_free(ctx->pinv); bm_cuda_free(ctx->ov); bm_cuda_free(ctx->ximg);
         ctx->pi = ctx->pinv = ctx->ov = nullptr;
+        ctx->ximg = nullptr;
         BM_CUDA(ctx, bm_cuda_malloc(&ctx->pi, sizeof(int32_t) * ((size_t)n + 1)));
         BM_CUDA(ctx, bm_cuda_malloc(&ctx->pinv, sizeof(int32_t) * ((size_t)n + 1)));
         BM_CUDA(ctx, bm_cuda_malloc(&ctx->ov, sizeof(int32_t) * (size_t)ctx->nvec));
+        BM_CUDA(ctx, bm_cuda_malloc(&ctx->ximg, sizeof(int4) * ((size_t)n + 1)));
     }
     BM_CUDA(ctx, cudaMemcpyAsync(ctx->pi, h.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
     BM_CUDA(ctx, cudaMemcpyAsync(ctx->pinv, hinv.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));

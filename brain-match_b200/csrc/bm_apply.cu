@@ -31,6 +31,7 @@ struct ApplyArgs {
     int32_t* pi;
     int32_t* pinv;
     int32_t* ov;
+    int4* ximg;
 };
 
 __device__ __forceinline__ void relabel_twins(const int32_t* __restrict__ ptr, const int32_t* __restrict__ twin,
@@ -95,6 +96,8 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(ApplyArgs a, const
         a.pi[sb] = fa;
         a.pinv[fa] = sb;
         a.pinv[fb] = sa;
+        a.ximg[sa] = bm_image_bounds(a.Bin_ptr, a.Bout_ptr, fb);
+        a.ximg[sb] = bm_image_bounds(a.Bin_ptr, a.Bout_ptr, fa);
     }
 }
 
@@ -115,6 +118,7 @@ bm_status bm_launch_apply(bm_ctx* ctx, const int32_t* d_pairs, int32_t k) {
     a.pi = ctx->pi;
     a.pinv = ctx->pinv;
     a.ov = ctx->ov;
+    a.ximg = ctx->ximg;
     apply_kernel<<<k, kApplyThreads, 0, ctx->stream>>>(a, d_pairs);
     BM_LAUNCH_CHECK(ctx, "apply_kernel");
     return BM_OK;

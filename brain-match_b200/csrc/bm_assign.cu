@@ -139,6 +139,7 @@ struct PermArgs {
     int32_t* pi;
     int32_t* pinv;
     int32_t* ov;
+    int4* ximg;
 };
 
 // One CTA per moved member u: old image g0, new image g1.  Members share no A
@@ -179,6 +180,7 @@ __global__ void __launch_bounds__(kPermThreads) apply_perm_kernel(PermArgs a, co
     if (threadIdx.x == 0) {
         a.pi[u] = g1;
         a.pinv[g1] = u;
+        a.ximg[u] = bm_image_bounds(a.Bin_ptr, a.Bout_ptr, g1);
     }
 }
 
@@ -266,7 +268,7 @@ bm_status assign_subset(bm_ctx* ctx, const int32_t* subset, int32_t k, int64_t* 
         BM_CUDA(ctx, cudaMemcpyAsync(d_new, n_img.data(), sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
         const DevGraph& B = ctx->g[1];
         PermArgs pa{gview(ctx->g[0]), B.out_ptr, B.in_ptr, B.out_ent, B.in_ent, B.out_twin, B.in_twin, hview(B),
-                    ctx->pi, ctx->pinv, ctx->ov};
+                    ctx->pi, ctx->pinv, ctx->ov, ctx->ximg};
         apply_perm_kernel<<<m, kPermThreads, 0, ctx->stream>>>(pa, d_who, d_old, d_new);
         BM_LAUNCH_CHECK(ctx, "apply_perm_kernel");
         BM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

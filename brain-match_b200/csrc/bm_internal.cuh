@@ -89,6 +89,10 @@ struct bm_ctx {
     int32_t* pi = nullptr;
     int32_t* pinv = nullptr;
     int32_t* ov = nullptr;          // S(v): per-vertex non-self overlap
+    // per A vertex x, the bounds of B's lists at its image pi x:
+    // {in begin, in end, out begin, out end}; kept with pi by every kernel
+    // that moves images (the row kernel's first-hop staging reads it)
+    int4* ximg = nullptr;
     unsigned long long* d_score = nullptr;  // scratch for score reductions
     bool mapped = false;
     int64_t score = 0;              // tracked score
@@ -132,7 +136,8 @@ struct bm_ctx {
     struct RowGraph {
         cudaGraphExec_t exec = nullptr;
         int32_t nrows = -1, n = -1, semantics = -1, row_tiers = 0, row_ctas = -1, row_threads = -1;
-        const void *stage = nullptr, *hstage = nullptr, *pi = nullptr, *ov = nullptr, *a = nullptr, *b = nullptr;
+        const void *stage = nullptr, *hstage = nullptr, *pi = nullptr, *ov = nullptr, *ximg = nullptr, *a = nullptr,
+                   *b = nullptr;
         int64_t launches = 0;  // kernels per replay
     } row_graph;
     // set while the row graph is captured: its launches write each row
@@ -295,6 +300,11 @@ __device__ __forceinline__ int32_t bm_row_weight(const uint32_t* row, int32_t le
 }
 
 __device__ __forceinline__ int32_t imin(int32_t a, int32_t b) { return a < b ? a : b; }
+
+// The list bounds of image g, as kept in ctx->ximg for the A vertex mapped to g.
+__device__ __forceinline__ int4 bm_image_bounds(const int32_t* Bin_ptr, const int32_t* Bout_ptr, int32_t g) {
+    return make_int4(Bin_ptr[g], Bin_ptr[g + 1], Bout_ptr[g], Bout_ptr[g + 1]);
+}
 
 // Kernel launchers implemented across the .cu files.
 bm_status bm_launch_score(bm_ctx* ctx, int64_t* score_out);

@@ -341,6 +341,7 @@ struct ApplySetsArgs {
     int32_t* pi;
     int32_t* pinv;
     int32_t* ov;
+    int4* ximg;
     int32_t k;
     const int32_t* sets;
     const int32_t* perms;
@@ -402,6 +403,7 @@ __global__ void __launch_bounds__(kKThreads) apply_sets_kernel(ApplySetsArgs a) 
         for (int i = 0; i < k; i++) {
             a.pi[t[i]] = fn[i];
             a.pinv[fn[i]] = t[i];
+            a.ximg[t[i]] = bm_image_bounds(a.Bin_ptr, a.Bout_ptr, fn[i]);
         }
 }
 
@@ -457,6 +459,7 @@ bm_status bm_launch_apply_sets(bm_ctx* ctx, int32_t k, const int32_t* d_sets, co
     a.pi = ctx->pi;
     a.pinv = ctx->pinv;
     a.ov = ctx->ov;
+    a.ximg = ctx->ximg;
     a.k = k;
     a.sets = d_sets;
     a.perms = d_perms;

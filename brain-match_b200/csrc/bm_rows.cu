@@ -86,6 +86,7 @@ struct RowArgs {
     HashView hb;
     const int32_t* pi;
     const int32_t* ov;
+    const int4* ximg;  // per A vertex x, the bounds of B's lists at pi x
     int32_t n;
     const int32_t* rows;
     const int32_t* col_lo;
@@ -226,17 +227,20 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
         for (int32_t i = tid; i < (nv >> 2); i += THREADS) acc4[i] = make_int4(0, 0, 0, 0);
     }
     {
-        // the per-vertex arrays every row reads at random (pi, the four CSR
-        // pointer arrays, S(v)) are prefetched into L2 once per launch, one
-        // 128-byte line per thread spread over the grid, so the dependent
-        // loads of the first-hop staging and the finalise pass hit L2
+        // the per-vertex arrays every row reads at random (pi, S(v), A's two
+        // CSR pointer arrays, the image list bounds) are prefetched into L2
+        // once per launch, one 128-byte line per thread spread over the grid,
+        // so the dependent loads of the first-hop staging and the finalise
+        // pass hit L2.  The image bounds (four int32 per vertex) count as four
+        // segments of `lines` lines.
         const int32_t lines = (int32_t)((sizeof(int32_t) * ((size_t)nv + 4) + 127) / 128);
-        const int32_t total = 6 * lines;
+        const int32_t total = 8 * lines;
         for (int32_t j = tid * (int32_t)gridDim.x + (int32_t)blockIdx.x; j < total; j += THREADS * (int32_t)gridDim.x) {
             const int32_t k = j / lines, l = j - k * lines;
+            const int32_t seg = k < 4 ? 0 : (k - 4) * lines * 32;  // ints before this segment of the bounds
             const int32_t* arr = k == 0 ? a.pi : k == 1 ? a.ov : k == 2 ? a.Aout_ptr : k == 3 ? a.Ain_ptr
-                               : k == 4 ? a.Bout_ptr : a.Bin_ptr;
-            const int32_t lim = (k == 0) ? n + 1 : (k == 1) ? nv : n + 2;  // int32 elements of the array
+                               : reinterpret_cast<const int32_t*>(a.ximg) + seg;
+            const int32_t lim = (k == 0) ? n + 1 : (k == 1) ? nv : (k < 4) ? n + 2 : 4 * (n + 1) - seg;
             const int32_t e = l * 32;
             if (e < lim) asm volatile("prefetch.global.L2 [%0];" :: "l"(arr + e));
         }
@@ -331,19 +335,20 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
                 if (i < d1 + d2) {
                     const uint32_t ent = (i < d1) ? __ldg(a.Aout_ent + ao + i) : __ldg(a.Ain_ent + ai + (i - d1));
                     if (ent != 0) {
+                        // the list bounds at pi x come from the per-vertex
+                        // image record: one load instead of pi x, then its bounds
                         const int32_t x = bm_eid(ent), w = bm_ew(ent);
-                        const int32_t g = __ldg(a.pi + x);
+                        const int4 xb = __ldg(a.ximg + x);
                         if (i < d1) {
-                            const int32_t o = __ldg(a.Bin_ptr + g);
-                            base = a.Bin_ent + o;
-                            len = __ldg(a.Bin_ptr + g + 1) - o;
+                            base = a.Bin_ent + xb.x;
+                            len = xb.y - xb.x;
                         } else {
-                            const int32_t o = __ldg(a.Bout_ptr + g);
-                            base = a.Bout_ent + o;
-                            len = __ldg(a.Bout_ptr + g + 1) - o;
+                            base = a.Bout_ent + xb.z;
+                            len = xb.w - xb.z;
                         }
                         cap = w;
                         if (!a.half && !side_path && (i % CL) == crank) {
+                            const int32_t g = __ldg(a.pi + x);
                             const int32_t c = imin(w, bm_hash_get_small(a.hb, fu, g)) + imin(w, bm_hash_get_small(a.hb, g, fu));
                             if (c) atomicAdd(acc + x, c);
                         }
@@ -815,6 +820,7 @@ bm_status bm_rows_refresh_work(bm_ctx* ctx) {
     args.Bout_ent = B.out_ent;
     args.Bin_ent = B.in_ent;
     args.pi = ctx->pi;
+    args.ximg = ctx->ximg;
     args.n = ctx->n;
     const size_t threads = (size_t)ctx->n * 32;
     const unsigned blocks = (unsigned)((threads + kWorkThreads - 1) / kWorkThreads);
@@ -950,6 +956,7 @@ bm_status bm_launch_rows_gen(bm_ctx* ctx, const int32_t* d_rows, const int32_t* 
     args.has_self = args.refcpu ? A.has_self : (A.has_self && B.has_self);
     args.hb = hview(B);
     args.pi = ctx->pi;
+    args.ximg = ctx->ximg;
     args.ov = ctx->ov;
     args.n = ctx->n;
     args.rows = d_rows;
@@ -1152,6 +1159,7 @@ bm_status rows_best_graph(bm_ctx* ctx, const int32_t* rows, int32_t nrows, bm_ro
     const bool hit = G.exec && G.nrows == nrows && G.n == ctx->n && G.semantics == ctx->semantics &&
                      G.row_tiers == ctx->row_tiers && G.row_ctas == ctx->row_ctas && G.row_threads == ctx->row_threads &&
                      G.stage == ctx->stage && G.hstage == ctx->hstage && G.pi == ctx->pi && G.ov == ctx->ov &&
+                     G.ximg == ctx->ximg &&
                      G.a == ctx->g[0].out_ptr && G.b == ctx->g[1].out_ptr;
     int32_t* d_rows = (int32_t*)ctx->stage;
     bm_row_result* d_out = (bm_row_result*)((char*)ctx->stage + rb);
@@ -1226,6 +1234,7 @@ bm_status rows_best_graph(bm_ctx* ctx, const int32_t* rows, int32_t nrows, bm_ro
     G.hstage = ctx->hstage;
     G.pi = ctx->pi;
     G.ov = ctx->ov;
+    G.ximg = ctx->ximg;
     G.a = ctx->g[0].out_ptr;
     G.b = ctx->g[1].out_ptr;
     return BM_OK;

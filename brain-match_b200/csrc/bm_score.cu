@@ -83,6 +83,13 @@ __global__ void spread_relabel_kernel(const int32_t* __restrict__ ptr, const uin
     }
 }
 
+// ximg[x] = the bounds of B's in- and out-lists at pi x, for every A vertex.
+__global__ void image_bounds_kernel(const int32_t* __restrict__ pi, const int32_t* __restrict__ Bin_ptr,
+                                    const int32_t* __restrict__ Bout_ptr, int32_t n, int4* __restrict__ ximg) {
+    for (int32_t x = blockIdx.x * blockDim.x + threadIdx.x; x <= n; x += gridDim.x * blockDim.x)
+        ximg[x] = x == 0 ? make_int4(0, 0, 0, 0) : bm_image_bounds(Bin_ptr, Bout_ptr, __ldg(pi + x));
+}
+
 // The twins of the live lists: the entry at live position pos_self[j] has its
 // reverse-direction twin at live position pos_other[twin0[j]] (-1: padding).
 __global__ void live_twins_kernel(const int32_t* __restrict__ twin0, const int32_t* __restrict__ pos_self,
@@ -132,6 +139,8 @@ bm_status bm_check_score(bm_ctx* ctx) {
 
 bm_status bm_launch_relabel(bm_ctx* ctx) {
     const DevGraph& B = ctx->g[1];
+    image_bounds_kernel<<<(ctx->n + 1 + 255) / 256, 256, 0, ctx->stream>>>(ctx->pi, B.in_ptr, B.out_ptr, ctx->n, ctx->ximg);
+    BM_LAUNCH_CHECK(ctx, "image_bounds_kernel");
     if (B.m_out + B.m_in == 0) return BM_OK;
     const int blocks = (ctx->n + 1 + 127) / 128;
     // the live twin arrays serve as the placement scratch, then are rebuilt
