@@ -996,7 +996,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) mlp_rows_tc_kernel(TcArgs a) {
             tile_row(t, r, v0);
             bool w = true;
             if (t >= 2) w = role_wait(bar(D1FULL, (t - 2) & 3), par(t - 2), lim, abort);  // X free
-            if (w && t >= 4) w = role_wait(bar(DFREE, q), par(t - 4), lim, abort);        // slot free
             if (!role_bar_and(gbar, w)) { ok = false; break; }
             if (r != cur_r) {
                 // a new row: its bitmaps of the v with B(pi u, pi v) > 0
@@ -1023,7 +1022,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) mlp_rows_tc_kernel(TcArgs a) {
             const int32_t v = a.cands ? (ci < a.span ? __ldg(a.cands + (size_t)r * a.span + ci) : a.n + 1) : v0 + gtid;
             build_features(a, ta, bits_out, bits_in, u, v, load_cand(a, v), sm + kSmX + grp * kSmXBytes, gtid);
             proxy_fence();
-            role_bar(gbar);
+            // the TMEM slot is waited for only now: the features are built
+            // while tile t - 4 still holds it
+            w = true;
+            if (t >= 4) w = role_wait(bar(DFREE, q), par(t - 4), lim, abort);
+            if (!role_bar_and(gbar, w)) { ok = false; break; }
             if (leader) {
                 tc_fence_after();
 #pragma unroll
