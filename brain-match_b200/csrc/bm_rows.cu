@@ -191,6 +191,33 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
     Partial* wparts = parts + kMaxCluster;       // [32] warp partials
     int32_t* plan = reinterpret_cast<int32_t*>(wparts + 32);  // row, part, parts, last-arrival flag
 
+    // zeroing the accumulator and prefetching the per-vertex arrays; in rank
+    // mode this overlaps the loads of the rows' work estimates
+    auto zero_and_prefetch = [&]() {
+        {
+            int4* acc4 = reinterpret_cast<int4*>(acc);
+            for (int32_t i = tid; i < (nv >> 2); i += THREADS) acc4[i] = make_int4(0, 0, 0, 0);
+        }
+        {
+            // the per-vertex arrays every row reads at random (pi, S(v), A's two
+            // CSR pointer arrays, the image list bounds) are prefetched into L2
+            // once per launch, one 128-byte line per thread spread over the grid,
+            // so the dependent loads of the first-hop staging and the finalise
+            // pass hit L2.  The image bounds (four int32 per vertex) count as four
+            // segments of `lines` lines.
+            const int32_t lines = (int32_t)((sizeof(int32_t) * ((size_t)nv + 4) + 127) / 128);
+            const int32_t total = 8 * lines;
+            for (int32_t j = tid * (int32_t)gridDim.x + (int32_t)blockIdx.x; j < total; j += THREADS * (int32_t)gridDim.x) {
+                const int32_t k = j / lines, l = j - k * lines;
+                const int32_t seg = k < 4 ? 0 : (k - 4) * lines * 32;  // ints before this segment of the bounds
+                const int32_t* arr = k == 0 ? a.pi : k == 1 ? a.ov : k == 2 ? a.Aout_ptr : k == 3 ? a.Ain_ptr
+                                   : reinterpret_cast<const int32_t*>(a.ximg) + seg;
+                const int32_t lim = (k == 0) ? n + 1 : (k == 1) ? nv : (k < 4) ? n + 2 : 4 * (n + 1) - seg;
+                const int32_t e = l * 32;
+                if (e < lim) asm volatile("prefetch.global.L2 [%0];" :: "l"(arr + e));
+            }
+        }
+    };
     // plan[0..2]: row, part of the row, parts of the row.  Read back from
     // shared memory where needed (short register live ranges).
     if (a.rank_work) {
@@ -198,7 +225,14 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
         // it_len is free until the first item chunk is staged
         int32_t* wr = it_len;
         if (tid == 0) { plan[0] = -1; plan[1] = 0; plan[2] = 1; }
-        for (int32_t j = tid; j < a.nrows; j += THREADS) {
+        int32_t w0 = -1;
+        if (tid < a.nrows) {
+            const int32_t u0 = __ldg(a.rows + tid);
+            w0 = (u0 >= 1 && u0 <= n) ? __ldg(a.rank_work + u0) : -1;
+        }
+        zero_and_prefetch();
+        if (tid < a.nrows) wr[tid] = w0;
+        for (int32_t j = tid + THREADS; j < a.nrows; j += THREADS) {
             const int32_t uj = __ldg(a.rows + j);
             wr[j] = (uj >= 1 && uj <= n) ? __ldg(a.rank_work + uj) : -1;
         }
@@ -213,38 +247,18 @@ __global__ void __launch_bounds__(THREADS, 2) rows_kernel(RowArgs a) {
             }
             if (rk == want) plan[0] = j;
         }
-    } else if (tid == 0) {
-        if (a.slots) {
-            const int4 d = __ldg(a.slots + slot);
-            plan[0] = d.x; plan[1] = d.y; plan[2] = d.z;
-        } else {
-            plan[0] = slot; plan[1] = 0; plan[2] = 1;
+    } else {
+        if (tid == 0) {
+            if (a.slots) {
+                const int4 d = __ldg(a.slots + slot);
+                plan[0] = d.x; plan[1] = d.y; plan[2] = d.z;
+            } else {
+                plan[0] = slot; plan[1] = 0; plan[2] = 1;
+            }
         }
+        zero_and_prefetch();
     }
     auto P = [&](int k) -> int32_t { return *reinterpret_cast<volatile int32_t*>(plan + k); };
-    {
-        int4* acc4 = reinterpret_cast<int4*>(acc);
-        for (int32_t i = tid; i < (nv >> 2); i += THREADS) acc4[i] = make_int4(0, 0, 0, 0);
-    }
-    {
-        // the per-vertex arrays every row reads at random (pi, S(v), A's two
-        // CSR pointer arrays, the image list bounds) are prefetched into L2
-        // once per launch, one 128-byte line per thread spread over the grid,
-        // so the dependent loads of the first-hop staging and the finalise
-        // pass hit L2.  The image bounds (four int32 per vertex) count as four
-        // segments of `lines` lines.
-        const int32_t lines = (int32_t)((sizeof(int32_t) * ((size_t)nv + 4) + 127) / 128);
-        const int32_t total = 8 * lines;
-        for (int32_t j = tid * (int32_t)gridDim.x + (int32_t)blockIdx.x; j < total; j += THREADS * (int32_t)gridDim.x) {
-            const int32_t k = j / lines, l = j - k * lines;
-            const int32_t seg = k < 4 ? 0 : (k - 4) * lines * 32;  // ints before this segment of the bounds
-            const int32_t* arr = k == 0 ? a.pi : k == 1 ? a.ov : k == 2 ? a.Aout_ptr : k == 3 ? a.Ain_ptr
-                               : reinterpret_cast<const int32_t*>(a.ximg) + seg;
-            const int32_t lim = (k == 0) ? n + 1 : (k == 1) ? nv : (k < 4) ? n + 2 : 4 * (n + 1) - seg;
-            const int32_t e = l * 32;
-            if (e < lim) asm volatile("prefetch.global.L2 [%0];" :: "l"(arr + e));
-        }
-    }
     // Quad ranges are shared out across the whole cluster from counters in
     // CTA 0's shared memory (one per chunk parity), so a CTA that shares its
     // SM or also runs the corrections simply takes fewer ranges.
